@@ -1,0 +1,160 @@
+/*
+ * rumb: B200-native (sm_100a) subset-lattice kernels for certified random-utility (RUM) distances.
+ *
+ * C ABI of librumb.so. Every entry point returns an int status (RUMB_OK or an RUMB_E_* code) and
+ * never aborts, traps or prints; rumb_last_error() gives the calling thread's last message.
+ * Buffers are plain pointers owned by the caller: host memory unless a field says otherwise.
+ * A context (rumb_ctx) owns all device memory, streams, graphs and cached lattice tables of one
+ * GPU; calls on one context are serialized by the caller, except rumb_cancel, which any thread
+ * may call at any time.
+ *
+ * Slab layout: one value per (alternative x, menu S containing x) at x * 2^(n-1) + compress(S, x),
+ * compress = drop bit x and shift the higher bits down (the reference's layout,
+ * solver/bm_admm/kernels.py:24-35). A slab has n * 2^(n-1) entries.
+ *
+ * Reference interfaces replaced (file:line in mingxiz/rum-testing-gpu):
+ *   rumb_bm_solve            solve_kadmm_v2 + the certified runner's hooks
+ *                            (solver/bm_admm/solver.py:148-377, solver/rum_solver.py:869-911)
+ *   rumb_bm_iterate          one_iter, replayed `iters` times (solver/bm_admm/solver.py:240-254)
+ *   rumb_butterfly           Bfly2.apply / butterfly_fast (solver/bm_admm/butterfly2.py:275-282,
+ *                            solver/common/butterfly.py:381-422)
+ *   rumb_prox                prox_all (solver/bm_admm/solver.py:66-139)
+ *   rumb_push_ub64           push_to_ub64 (solver/common/transforms.py:94-98)
+ *   rumb_fw_lb64             fw_lb_rows_gpu (solver/common/transforms.py:101-114)
+ *   rumb_mem_info            machine.gpu_free_bytes (solver/machine.py:156-159)
+ */
+#ifndef RUMB_H
+#define RUMB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RUMB_API __attribute__((visibility("default")))
+#else
+#define RUMB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RUMB_VERSION 100
+
+/* status codes */
+#define RUMB_OK 0
+#define RUMB_E_INVAL 1    /* bad argument: sizes, dtype, n out of range */
+#define RUMB_E_OOM 2      /* device memory exhausted */
+#define RUMB_E_CUDA 3     /* any other CUDA error (message says which) */
+#define RUMB_E_TIMEOUT 4  /* a bounded device wait gave up */
+#define RUMB_E_CANCEL 5   /* rumb_cancel was called */
+#define RUMB_E_NODEV 6    /* no usable CUDA device */
+#define RUMB_E_INTERNAL 7 /* anything else */
+
+/* state dtypes of the ADMM iterate (the certificate is float64 in every mode) */
+#define RUMB_F64 0   /* float64 state */
+#define RUMB_F32 1   /* float32 state */
+#define RUMB_MIXED 2 /* float32 state until progress stalls, then float64 to the end */
+
+/* stop reasons of rumb_bm_solve */
+#define RUMB_STOP_GAP_ABS 1
+#define RUMB_STOP_GAP_REL 2
+#define RUMB_STOP_TIME 3
+#define RUMB_STOP_MAX_ITER 4
+#define RUMB_STOP_UB_TARGET 5
+#define RUMB_STOP_LB_TARGET 6
+#define RUMB_STOP_CANCEL 7
+
+typedef struct rumb_ctx rumb_ctx;
+typedef struct rumb_bm_state rumb_bm_state;
+
+RUMB_API int rumb_version(void);
+/* copies the calling thread's last error message (NUL-terminated, truncated to len) */
+RUMB_API int rumb_last_error(char *buf, size_t len);
+
+RUMB_API int rumb_ctx_create(int device, rumb_ctx **out);
+RUMB_API int rumb_ctx_destroy(rumb_ctx *ctx);
+/* run subsequent work on `stream` (a cudaStream_t of the context's device; NULL = the context's
+ * own stream) */
+RUMB_API int rumb_ctx_set_stream(rumb_ctx *ctx, void *stream);
+RUMB_API int rumb_ctx_sync(rumb_ctx *ctx);
+RUMB_API int rumb_mem_info(rumb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
+/* ask a running solve on ctx to stop at its next check (thread-safe) */
+RUMB_API int rumb_cancel(rumb_ctx *ctx);
+
+/* ---------------------------------------------------------------- primitives (host slabs) */
+/* out = the (a,b,c,d) 2x2 butterfly over the n-1 rest bits of every alternative block:
+ * pair (l, l | 2^j), lo' = a*lo + b*hi, hi' = c*lo + d*hi; dtype RUMB_F64 or RUMB_F32. */
+RUMB_API int rumb_butterfly(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, double a, double b,
+                   double c, double d);
+/* out = the per-menu simplex prox of v (all 2^n - 1 menus); xhat holds p_hat at observed entries,
+ * wmask is 1 at observed entries and 0 elsewhere. */
+RUMB_API int rumb_prox(rumb_ctx *ctx, int n, int dtype, const void *v, const void *xhat, const void *wmask,
+              double beta2, void *out);
+/* float64 upper bound at slab iterate x (dtype of x): the point pushed to an exact unit flow;
+ * ub = its distance to p on the mp observed rows, p_fit[mp] its values there (may be NULL). */
+RUMB_API int rumb_push_ub64(rumb_ctx *ctx, int n, int dtype, const void *x, long long mp, const uint32_t *menu,
+                   const int32_t *alt, const double *p, double *ub, double *p_fit);
+/* float64 Frank-Wolfe lower bound at the point with values y[mp] on the observed rows. */
+RUMB_API int rumb_fw_lb64(rumb_ctx *ctx, int n, long long mp, const uint32_t *menu, const int32_t *alt,
+                 const double *y, const double *p, double *lb);
+
+/* ---------------------------------------------------------------- BM-ADMM */
+typedef struct {
+    int n;               /* alternatives, 2 <= n <= 30 */
+    long long mp;        /* observed (menu, alternative) rows, menus with >= 2 members */
+    const uint32_t *menu;
+    const int32_t *alt;
+    const double *p;     /* p_hat (any finite values) */
+    int on_device;       /* 1: menu, alt, p are device pointers of the context's device */
+} rumb_bm_problem;
+
+typedef struct {
+    double beta;         /* penalty (beta1 = beta2) */
+    double alpha;        /* over-relaxation */
+    double precond_p;    /* per-bit preconditioner p of the inequality block */
+    int check;           /* iterations between upper bounds */
+    int lb_every;        /* upper-bound checks between lower bounds */
+    long long max_iter;
+    double abs_tol;      /* stop at ub - lb <= abs_tol (< 0: off) */
+    double rel_tol;      /* stop at (ub - lb) / lb <= rel_tol (< 0: off) */
+    double time_limit;   /* seconds from the start of the call (<= 0: none) */
+    double ub_target;    /* stop once ub <= ub_target (NaN: none) */
+    double lb_target;    /* stop once lb >= lb_target (NaN: none) */
+    int dtype;           /* RUMB_F64, RUMB_F32 or RUMB_MIXED */
+    int use_graph;       /* 1: replay each check interval as one CUDA graph */
+    int stall_checks;    /* RUMB_MIXED: checks without progress before float64 takes over */
+    double stall_rtol;   /* RUMB_MIXED: relative progress that counts */
+} rumb_bm_params;
+
+typedef struct {
+    double lb, ub;       /* best certified bracket on the observed rows */
+    double phi;          /* distance of the last iterate (not a bound) */
+    long long iters;     /* ADMM iterations run */
+    long long iters_f32; /* of which in float32 (RUMB_F32 / RUMB_MIXED) */
+    int stop;            /* RUMB_STOP_* */
+    int n_push, n_lb;
+    double setup_s, solve_s, push_s, per_iter_ms;
+    double device_ms;    /* CUDA-event time of the solve on the context's stream */
+} rumb_bm_result;
+
+/* called once per check with (iterations, seconds since the call, phi, best ub, best lb) */
+typedef void (*rumb_trace_fn)(void *user, long long iter, double wall_s, double phi, double ub, double lb);
+
+/* Certified solve. warm: start from a kept state (NULL: the cold start prox(xhat)); keep: if not
+ * NULL, receives a new handle holding the final state (free with rumb_bm_state_destroy);
+ * p_fit[mp] (may be NULL): the observed values of the best upper-bound point. */
+RUMB_API int rumb_bm_solve(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par,
+                  const rumb_bm_state *warm, rumb_bm_state **keep, rumb_bm_result *res, double *p_fit,
+                  rumb_trace_fn trace, void *user);
+RUMB_API int rumb_bm_state_destroy(rumb_bm_state *st);
+/* Runs `iters` ADMM iterations from the host state (x2, s, y, z: slabs in par->dtype, float32
+ * for RUMB_MIXED) and writes the state back; cold_start = 1 first sets x2 = prox(xhat), s = y = z
+ * = 0. For iterate-level parity checks. */
+RUMB_API int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, void *x2,
+                    void *s, void *y, void *z, int iters, int cold_start);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

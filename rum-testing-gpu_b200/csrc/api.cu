@@ -1,0 +1,192 @@
+// The C ABI of librumb.so (include/rumb.h): argument checks, the context, error capture.
+// Every entry point catches everything, records a message for rumb_last_error and returns a
+// status code; nothing here aborts, traps or prints.
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "bm.cuh"
+#include "ctx.cuh"
+
+namespace rumb {
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace rumb
+
+using rumb::Error;
+
+#define RUMB_API_BEGIN try {
+#define RUMB_API_END                                                   \
+    }                                                                  \
+    catch (const Error &e) {                                           \
+        rumb::set_last_error(e.what());                                \
+        return e.code;                                                 \
+    }                                                                  \
+    catch (const std::bad_alloc &) {                                   \
+        rumb::set_last_error("host memory exhausted");                 \
+        return RUMB_E_OOM;                                             \
+    }                                                                  \
+    catch (const std::exception &e) {                                  \
+        rumb::set_last_error(e.what());                                \
+        return RUMB_E_INTERNAL;                                        \
+    }                                                                  \
+    catch (...) {                                                      \
+        rumb::set_last_error("unknown error");                         \
+        return RUMB_E_INTERNAL;                                        \
+    }
+
+#define NEED_CTX(ctx)                                                  \
+    if (!(ctx)) rumb::fail(RUMB_E_INVAL, "context is NULL");           \
+    rumb::DeviceGuard _dg((ctx)->c.device)
+
+extern "C" {
+
+int rumb_version(void) { return RUMB_VERSION; }
+
+int rumb_last_error(char *buf, size_t len) {
+    if (!buf || len == 0) return RUMB_E_INVAL;
+    std::snprintf(buf, len, "%s", rumb::g_last_error.c_str());
+    return RUMB_OK;
+}
+
+int rumb_ctx_create(int device, rumb_ctx **out) {
+    RUMB_API_BEGIN
+    if (!out) rumb::fail(RUMB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        rumb::fail(RUMB_E_NODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count) rumb::fail(RUMB_E_INVAL, "device index out of range");
+    rumb::DeviceGuard dg(device);
+    rumb_ctx *c = new rumb_ctx();
+    c->c.device = device;
+    try {
+        RUMB_CUDA(cudaStreamCreateWithFlags(&c->c.own, cudaStreamNonBlocking));
+        RUMB_CUDA(cudaEventCreateWithFlags(&c->c.ev_a, cudaEventDisableTiming));
+        RUMB_CUDA(cudaEventCreateWithFlags(&c->c.ev_b, cudaEventDisableTiming));
+    } catch (...) {
+        delete c;
+        throw;
+    }
+    *out = c;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_ctx_destroy(rumb_ctx *ctx) {
+    RUMB_API_BEGIN
+    if (!ctx) return RUMB_OK;
+    {
+        rumb::DeviceGuard dg(ctx->c.device);
+        cudaStreamSynchronize(ctx->c.own);
+        ctx->c.bm64.reset();
+        ctx->c.bm32.reset();
+        ctx->c.cert.reset();
+        ctx->c.scratch.reset();
+        ctx->c.layers.clear();
+        if (ctx->c.ev_a) cudaEventDestroy(ctx->c.ev_a);
+        if (ctx->c.ev_b) cudaEventDestroy(ctx->c.ev_b);
+        if (ctx->c.own) cudaStreamDestroy(ctx->c.own);
+    }
+    delete ctx;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_ctx_set_stream(rumb_ctx *ctx, void *stream) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    ctx->c.user = reinterpret_cast<cudaStream_t>(stream);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_ctx_sync(rumb_ctx *ctx) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    RUMB_CUDA(cudaStreamSynchronize(ctx->c.own));
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mem_info(rumb_ctx *ctx, size_t *free_bytes, size_t *total_bytes) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    size_t f = 0, t = 0;
+    RUMB_CUDA(cudaMemGetInfo(&f, &t));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cancel(rumb_ctx *ctx) {
+    if (!ctx) return RUMB_E_INVAL;
+    ctx->c.cancel.store(1);
+    return RUMB_OK;
+}
+
+int rumb_butterfly(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, double a, double b, double c,
+                   double d) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::butterfly_host(ctx->c, n, dtype, in, out, a, b, c, d);
+    RUMB_API_END
+}
+
+int rumb_prox(rumb_ctx *ctx, int n, int dtype, const void *v, const void *xhat, const void *wmask, double beta2,
+              void *out) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::prox_host(ctx->c, n, dtype, v, xhat, wmask, beta2, out);
+    RUMB_API_END
+}
+
+int rumb_push_ub64(rumb_ctx *ctx, int n, int dtype, const void *x, long long mp, const uint32_t *menu,
+                   const int32_t *alt, const double *p, double *ub, double *p_fit) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::push_ub64_host(ctx->c, n, dtype, x, mp, menu, alt, p, ub, p_fit);
+    RUMB_API_END
+}
+
+int rumb_fw_lb64(rumb_ctx *ctx, int n, long long mp, const uint32_t *menu, const int32_t *alt, const double *y,
+                 const double *p, double *lb) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::fw_lb64_host(ctx->c, n, mp, menu, alt, y, p, lb);
+    RUMB_API_END
+}
+
+int rumb_bm_solve(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, const rumb_bm_state *warm,
+                  rumb_bm_state **keep, rumb_bm_result *res, double *p_fit, rumb_trace_fn trace, void *user) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    if (keep) *keep = nullptr;
+    return rumb::bm_solve(ctx->c, prob, par, warm, keep, res, p_fit, trace, user);
+    RUMB_API_END
+}
+
+int rumb_bm_state_destroy(rumb_bm_state *st) {
+    RUMB_API_BEGIN
+    if (!st) return RUMB_OK;
+    rumb::DeviceGuard dg(st->device);
+    delete st;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, void *x2, void *s,
+                    void *y, void *z, int iters, int cold_start) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    if (!x2 || !s || !y || !z) rumb::fail(RUMB_E_INVAL, "state buffers must not be NULL");
+    if (iters < 0) rumb::fail(RUMB_E_INVAL, "iters must be >= 0");
+    return rumb::bm_iterate(ctx->c, prob, par, x2, s, y, z, iters, cold_start);
+    RUMB_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,1124 @@
+// BM-ADMM on the Block-Marschak slab (sm_100a): the fused per-menu prox, the float64
+// certificate (feasibility push -> upper bound, Frank-Wolfe longest path -> lower bound) and the
+// certified solve loop.
+//
+// Reference behaviour (mingxiz/rum-testing-gpu):
+//   iteration        solver/bm_admm/solver.py:33-54 (_EW_SRC), :240-254 (one_iter)
+//   prox             solver/bm_admm/solver.py:66-139 (prox_all)
+//   setup            solver/bm_admm/solver.py:184-238 (scatter, eigen data, cold start)
+//   check loop       solver/bm_admm/solver.py:308-367 with the runner's hooks
+//                    solver/rum_solver.py:869-911 (running-min push, lower bound every lb_every)
+//   push (UB)        solver/common/transforms.py:94-98, solver/common/arcflow_kernels.py:357-434
+//   Frank-Wolfe LB   solver/common/transforms.py:101-114, solver/common/arcflow_kernels.py:388-448
+//
+// Per iteration this runs 4 butterflies (A', Q^T with the eigen-space diagonal fused into its
+// last store, Q, A) with the w / rhs elementwise steps fused into the A' loads and stores, and
+// ONE prox kernel that also does the over-relaxed point, the z update, the s/y update with its
+// nonnegativity clamp and the x2 copy (the reference's fuse_xk, prox_all, fuse_z, fuse_sy and
+// copyto). The prox walks menus in mask order, so a warp's members of one alternative are 32
+// consecutive entries of that alternative's block (coalesced), and projects with Michelot's
+// active-set iteration in registers instead of an insertion sort.
+#include <chrono>
+#include <cstring>
+
+#include "bfly.cuh"
+#include "bm.cuh"
+#include "ctx.cuh"
+
+namespace rumb {
+
+// ================================================================= prox
+template <class T>
+struct ProxArgs {
+    int n;
+    ll Nloc, nmenus;
+    const T *v;         // PROX mode input
+    T *out;             // PROX mode output
+    const T *x, *Ax;    // ITER mode inputs
+    T *x2, *z, *s, *y;  // ITER mode state (updated in place)
+    const T *xhat;
+    const uint32_t *obsbits;
+    T alpha, b1, b2, ib1, ib2;
+};
+
+enum { PROX_ONLY = 0, PROX_ITER = 1 };
+
+template <class T, int N, int MODE>
+__global__ void __launch_bounds__(128) prox_kernel(ProxArgs<T> P) {
+    ll gid = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (gid >= P.nmenus) return;
+    const uint32_t S = (uint32_t)(gid + 1);
+    const int n = P.n;
+    const int k = __popc(S);
+    // observed members
+    uint32_t wb = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (i < n && ((S >> i) & 1u)) {
+            ll pos = (ll)i * P.Nloc + (ll)compress_bit(S ^ (1u << i), i);
+            if ((P.obsbits[pos >> 5] >> (pos & 31)) & 1u) wb |= 1u << i;
+        }
+    }
+    const bool mixed = wb != 0 && wb != S;
+    double t[N];
+    T q[N];
+    const T two = (T)2, one = (T)1;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        t[i] = 0.0;
+        q[i] = (T)0;
+        if (i < n && ((S >> i) & 1u)) {
+            ll pos = (ll)i * P.Nloc + (ll)compress_bit(S ^ (1u << i), i);
+            T v;
+            if (MODE == PROX_ITER) {
+                T xi = P.x[pos], x2i = P.x2[pos], zi = P.z[pos];
+                T xo = P.alpha * xi + (one - P.alpha) * x2i;
+                v = xo - P.ib2 * zi;
+                q[i] = xo;
+                T ax = P.Ax[pos], si = P.s[pos], yi = P.y[pos];
+                T axor = -P.alpha * ax - (one - P.alpha) * si;
+                T sn = P.ib1 * yi - axor;
+                sn = sn > (T)0 ? sn : (T)0;
+                P.y[pos] = yi - P.b1 * (axor + sn);
+                P.s[pos] = sn;
+            } else {
+                v = P.v[pos];
+            }
+            bool w = (wb >> i) & 1u;
+            T xh = w ? P.xhat[pos] : (T)0;
+            T wt = w ? one : (T)0;
+            if (mixed) t[i] = (double)P.b2 * (double)v + 2.0 * (double)wt * (double)xh;
+            else t[i] = (double)((P.b2 * v + two * wt * xh) / (P.b2 + two * wt));
+        }
+    }
+    // threshold (Michelot's active-set iteration: the active set only shrinks, <= k rounds)
+    double tau = 0.0;
+    if (k > 1) {
+        if (!mixed) {
+            uint32_t A = S;
+            double sum = 0.0;
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+                if ((A >> i) & 1u) sum += t[i];
+            tau = (sum - 1.0) / (double)k;
+            for (int round = 0; round < N; ++round) {
+                uint32_t A2 = 0;
+                double s2 = 0.0;
+                int c2 = 0;
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                    if (((A >> i) & 1u) && t[i] > tau) { A2 |= 1u << i; s2 += t[i]; ++c2; }
+                if (A2 == A) break;
+                A = A2;
+                tau = (s2 - 1.0) / (double)c2;
+            }
+        } else {
+            const double cw = (double)P.b2 + 2.0, cu = (double)P.b2;   // curvature observed / not
+            uint32_t A = S;
+            double stc = 0.0, sic = 0.0;
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+                if ((A >> i) & 1u) {
+                    double c = ((wb >> i) & 1u) ? cw : cu;
+                    stc += t[i] / c;
+                    sic += 1.0 / c;
+                }
+            tau = (stc - 1.0) / sic;
+            for (int round = 0; round < N; ++round) {
+                uint32_t A2 = 0;
+                double s2 = 0.0, i2 = 0.0;
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                    if (((A >> i) & 1u) && t[i] > tau) {
+                        double c = ((wb >> i) & 1u) ? cw : cu;
+                        A2 |= 1u << i; s2 += t[i] / c; i2 += 1.0 / c;
+                    }
+                if (A2 == A) break;
+                A = A2;
+                tau = (s2 - 1.0) / i2;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (i < n && ((S >> i) & 1u)) {
+            ll pos = (ll)i * P.Nloc + (ll)compress_bit(S ^ (1u << i), i);
+            T u;
+            if (k == 1) {
+                u = one;
+            } else if (mixed) {
+                double c = ((wb >> i) & 1u) ? (double)P.b2 + 2.0 : (double)P.b2;
+                double yv = (t[i] - tau) / c;
+                u = yv > 0.0 ? (T)yv : (T)0;
+            } else {
+                double yv = t[i] - tau;
+                u = yv > 0.0 ? (T)yv : (T)0;
+            }
+            if (MODE == PROX_ITER) {
+                P.z[pos] = P.z[pos] - P.b2 * (q[i] - u);
+                P.x2[pos] = u;
+            } else {
+                P.out[pos] = u;
+            }
+        }
+    }
+}
+
+template <class T, int MODE>
+static void launch_prox_n(const ProxArgs<T> &P, cudaStream_t st) {
+    const int TB = 128;
+    unsigned grid = grid_for(P.nmenus, TB);
+    int n = P.n;
+#define RUMB_PROX_CASE(NN)                                          \
+    if (n <= NN) {                                                  \
+        prox_kernel<T, NN, MODE><<<grid, TB, 0, st>>>(P);           \
+        RUMB_LAUNCH("prox_kernel");                                 \
+        return;                                                     \
+    }
+    RUMB_PROX_CASE(8)
+    RUMB_PROX_CASE(12)
+    RUMB_PROX_CASE(16)
+    RUMB_PROX_CASE(20)
+    RUMB_PROX_CASE(24)
+    RUMB_PROX_CASE(28)
+    RUMB_PROX_CASE(30)
+#undef RUMB_PROX_CASE
+    fail(RUMB_E_INVAL, "prox: n > 30");
+}
+
+// ================================================================= observation setup
+template <class T>
+__global__ void obs_setup_kernel(const uint32_t *menu, const int32_t *alt, const double *p, ll mp, int n,
+                                 ll Nloc, ll *obs, T *xhat, uint32_t *obsbits, int *bad) {
+    ll j = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (j >= mp) return;
+    int x = alt[j];
+    uint32_t m = menu[j];
+    if (x < 0 || x >= n || !((m >> x) & 1u) || (n < 32 && (m >> n) != 0) || __popc(m) < 2) {
+        atomicExch(bad, 1);
+        obs[j] = 0;
+        return;
+    }
+    ll pos = (ll)x * Nloc + (ll)compress_bit(m & ~(1u << x), x);
+    obs[j] = pos;
+    xhat[pos] = (T)p[j];
+    atomicOr(&obsbits[pos >> 5], 1u << (pos & 31));
+}
+
+// ================================================================= float64 certificate
+// The push works on q = Mobius(x) and recomputes the clipped weights w = max(q, 0) + eps where
+// they are read, instead of storing a w slab.
+__device__ __forceinline__ double wclip(double q, double eps) { return (q > 0.0 ? q : 0.0) + eps; }
+
+__global__ void outw_kernel(const double *q, double *outw, int n, ll Nloc, double eps) {
+    ll D = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    ll N = 1LL << n;
+    if (D >= N) return;
+    double s = 0.0;
+    for (int x = 0; x < n; ++x) {
+        ll bit = 1LL << x;
+        if (!(D & bit)) s += wclip(q[(ll)x * Nloc + (ll)compress_bit((ull)D, x)], eps);
+    }
+    outw[D] = s;
+}
+
+__global__ void mass_layer_kernel(const double *q, const double *outw, double *mass, const int *nodes, ll ns,
+                                  int n, ll Nloc, double eps) {
+    ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    ll C = nodes[i];
+    double s = 0.0;
+    for (int x = 0; x < n; ++x) {
+        ll bit = 1LL << x;
+        if (C & bit) {
+            ll P = C ^ bit;
+            double ow = outw[P];
+            if (ow > 0.0) s += mass[P] * wclip(q[(ll)x * Nloc + (ll)compress_bit((ull)P, x)], eps) / ow;
+        }
+    }
+    mass[C] = s;
+}
+
+__global__ void extract_kernel(const double *q, const double *outw, const double *mass, double *rf, int n,
+                               ll Nloc, double eps) {
+    ll a = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    ll m2 = (ll)n * Nloc;
+    if (a >= m2) return;
+    ll x = a / Nloc, rest = a - x * Nloc;
+    ll T = (ll)expand_bit((ull)rest, (int)x);
+    double ow = outw[T];
+    rf[a] = (ow > 0.0) ? mass[T] * wclip(q[a], eps) / ow : 0.0;
+}
+
+__global__ void lpath_layer_kernel(const double *R, double *dp, const int *nodes, ll ns, int n, ll Nloc) {
+    ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    ll C = nodes[i];
+    double best = -1e300;
+    for (int x = 0; x < n; ++x) {
+        ll bit = 1LL << x;
+        if (C & bit) {
+            ll P = C ^ bit;
+            double v = dp[P] + R[(ll)x * Nloc + (ll)compress_bit((ull)P, x)];
+            if (v > best) best = v;
+        }
+    }
+    dp[C] = best;
+}
+
+constexpr int RED_THREADS = 1024;
+
+// Deterministic single-block sum of the per-thread partials (fixed order for a fixed size).
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x < 32) {
+        r = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    return r;  // valid in thread 0
+}
+
+// Result slots of one check (device doubles)
+enum { R_PHI2 = 0, R_RY = 1, R_UB_NOW = 2, R_UB_BEST = 3, R_LB_NOW = 4, R_SLOTS = 8 };
+
+// phi^2 = sum (p - x2[obs])^2 and sum (p - y) y at the iterate; LB scatter g[obs] = r if g
+template <class T>
+__global__ void obs_stats_kernel(const T *x2, const ll *obs, const double *p, ll mp, double *g, double *res) {
+    __shared__ double sh[32];
+    double f = 0.0, ry = 0.0;
+    for (ll j = threadIdx.x; j < mp; j += blockDim.x) {
+        double y = (double)x2[obs[j]];
+        double r = p[j] - y;
+        f += r * r;
+        ry += r * y;
+        if (g) g[obs[j]] = r;
+    }
+    double F = block_sum(f, sh);
+    double RY = block_sum(ry, sh);
+    if (threadIdx.x == 0) { res[R_PHI2] = F; res[R_RY] = RY; }
+}
+
+__global__ void ub_eval_kernel(const double *xub, const ll *obs, const double *p, ll mp, double *pfit_cur,
+                               double *res) {
+    __shared__ double sh[32];
+    double f = 0.0;
+    for (ll j = threadIdx.x; j < mp; j += blockDim.x) {
+        double v = xub[obs[j]];
+        pfit_cur[j] = v;
+        double d = v - p[j];
+        f += d * d;
+    }
+    double F = block_sum(f, sh);
+    if (threadIdx.x == 0) res[R_UB_NOW] = sqrt(F);
+}
+
+__global__ void ub_commit_kernel(const double *pfit_cur, double *pfit_best, ll mp, const double *res) {
+    ll j = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (j >= mp) return;
+    if (res[R_UB_NOW] < res[R_UB_BEST]) pfit_best[j] = pfit_cur[j];
+}
+
+__global__ void ub_best_kernel(double *res) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && res[R_UB_NOW] < res[R_UB_BEST]) res[R_UB_BEST] = res[R_UB_NOW];
+}
+
+__global__ void lb_final_kernel(const double *dp, ll N, double *res) {
+    double rc = dp[N - 1] - res[R_RY];
+    double v = res[R_PHI2] - 2.0 * rc;
+    res[R_LB_NOW] = sqrt(v > 0.0 ? v : 0.0);
+}
+
+__global__ void set_doubles_kernel(double *p, int count, double v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) p[i] = v;
+}
+
+template <class TI, class TO>
+__global__ void convert_kernel(const TI *in, TO *out, ll m) {
+    ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (i < m) out[i] = (TO)in[i];
+}
+
+// ----------------------------------------------------------------- layers (host build, cached)
+const int *Ctx::layer_table(int n, std::vector<ll> &bounds) {
+    auto it = layers.find(n);
+    if (it != layers.end()) {
+        bounds = layer_bounds[n];
+        return it->second->as<int>();
+    }
+    ll N = 1LL << n;
+    std::vector<ll> cnt(n + 2, 0);
+    for (ll v = 0; v < N; ++v) cnt[__builtin_popcountll((ull)v) + 1]++;
+    std::vector<ll> b(n + 2, 0);
+    for (int c = 0; c <= n; ++c) b[c + 1] = b[c] + cnt[c + 1];
+    std::vector<ll> fill(b.begin(), b.end() - 1);
+    std::vector<int> order(N);
+    for (ll v = 0; v < N; ++v) order[fill[__builtin_popcountll((ull)v)]++] = (int)v;
+    auto buf = std::make_shared<DevBuf>();
+    buf->ensure((size_t)N * sizeof(int));
+    RUMB_CUDA(cudaMemcpy(buf->ptr, order.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice));
+    layers[n] = buf;
+    layer_bounds[n] = b;
+    bounds = b;
+    return buf->as<int>();
+}
+
+// ----------------------------------------------------------------- certificate workspace
+struct CertWork : public BmWorkBase {
+    DevBuf qa, qb;            // float64 slabs
+    DevBuf outw, mass, dp;    // float64 node arrays
+    DevBuf obs, p;            // observed positions and p (mp)
+    DevBuf pfit_cur, pfit_best;
+    DevBuf res;               // R_SLOTS doubles
+    ll mp = 0;
+    int n = 0;
+    void ensure(int n_, ll mp_) {
+        n = n_;
+        mp = mp_;
+        ll m2 = (ll)n << (n - 1), N = 1LL << n;
+        qa.ensure((size_t)m2 * 8);
+        qb.ensure((size_t)m2 * 8);
+        outw.ensure((size_t)N * 8);
+        mass.ensure((size_t)N * 8);
+        dp.ensure((size_t)N * 8);
+        obs.ensure((size_t)mp * 8);
+        p.ensure((size_t)mp * 8);
+        pfit_cur.ensure((size_t)mp * 8);
+        pfit_best.ensure((size_t)mp * 8);
+        res.ensure(R_SLOTS * 8);
+    }
+};
+
+static CertWork &cert_work(Ctx &c) {
+    if (!c.cert) c.cert.reset(new CertWork());
+    return *static_cast<CertWork *>(c.cert.get());
+}
+
+// UB part of a check: x2 (dtype T) -> q = Mobius -> push -> zeta -> ub_now, pfit; running best.
+template <class T>
+static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t st) {
+    ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
+    const double eps = 1e-12;
+    double *qa = W.qa.as<double>(), *qb = W.qb.as<double>();
+    bf_transform<double, T>(n, x2, qa, 1.0, -1.0, 0.0, 1.0, st);          // Mobius
+    outw_kernel<<<grid_for(N, 256), 256, 0, st>>>(qa, W.outw.as<double>(), n, Nloc, eps);
+    RUMB_LAUNCH("outw_kernel");
+    std::vector<ll> bounds;
+    const int *nodes = c.layer_table(n, bounds);
+    set_doubles_kernel<<<1, 32, 0, st>>>(W.mass.as<double>(), 1, 1.0);    // mass[empty set] = 1
+    RUMB_LAUNCH("set_doubles");
+    for (int cc = 1; cc <= n; ++cc) {
+        ll lo = bounds[cc], ns = bounds[cc + 1] - lo;
+        if (ns <= 0) continue;
+        mass_layer_kernel<<<grid_for(ns, 256), 256, 0, st>>>(qa, W.outw.as<double>(), W.mass.as<double>(),
+                                                             nodes + lo, ns, n, Nloc, eps);
+        RUMB_LAUNCH("mass_layer_kernel");
+    }
+    extract_kernel<<<grid_for(m2, 256), 256, 0, st>>>(qa, W.outw.as<double>(), W.mass.as<double>(), qb, n, Nloc,
+                                                      eps);
+    RUMB_LAUNCH("extract_kernel");
+    bf_transform<double, double>(n, qb, qa, 1.0, 1.0, 0.0, 1.0, st);      // zeta -> x_ub in qa
+    ub_eval_kernel<<<1, RED_THREADS, 0, st>>>(qa, W.obs.as<ll>(), W.p.as<double>(), W.mp,
+                                              W.pfit_cur.as<double>(), W.res.as<double>());
+    RUMB_LAUNCH("ub_eval_kernel");
+    ub_commit_kernel<<<grid_for(W.mp, 256), 256, 0, st>>>(W.pfit_cur.as<double>(), W.pfit_best.as<double>(), W.mp,
+                                                         W.res.as<double>());
+    RUMB_LAUNCH("ub_commit_kernel");
+    ub_best_kernel<<<1, 32, 0, st>>>(W.res.as<double>());
+    RUMB_LAUNCH("ub_best_kernel");
+}
+
+// phi (and the LB's residual sums); with_lb also scatters g and runs the longest path.
+template <class T>
+static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_lb, cudaStream_t st) {
+    ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
+    double *g = W.qb.as<double>();
+    if (with_lb) RUMB_CUDA(cudaMemsetAsync(g, 0, (size_t)m2 * 8, st));
+    obs_stats_kernel<T><<<1, RED_THREADS, 0, st>>>(x2, W.obs.as<ll>(), W.p.as<double>(), W.mp,
+                                                   with_lb ? g : nullptr, W.res.as<double>());
+    RUMB_LAUNCH("obs_stats_kernel");
+    if (!with_lb) return;
+    bf_transform<double, double>(n, g, g, 1.0, 0.0, 1.0, 1.0, st);        // subset sums
+    std::vector<ll> bounds;
+    const int *nodes = c.layer_table(n, bounds);
+    double *dp = W.dp.as<double>();
+    set_doubles_kernel<<<1, 32, 0, st>>>(dp, 1, 0.0);
+    RUMB_LAUNCH("set_doubles");
+    for (int cc = 1; cc <= n; ++cc) {
+        ll lo = bounds[cc], ns = bounds[cc + 1] - lo;
+        if (ns <= 0) continue;
+        lpath_layer_kernel<<<grid_for(ns, 256), 256, 0, st>>>(g, dp, nodes + lo, ns, n, Nloc);
+        RUMB_LAUNCH("lpath_layer_kernel");
+    }
+    lb_final_kernel<<<1, 1, 0, st>>>(dp, N, W.res.as<double>());
+    RUMB_LAUNCH("lb_final_kernel");
+}
+
+// ================================================================= ADMM workspace
+template <class T>
+struct BmWork : public BmWorkBase {
+    DevBuf x2, s, y, z, x, Ax, t1, t2, xhat, obsbits, diag;
+    int n = 0;
+    void ensure(int n_) {
+        n = n_;
+        ll m2 = (ll)n << (n - 1);
+        size_t sb = (size_t)m2 * sizeof(T);
+        for (DevBuf *b : {&x2, &s, &y, &z, &x, &Ax, &t1, &t2, &xhat}) b->ensure(sb);
+        obsbits.ensure((size_t)((m2 + 31) / 32) * 4);
+        diag.ensure(64 * sizeof(T));
+    }
+};
+
+template <class T>
+static BmWork<T> &bm_work(Ctx &c) {
+    std::unique_ptr<BmWorkBase> &slot = sizeof(T) == 8 ? c.bm64 : c.bm32;
+    if (!slot) slot.reset(new BmWork<T>());
+    return *static_cast<BmWork<T> *>(slot.get());
+}
+
+// Per-bit eigen data of G = [[1, -1], [-1, 1 + p^2]] (ascending eigenvalues, orthonormal
+// eigenvectors as columns of Q) and the eigen-space diagonal 1/(gamma + lambda(rest)) by the
+// popcount of the rest index, lambda = ev1^pc * ev0^(nb - pc) multiplied bit by bit.
+struct Eigen {
+    double Q[2][2];
+    double ev[2];
+};
+
+static Eigen eigen2(double p) {
+    double a = 1.0, b = -1.0, d = 1.0 + p * p;
+    double mid = 0.5 * (a + d), rad = std::sqrt(0.25 * (a - d) * (a - d) + b * b);
+    Eigen E;
+    E.ev[0] = mid - rad;
+    E.ev[1] = mid + rad;
+    for (int k = 0; k < 2; ++k) {
+        double vx = b, vy = E.ev[k] - a;                     // (G - ev I) v = 0
+        double nr = std::sqrt(vx * vx + vy * vy);
+        E.Q[0][k] = vx / nr;
+        E.Q[1][k] = vy / nr;
+    }
+    return E;
+}
+
+struct BmCoef {
+    double b1, b2, ib1, ib2, alpha, p;
+    double Qt[4], Q[4];
+    std::vector<double> diag;   // by popcount, nb + 1 entries
+};
+
+static BmCoef make_coef(int n, double beta, double alpha, double p) {
+    BmCoef C;
+    C.b1 = C.b2 = beta;
+    C.ib1 = C.ib2 = 1.0 / beta;
+    C.alpha = alpha;
+    C.p = p;
+    Eigen E = eigen2(p);
+    C.Qt[0] = E.Q[0][0]; C.Qt[1] = E.Q[1][0]; C.Qt[2] = E.Q[0][1]; C.Qt[3] = E.Q[1][1];
+    C.Q[0] = E.Q[0][0]; C.Q[1] = E.Q[0][1]; C.Q[2] = E.Q[1][0]; C.Q[3] = E.Q[1][1];
+    int nb = n - 1;
+    double gamma = 1.0;                                  // beta2 / beta1
+    for (int pc = 0; pc <= nb; ++pc) {
+        double lam = 1.0;
+        for (int bit = 0; bit < nb; ++bit) lam *= (bit < pc) ? E.ev[1] : E.ev[0];
+        C.diag.push_back(1.0 / (gamma + lam));
+    }
+    return C;
+}
+
+template <class T>
+static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
+    T *x2 = W.x2.template as<T>(), *s = W.s.template as<T>(), *y = W.y.template as<T>(), *z = W.z.template as<T>();
+    T *x = W.x.template as<T>(), *Ax = W.Ax.template as<T>(), *t1 = W.t1.template as<T>(), *t2 = W.t2.template as<T>();
+    T p = (T)C.p;
+    // rhs = (z + b2 x2 - A'(y - b1 s)) / b1
+    bf_transform<T, T>(n, t1, t1, (T)1, (T)0, (T)-1, p, st, PRO_W, y, s, (T)C.b1, EPI_RHS, z, x2, (T)C.b2,
+                       (T)C.ib1);
+    // x = Q diag Q^T rhs
+    bf_transform<T, T>(n, t1, t2, (T)C.Qt[0], (T)C.Qt[1], (T)C.Qt[2], (T)C.Qt[3], st, PRO_PLAIN, nullptr, nullptr,
+                       (T)0, EPI_DIAG, nullptr, nullptr, (T)0, (T)0, W.diag.template as<T>());
+    bf_transform<T, T>(n, t2, x, (T)C.Q[0], (T)C.Q[1], (T)C.Q[2], (T)C.Q[3], st);
+    // Ax
+    bf_transform<T, T>(n, x, Ax, (T)1, (T)-1, (T)0, p, st);
+    // fused prox + z + s/y + x2
+    ProxArgs<T> P{};
+    P.n = n;
+    P.Nloc = 1LL << (n - 1);
+    P.nmenus = (1LL << n) - 1;
+    P.x = x; P.Ax = Ax; P.x2 = x2; P.z = z; P.s = s; P.y = y;
+    P.xhat = W.xhat.template as<T>();
+    P.obsbits = W.obsbits.template as<uint32_t>();
+    P.alpha = (T)C.alpha; P.b1 = (T)C.b1; P.b2 = (T)C.b2; P.ib1 = (T)C.ib1; P.ib2 = (T)C.ib2;
+    launch_prox_n<T, PROX_ITER>(P, st);
+}
+
+template <class T>
+static void enqueue_cold_start(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
+    ll m2 = (ll)n << (n - 1);
+    ProxArgs<T> P{};
+    P.n = n;
+    P.Nloc = 1LL << (n - 1);
+    P.nmenus = (1LL << n) - 1;
+    P.v = W.xhat.template as<T>();
+    P.out = W.x2.template as<T>();
+    P.xhat = W.xhat.template as<T>();
+    P.obsbits = W.obsbits.template as<uint32_t>();
+    P.b2 = (T)C.b2;
+    launch_prox_n<T, PROX_ONLY>(P, st);
+    for (DevBuf *b : {&W.s, &W.y, &W.z}) RUMB_CUDA(cudaMemsetAsync(b->ptr, 0, (size_t)m2 * sizeof(T), st));
+}
+
+// ----------------------------------------------------------------- problem upload
+struct DevProblem {
+    DevBuf menu, alt, p;
+    const uint32_t *d_menu = nullptr;
+    const int32_t *d_alt = nullptr;
+    const double *d_p = nullptr;
+};
+
+static void upload_problem(const rumb_bm_problem &pr, DevProblem &D, cudaStream_t st) {
+    if (pr.on_device) {
+        D.d_menu = pr.menu; D.d_alt = pr.alt; D.d_p = pr.p;
+        return;
+    }
+    D.menu.ensure((size_t)pr.mp * 4);
+    D.alt.ensure((size_t)pr.mp * 4);
+    D.p.ensure((size_t)pr.mp * 8);
+    RUMB_CUDA(cudaMemcpyAsync(D.menu.ptr, pr.menu, (size_t)pr.mp * 4, cudaMemcpyHostToDevice, st));
+    RUMB_CUDA(cudaMemcpyAsync(D.alt.ptr, pr.alt, (size_t)pr.mp * 4, cudaMemcpyHostToDevice, st));
+    RUMB_CUDA(cudaMemcpyAsync(D.p.ptr, pr.p, (size_t)pr.mp * 8, cudaMemcpyHostToDevice, st));
+    D.d_menu = D.menu.as<uint32_t>(); D.d_alt = D.alt.as<int32_t>(); D.d_p = D.p.as<double>();
+}
+
+// observations -> obs positions + p (cert workspace), xhat + obsbits (ADMM workspace of dtype T)
+template <class T>
+static void setup_obs(Ctx &c, CertWork &CW, BmWork<T> *W, const rumb_bm_problem &pr, const DevProblem &D,
+                      cudaStream_t st) {
+    int n = pr.n;
+    ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc;
+    DevBuf bad;
+    bad.ensure(4);
+    RUMB_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, st));
+    DevBuf tmpx, tmpb;
+    T *xhat;
+    uint32_t *bits;
+    if (W) {
+        xhat = W->xhat.template as<T>();
+        bits = W->obsbits.template as<uint32_t>();
+    } else {
+        tmpx.ensure((size_t)m2 * sizeof(T));
+        tmpb.ensure((size_t)((m2 + 31) / 32) * 4);
+        xhat = tmpx.as<T>();
+        bits = tmpb.as<uint32_t>();
+    }
+    RUMB_CUDA(cudaMemsetAsync(xhat, 0, (size_t)m2 * sizeof(T), st));
+    RUMB_CUDA(cudaMemsetAsync(bits, 0, (size_t)((m2 + 31) / 32) * 4, st));
+    obs_setup_kernel<T><<<grid_for(pr.mp, 256), 256, 0, st>>>(D.d_menu, D.d_alt, D.d_p, pr.mp, n, Nloc,
+                                                              CW.obs.as<ll>(), xhat, bits, bad.as<int>());
+    RUMB_LAUNCH("obs_setup_kernel");
+    RUMB_CUDA(cudaMemcpyAsync(CW.p.ptr, D.d_p, (size_t)pr.mp * 8, cudaMemcpyDeviceToDevice, st));
+    int hbad = 0;
+    RUMB_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    if (hbad) fail(RUMB_E_INVAL, "an observed row's alternative is not in its menu, is out of range, or its menu has "
+                                 "fewer than 2 members");
+}
+
+static void check_problem(const rumb_bm_problem *pr) {
+    if (!pr) fail(RUMB_E_INVAL, "problem is NULL");
+    if (pr->n < 2 || pr->n > 30) fail(RUMB_E_INVAL, "bm_admm handles 2 <= n <= 30");
+    if (pr->mp < 1) fail(RUMB_E_INVAL, "no observed rows");
+    if (!pr->menu || !pr->alt || !pr->p) fail(RUMB_E_INVAL, "menu, alt and p must not be NULL");
+}
+
+static void check_params(const rumb_bm_params *par) {
+    if (!par) fail(RUMB_E_INVAL, "params is NULL");
+    if (par->check < 1 || par->lb_every < 1 || par->max_iter < 1)
+        fail(RUMB_E_INVAL, "check, lb_every and max_iter must be >= 1");
+    if (!(par->beta > 0.0) || !std::isfinite(par->beta)) fail(RUMB_E_INVAL, "beta must be > 0");
+    if (!std::isfinite(par->alpha) || !std::isfinite(par->precond_p)) fail(RUMB_E_INVAL, "alpha and precond_p must be finite");
+    if (par->dtype < RUMB_F64 || par->dtype > RUMB_MIXED) fail(RUMB_E_INVAL, "dtype must be RUMB_F64, RUMB_F32 or RUMB_MIXED");
+}
+
+
+template <class T>
+static void copy_state_in(BmWork<T> &W, const rumb_bm_state &st, ll m2, cudaStream_t s) {
+    DevBuf *dst[4] = {&W.x2, &W.s, &W.y, &W.z};
+    const DevBuf *src[4] = {&st.x2, &st.s, &st.y, &st.z};
+    for (int i = 0; i < 4; ++i) {
+        if ((st.dtype == RUMB_F64) == (sizeof(T) == 8)) {
+            RUMB_CUDA(cudaMemcpyAsync(dst[i]->ptr, src[i]->ptr, (size_t)m2 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        } else if (st.dtype == RUMB_F64) {
+            convert_kernel<double, T><<<grid_for(m2, 256), 256, 0, s>>>(src[i]->as<double>(), dst[i]->as<T>(), m2);
+            RUMB_LAUNCH("convert_kernel");
+        } else {
+            convert_kernel<float, T><<<grid_for(m2, 256), 256, 0, s>>>(src[i]->as<float>(), dst[i]->as<T>(), m2);
+            RUMB_LAUNCH("convert_kernel");
+        }
+    }
+}
+
+template <class T>
+static rumb_bm_state *copy_state_out(BmWork<T> &W, int n, int device, cudaStream_t s) {
+    ll m2 = (ll)n << (n - 1);
+    rumb_bm_state *st = new rumb_bm_state();
+    st->n = n;
+    st->dtype = sizeof(T) == 8 ? RUMB_F64 : RUMB_F32;
+    st->device = device;
+    try {
+        DevBuf *dst[4] = {&st->x2, &st->s, &st->y, &st->z};
+        const DevBuf *src[4] = {&W.x2, &W.s, &W.y, &W.z};
+        for (int i = 0; i < 4; ++i) {
+            dst[i]->ensure((size_t)m2 * sizeof(T));
+            RUMB_CUDA(cudaMemcpyAsync(dst[i]->ptr, src[i]->ptr, (size_t)m2 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        }
+    } catch (...) {
+        delete st;
+        throw;
+    }
+    return st;
+}
+
+// Converts a float32 state into the float64 workspace (the mixed mode's hand-over).
+static void promote_state(BmWork<float> &F, BmWork<double> &D, ll m2, cudaStream_t s) {
+    const DevBuf *src[4] = {&F.x2, &F.s, &F.y, &F.z};
+    DevBuf *dst[4] = {&D.x2, &D.s, &D.y, &D.z};
+    for (int i = 0; i < 4; ++i) {
+        convert_kernel<float, double><<<grid_for(m2, 256), 256, 0, s>>>(src[i]->as<float>(), dst[i]->as<double>(), m2);
+        RUMB_LAUNCH("convert_kernel");
+    }
+}
+
+// ----------------------------------------------------------------- graphs
+struct Graph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~Graph() { reset(); }
+    void reset() {
+        if (e) cudaGraphExecDestroy(e);
+        if (g) cudaGraphDestroy(g);
+        e = nullptr;
+        g = nullptr;
+    }
+    template <class F>
+    void capture(cudaStream_t st, F &&fn) {
+        reset();
+        RUMB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            fn();
+        } catch (...) {
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(st, &tmp);
+            if (tmp) cudaGraphDestroy(tmp);
+            throw;
+        }
+        RUMB_CUDA(cudaStreamEndCapture(st, &g));
+        RUMB_CUDA(cudaGraphInstantiate(&e, g, 0));
+    }
+    void launch(cudaStream_t st) { RUMB_CUDA(cudaGraphLaunch(e, st)); }
+};
+
+static int graph_chunk(int check) {
+    int k = 1;
+    for (int d = 1; d <= 32 && d <= check; ++d)
+        if (check % d == 0) k = d;
+    return k;
+}
+
+using Clock = std::chrono::steady_clock;
+static double secs(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+}
+
+// One leg of the solve in dtype T: iterate + check until a stop. Returns true when the solve
+// is over (any stop), false when a mixed-mode float32 leg stalled and float64 should take over.
+struct LoopState {
+    ll it = 0, it32 = 0;
+    int checks = 0, n_lb = 0;
+    double ub = INFINITY, lb = 0.0, phi = NAN;
+    int stop = RUMB_STOP_MAX_ITER;
+    double push_s = 0.0;
+    double best_prog = -INFINITY;
+    int n_flat = 0;
+};
+
+template <class T>
+static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const rumb_bm_problem &pr,
+                    const rumb_bm_params &par, LoopState &L, Clock::time_point t0, bool stall_exit,
+                    rumb_trace_fn trace, void *user) {
+    int n = pr.n;
+    cudaStream_t st = c.own;
+    int chunk = graph_chunk(par.check);
+    Graph g_iter, g_ub, g_ublb;
+    bool graphs = par.use_graph != 0;
+    if (graphs) {
+        g_iter.capture(st, [&] { for (int i = 0; i < chunk; ++i) enqueue_iteration<T>(W, C, n, st); });
+        g_ub.capture(st, [&] {
+            enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), false, st);
+            enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+        });
+        g_ublb.capture(st, [&] {
+            enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
+            enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+        });
+    }
+    double res[R_SLOTS];
+    while (L.it < par.max_iter) {
+        if (graphs) {
+            for (int i = 0; i < par.check / chunk; ++i) g_iter.launch(st);
+        } else {
+            for (int i = 0; i < par.check; ++i) enqueue_iteration<T>(W, C, n, st);
+        }
+        L.it += par.check;
+        if (sizeof(T) == 4) L.it32 += par.check;
+        double el = secs(t0, Clock::now());
+        if (par.time_limit > 0 && el > par.time_limit) {
+            RUMB_CUDA(cudaStreamSynchronize(st));
+            L.stop = RUMB_STOP_TIME;
+            return true;
+        }
+        if (c.cancel.load()) {
+            RUMB_CUDA(cudaStreamSynchronize(st));
+            L.stop = RUMB_STOP_CANCEL;
+            return true;
+        }
+        bool want_lb = (L.checks % par.lb_every) == 0;
+        auto tp = Clock::now();
+        if (graphs) {
+            (want_lb ? g_ublb : g_ub).launch(st);
+        } else {
+            enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), want_lb, st);
+            enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+        }
+        RUMB_CUDA(cudaMemcpyAsync(res, CW.res.ptr, sizeof(res), cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        L.push_s += secs(tp, Clock::now());
+        L.checks++;
+        L.phi = std::sqrt(res[R_PHI2]);
+        L.ub = res[R_UB_BEST];
+        if (want_lb) {
+            L.n_lb++;
+            if (res[R_LB_NOW] > L.lb) L.lb = res[R_LB_NOW];
+        }
+        if (trace) trace(user, L.it, secs(t0, Clock::now()), L.phi, L.ub, L.lb);
+        if (std::isfinite(par.ub_target) && L.ub <= par.ub_target) { L.stop = RUMB_STOP_UB_TARGET; return true; }
+        if (std::isfinite(par.lb_target) && L.lb >= par.lb_target) { L.stop = RUMB_STOP_LB_TARGET; return true; }
+        double gap = L.ub - L.lb;
+        if (par.abs_tol >= 0 && gap <= par.abs_tol) { L.stop = RUMB_STOP_GAP_ABS; return true; }
+        if (par.rel_tol >= 0 && L.lb > 0 && gap / L.lb <= par.rel_tol) { L.stop = RUMB_STOP_GAP_REL; return true; }
+        if (stall_exit) {
+            // progress = -ub (falls); a float32 state stops improving at its rounding floor
+            double prog = -L.ub;
+            if (L.best_prog == -INFINITY || prog > L.best_prog * (1.0 + (L.best_prog > 0 ? 1 : -1) * par.stall_rtol)) {
+                L.best_prog = prog;
+                L.n_flat = 0;
+            } else if (++L.n_flat >= par.stall_checks) {
+                return false;
+            }
+        }
+    }
+    L.stop = RUMB_STOP_MAX_ITER;
+    return true;
+}
+
+int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_bm_state *warm,
+             rumb_bm_state **keep, rumb_bm_result *out, double *p_fit, rumb_trace_fn trace, void *user) {
+    check_problem(pr);
+    check_params(par);
+    if (!out) fail(RUMB_E_INVAL, "result is NULL");
+    auto t0 = Clock::now();
+    int n = pr->n;
+    ll m2 = (ll)n << (n - 1);
+    if (warm && (warm->n != n)) fail(RUMB_E_INVAL, "warm state was kept for another n");
+    cudaStream_t st = c.own;
+    c.cancel.store(0);
+    c.join_in();
+    cudaEvent_t e0, e1;
+    RUMB_CUDA(cudaEventCreate(&e0));
+    RUMB_CUDA(cudaEventCreate(&e1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } eg{e0, e1};
+    RUMB_CUDA(cudaEventRecord(e0, st));
+
+    CertWork &CW = cert_work(c);
+    CW.ensure(n, pr->mp);
+    DevProblem D;
+    upload_problem(*pr, D, st);
+    BmCoef C = make_coef(n, par->beta, par->alpha, par->precond_p);
+    bool use32 = par->dtype != RUMB_F64;
+    BmWork<double> *W64 = nullptr;
+    BmWork<float> *W32 = nullptr;
+    if (use32) { W32 = &bm_work<float>(c); W32->ensure(n); }
+    if (!use32 || par->dtype == RUMB_MIXED) { W64 = &bm_work<double>(c); W64->ensure(n); }
+    if (W32) setup_obs<float>(c, CW, W32, *pr, D, st);
+    if (W64) setup_obs<double>(c, CW, W64, *pr, D, st);
+    std::vector<float> d32(C.diag.begin(), C.diag.end());
+    if (W32) RUMB_CUDA(cudaMemcpyAsync(W32->diag.ptr, d32.data(), d32.size() * 4, cudaMemcpyHostToDevice, st));
+    if (W64) RUMB_CUDA(cudaMemcpyAsync(W64->diag.ptr, C.diag.data(), C.diag.size() * 8, cudaMemcpyHostToDevice, st));
+    // initial state
+    if (use32) {
+        if (warm) copy_state_in<float>(*W32, *warm, m2, st);
+        else enqueue_cold_start<float>(*W32, C, n, st);
+    } else {
+        if (warm) copy_state_in<double>(*W64, *warm, m2, st);
+        else enqueue_cold_start<double>(*W64, C, n, st);
+    }
+    set_doubles_kernel<<<1, 32, 0, st>>>(CW.res.as<double>(), R_SLOTS, 0.0);
+    RUMB_LAUNCH("set_doubles");
+    set_doubles_kernel<<<1, 32, 0, st>>>(CW.res.as<double>() + R_UB_BEST, 1, INFINITY);
+    RUMB_LAUNCH("set_doubles");
+    std::vector<ll> bounds;
+    c.layer_table(n, bounds);
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    auto t_setup = Clock::now();
+
+    LoopState L;
+    bool final_dtype64 = !use32;
+    if (use32) {
+        bool done = run_leg<float>(c, CW, *W32, C, *pr, *par, L, t0, par->dtype == RUMB_MIXED, trace, user);
+        if (!done) {
+            promote_state(*W32, *W64, m2, st);
+            final_dtype64 = true;
+            run_leg<double>(c, CW, *W64, C, *pr, *par, L, t0, false, trace, user);
+        }
+    } else {
+        run_leg<double>(c, CW, *W64, C, *pr, *par, L, t0, false, trace, user);
+    }
+    RUMB_CUDA(cudaEventRecord(e1, st));
+    if (p_fit && std::isfinite(L.ub))
+        RUMB_CUDA(cudaMemcpyAsync(p_fit, CW.pfit_best.ptr, (size_t)pr->mp * 8, cudaMemcpyDeviceToHost, st));
+    if (keep) {
+        *keep = final_dtype64 ? copy_state_out<double>(*W64, n, c.device, st)
+                              : copy_state_out<float>(*W32, n, c.device, st);
+    }
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    float dms = 0.f;
+    RUMB_CUDA(cudaEventElapsedTime(&dms, e0, e1));
+    auto t_end = Clock::now();
+    out->lb = L.lb;
+    out->ub = L.ub;
+    out->phi = L.phi;
+    out->iters = L.it;
+    out->iters_f32 = L.it32;
+    out->stop = L.stop;
+    out->n_push = L.checks;
+    out->n_lb = L.n_lb;
+    out->setup_s = secs(t0, t_setup);
+    out->solve_s = secs(t_setup, t_end);
+    out->push_s = L.push_s;
+    out->per_iter_ms = L.it > 0 ? 1e3 * out->solve_s / (double)L.it : 0.0;
+    out->device_ms = dms;
+    c.join_out();
+    return RUMB_OK;
+}
+
+int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, void *x2, void *s, void *y, void *z,
+               int iters, int cold) {
+    check_problem(pr);
+    check_params(par);
+    int n = pr->n;
+    ll m2 = (ll)n << (n - 1);
+    cudaStream_t st = c.own;
+    c.join_in();
+    CertWork &CW = cert_work(c);
+    CW.ensure(n, pr->mp);
+    DevProblem D;
+    upload_problem(*pr, D, st);
+    BmCoef C = make_coef(n, par->beta, par->alpha, par->precond_p);
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        BmWork<T> &W = bm_work<T>(c);
+        W.ensure(n);
+        setup_obs<T>(c, CW, &W, *pr, D, st);
+        std::vector<T> dg(C.diag.begin(), C.diag.end());
+        RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        size_t sb = (size_t)m2 * sizeof(T);
+        if (cold) {
+            enqueue_cold_start<T>(W, C, n, st);
+        } else {
+            RUMB_CUDA(cudaMemcpyAsync(W.x2.ptr, x2, sb, cudaMemcpyHostToDevice, st));
+            RUMB_CUDA(cudaMemcpyAsync(W.s.ptr, s, sb, cudaMemcpyHostToDevice, st));
+            RUMB_CUDA(cudaMemcpyAsync(W.y.ptr, y, sb, cudaMemcpyHostToDevice, st));
+            RUMB_CUDA(cudaMemcpyAsync(W.z.ptr, z, sb, cudaMemcpyHostToDevice, st));
+        }
+        for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
+        RUMB_CUDA(cudaMemcpyAsync(x2, W.x2.ptr, sb, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaMemcpyAsync(s, W.s.ptr, sb, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaMemcpyAsync(y, W.y.ptr, sb, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaMemcpyAsync(z, W.z.ptr, sb, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaStreamSynchronize(st));
+    };
+    if (par->dtype == RUMB_F64) run(double());
+    else run(float());
+    c.join_out();
+    return RUMB_OK;
+}
+
+// ----------------------------------------------------------------- primitives on host slabs
+struct Scratch : public BmWorkBase {
+    DevBuf a, b, c, d;
+};
+static Scratch &scratch(Ctx &c) {
+    if (!c.scratch) c.scratch.reset(new Scratch());
+    return *static_cast<Scratch *>(c.scratch.get());
+}
+
+int butterfly_host(Ctx &c, int n, int dtype, const void *in, void *out, double a, double b, double cc, double d) {
+    if (n < 2 || n > 30) fail(RUMB_E_INVAL, "butterfly: 2 <= n <= 30");
+    if (dtype != RUMB_F64 && dtype != RUMB_F32) fail(RUMB_E_INVAL, "butterfly: dtype RUMB_F64 or RUMB_F32");
+    if (!in || !out) fail(RUMB_E_INVAL, "butterfly: NULL buffer");
+    ll m2 = (ll)n << (n - 1);
+    size_t es = dtype == RUMB_F64 ? 8 : 4;
+    Scratch &S = scratch(c);
+    S.a.ensure((size_t)m2 * es);
+    cudaStream_t st = c.own;
+    c.join_in();
+    RUMB_CUDA(cudaMemcpyAsync(S.a.ptr, in, (size_t)m2 * es, cudaMemcpyHostToDevice, st));
+    if (dtype == RUMB_F64)
+        bf_transform<double, double>(n, S.a.as<double>(), S.a.as<double>(), a, b, cc, d, st);
+    else
+        bf_transform<float, float>(n, S.a.as<float>(), S.a.as<float>(), (float)a, (float)b, (float)cc, (float)d, st);
+    RUMB_CUDA(cudaMemcpyAsync(out, S.a.ptr, (size_t)m2 * es, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    c.join_out();
+    return RUMB_OK;
+}
+
+template <class T>
+static void prox_host_t(Ctx &c, int n, const T *v, const T *xhat, const T *wmask, double beta2, T *out) {
+    ll m2 = (ll)n << (n - 1);
+    ll nw = (m2 + 31) / 32;
+    std::vector<uint32_t> bits((size_t)nw, 0u);
+    for (ll i = 0; i < m2; ++i) {
+        if (wmask[i] == (T)1) bits[(size_t)(i >> 5)] |= 1u << (i & 31);
+        else if (wmask[i] != (T)0) fail(RUMB_E_INVAL, "prox: wmask entries must be 0 or 1");
+    }
+    Scratch &S = scratch(c);
+    S.a.ensure((size_t)m2 * sizeof(T));
+    S.b.ensure((size_t)m2 * sizeof(T));
+    S.c.ensure((size_t)m2 * sizeof(T));
+    S.d.ensure((size_t)nw * 4);
+    cudaStream_t st = c.own;
+    RUMB_CUDA(cudaMemcpyAsync(S.a.ptr, v, (size_t)m2 * sizeof(T), cudaMemcpyHostToDevice, st));
+    RUMB_CUDA(cudaMemcpyAsync(S.b.ptr, xhat, (size_t)m2 * sizeof(T), cudaMemcpyHostToDevice, st));
+    RUMB_CUDA(cudaMemcpyAsync(S.d.ptr, bits.data(), (size_t)nw * 4, cudaMemcpyHostToDevice, st));
+    ProxArgs<T> P{};
+    P.n = n;
+    P.Nloc = 1LL << (n - 1);
+    P.nmenus = (1LL << n) - 1;
+    P.v = S.a.as<T>();
+    P.out = S.c.as<T>();
+    P.xhat = S.b.as<T>();
+    P.obsbits = S.d.as<uint32_t>();
+    P.b2 = (T)beta2;
+    launch_prox_n<T, PROX_ONLY>(P, st);
+    RUMB_CUDA(cudaMemcpyAsync(out, S.c.ptr, (size_t)m2 * sizeof(T), cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+}
+
+int prox_host(Ctx &c, int n, int dtype, const void *v, const void *xhat, const void *wmask, double beta2, void *out) {
+    if (n < 2 || n > 30) fail(RUMB_E_INVAL, "prox: 2 <= n <= 30");
+    if (!v || !xhat || !wmask || !out) fail(RUMB_E_INVAL, "prox: NULL buffer");
+    c.join_in();
+    if (dtype == RUMB_F64)
+        prox_host_t<double>(c, n, (const double *)v, (const double *)xhat, (const double *)wmask, beta2, (double *)out);
+    else if (dtype == RUMB_F32)
+        prox_host_t<float>(c, n, (const float *)v, (const float *)xhat, (const float *)wmask, beta2, (float *)out);
+    else
+        fail(RUMB_E_INVAL, "prox: dtype RUMB_F64 or RUMB_F32");
+    c.join_out();
+    return RUMB_OK;
+}
+
+static void small_problem(rumb_bm_problem &pr, int n, ll mp, const uint32_t *menu, const int32_t *alt,
+                          const double *p) {
+    pr.n = n;
+    pr.mp = mp;
+    pr.menu = menu;
+    pr.alt = alt;
+    pr.p = p;
+    pr.on_device = 0;
+    check_problem(&pr);
+}
+
+int push_ub64_host(Ctx &c, int n, int dtype, const void *x, ll mp, const uint32_t *menu, const int32_t *alt,
+                   const double *p, double *ub, double *p_fit) {
+    rumb_bm_problem pr;
+    small_problem(pr, n, mp, menu, alt, p);
+    if (!x || !ub) fail(RUMB_E_INVAL, "push: NULL buffer");
+    if (dtype != RUMB_F64 && dtype != RUMB_F32) fail(RUMB_E_INVAL, "push: dtype RUMB_F64 or RUMB_F32");
+    ll m2 = (ll)n << (n - 1);
+    cudaStream_t st = c.own;
+    c.join_in();
+    CertWork &CW = cert_work(c);
+    CW.ensure(n, mp);
+    DevProblem D;
+    upload_problem(pr, D, st);
+    setup_obs<double>(c, CW, nullptr, pr, D, st);
+    Scratch &S = scratch(c);
+    size_t es = dtype == RUMB_F64 ? 8 : 4;
+    S.a.ensure((size_t)m2 * es);
+    RUMB_CUDA(cudaMemcpyAsync(S.a.ptr, x, (size_t)m2 * es, cudaMemcpyHostToDevice, st));
+    set_doubles_kernel<<<1, 32, 0, st>>>(CW.res.as<double>() + R_UB_BEST, 1, INFINITY);
+    RUMB_LAUNCH("set_doubles");
+    if (dtype == RUMB_F64) enqueue_push<double>(c, CW, n, S.a.as<double>(), st);
+    else enqueue_push<float>(c, CW, n, S.a.as<float>(), st);
+    double res[R_SLOTS];
+    RUMB_CUDA(cudaMemcpyAsync(res, CW.res.ptr, sizeof(res), cudaMemcpyDeviceToHost, st));
+    if (p_fit) RUMB_CUDA(cudaMemcpyAsync(p_fit, CW.pfit_cur.ptr, (size_t)mp * 8, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    *ub = res[R_UB_NOW];
+    c.join_out();
+    return RUMB_OK;
+}
+
+// LB at observed values y: runs the LB on a slab whose observed entries are y (others unread).
+int fw_lb64_host(Ctx &c, int n, ll mp, const uint32_t *menu, const int32_t *alt, const double *y, const double *p,
+                 double *lb) {
+    rumb_bm_problem pr;
+    small_problem(pr, n, mp, menu, alt, p);
+    if (!y || !lb) fail(RUMB_E_INVAL, "fw_lb: NULL buffer");
+    ll m2 = (ll)n << (n - 1);
+    cudaStream_t st = c.own;
+    c.join_in();
+    CertWork &CW = cert_work(c);
+    CW.ensure(n, mp);
+    DevProblem D;
+    upload_problem(pr, D, st);
+    // the y slab: scatter y at the observed positions through the xhat path (xhat := y)
+    rumb_bm_problem py = pr;
+    py.p = y;
+    DevProblem Dy;
+    upload_problem(py, Dy, st);
+    Scratch &S = scratch(c);
+    S.a.ensure((size_t)m2 * 8);
+    S.d.ensure((size_t)((m2 + 31) / 32) * 4);
+    // positions with xhat = y
+    {
+        DevBuf bad;
+        bad.ensure(4);
+        RUMB_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, st));
+        RUMB_CUDA(cudaMemsetAsync(S.a.ptr, 0, (size_t)m2 * 8, st));
+        RUMB_CUDA(cudaMemsetAsync(S.d.ptr, 0, (size_t)((m2 + 31) / 32) * 4, st));
+        obs_setup_kernel<double><<<grid_for(mp, 256), 256, 0, st>>>(Dy.d_menu, Dy.d_alt, Dy.d_p, mp, n, 1LL << (n - 1),
+                                                                    CW.obs.as<ll>(), S.a.as<double>(),
+                                                                    S.d.as<uint32_t>(), bad.as<int>());
+        RUMB_LAUNCH("obs_setup_kernel");
+        int hbad = 0;
+        RUMB_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        if (hbad) fail(RUMB_E_INVAL, "an observed row's alternative is not in its menu or is out of range");
+    }
+    RUMB_CUDA(cudaMemcpyAsync(CW.p.ptr, D.d_p, (size_t)mp * 8, cudaMemcpyDeviceToDevice, st));
+    enqueue_stats_lb<double>(c, CW, n, S.a.as<double>(), true, st);
+    double res[R_SLOTS];
+    RUMB_CUDA(cudaMemcpyAsync(res, CW.res.ptr, sizeof(res), cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    *lb = res[R_LB_NOW];
+    c.join_out();
+    return RUMB_OK;
+}
+
+}  // namespace rumb

@@ -1,0 +1,90 @@
+// Shared definitions of the rumb CUDA library (sm_100a): error handling, the context, the slab
+// layout helpers and small device utilities.
+//
+// Slab layout (the reference's Block-Marschak layout, solver/bm_admm/kernels.py:24-35): a slab holds
+// one value per (alternative x, menu S containing x) at x * 2^(n-1) + compress(S \ {x}, x), where
+// compress drops bit x and shifts the higher bits down. Alternative x's 2^(n-1) entries form its
+// "block"; the butterflies act on the n-1 "rest" bits of each block.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/rumb.h"
+
+namespace rumb {
+
+typedef long long ll;
+typedef unsigned long long ull;
+
+// ---------------------------------------------------------------- errors (host)
+struct Error : public std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+inline void fail(int code, const std::string &msg) { throw Error(code, msg); }
+
+inline void cuda_check(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();  // clear a sticky launch error so the context stays usable
+    int code = (e == cudaErrorMemoryAllocation) ? RUMB_E_OOM : RUMB_E_CUDA;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RUMB_CUDA(call) ::rumb::cuda_check((call), #call)
+#define RUMB_LAUNCH(what) ::rumb::cuda_check(cudaGetLastError(), what)
+
+void set_last_error(const std::string &msg);
+
+// ---------------------------------------------------------------- device buffers
+// An owning device allocation. The library allocates through the context only (cudaMalloc on
+// the context's device); buffers are reused across solves of one shape.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() {}
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    void ensure(size_t b) {
+        if (b <= bytes && ptr) return;
+        release();
+        if (b == 0) return;
+        RUMB_CUDA(cudaMalloc(&ptr, b));
+        bytes = b;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+// ---------------------------------------------------------------- lattice helpers
+__host__ __device__ __forceinline__ ull compress_bit(ull mask, int x) {
+    return (mask & ((1ULL << x) - 1ULL)) | ((mask >> (x + 1)) << x);
+}
+__host__ __device__ __forceinline__ ull expand_bit(ull rest, int x) {
+    return (rest & ((1ULL << x) - 1ULL)) | ((rest >> x) << (x + 1));
+}
+
+inline int num_sms(int dev) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+}
+
+inline unsigned grid_for(ll n, int block) {
+    ll g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    return (unsigned)g;
+}
+
+}  // namespace rumb

@@ -1,0 +1,274 @@
+"""ctypes binding of librumb.so (include/rumb.h).
+
+The library is the product path: there is no fallback. Loading fails loudly, with the reason,
+when librumb.so is missing or cannot be loaded; every call raises RumbError on a nonzero status.
+"""
+import ctypes
+import math
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "librumb.so")
+
+OK, E_INVAL, E_OOM, E_CUDA, E_TIMEOUT, E_CANCEL, E_NODEV, E_INTERNAL = range(8)
+F64, F32, MIXED = 0, 1, 2
+STOP = {1: "gap_abs", 2: "gap_rel", 3: "time_limit", 4: "max_iter", 5: "ub_target", 6: "lb_target", 7: "cancel"}
+DTYPES = {"float64": F64, "float32": F32, "mixed": MIXED}
+
+
+class RumbError(RuntimeError):
+    """A nonzero status from librumb; .code is the RUMB_E_* value."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class OutOfMemory(RumbError, MemoryError):
+    pass
+
+
+class BMProblem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("mp", ctypes.c_longlong), ("menu", ctypes.c_void_p),
+                ("alt", ctypes.c_void_p), ("p", ctypes.c_void_p), ("on_device", ctypes.c_int)]
+
+
+class BMParams(ctypes.Structure):
+    _fields_ = [("beta", ctypes.c_double), ("alpha", ctypes.c_double), ("precond_p", ctypes.c_double),
+                ("check", ctypes.c_int), ("lb_every", ctypes.c_int), ("max_iter", ctypes.c_longlong),
+                ("abs_tol", ctypes.c_double), ("rel_tol", ctypes.c_double), ("time_limit", ctypes.c_double),
+                ("ub_target", ctypes.c_double), ("lb_target", ctypes.c_double), ("dtype", ctypes.c_int),
+                ("use_graph", ctypes.c_int), ("stall_checks", ctypes.c_int), ("stall_rtol", ctypes.c_double)]
+
+
+class BMResult(ctypes.Structure):
+    _fields_ = [("lb", ctypes.c_double), ("ub", ctypes.c_double), ("phi", ctypes.c_double),
+                ("iters", ctypes.c_longlong), ("iters_f32", ctypes.c_longlong), ("stop", ctypes.c_int),
+                ("n_push", ctypes.c_int), ("n_lb", ctypes.c_int), ("setup_s", ctypes.c_double),
+                ("solve_s", ctypes.c_double), ("push_s", ctypes.c_double), ("per_iter_ms", ctypes.c_double),
+                ("device_ms", ctypes.c_double)]
+
+
+TRACE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                            ctypes.c_double, ctypes.c_double)
+
+_vp = ctypes.c_void_p
+_SIGS = {
+    "rumb_version": ([], ctypes.c_int),
+    "rumb_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+    "rumb_ctx_create": ([ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "rumb_ctx_destroy": ([_vp], ctypes.c_int),
+    "rumb_ctx_set_stream": ([_vp, _vp], ctypes.c_int),
+    "rumb_ctx_sync": ([_vp], ctypes.c_int),
+    "rumb_mem_info": ([_vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+    "rumb_cancel": ([_vp], ctypes.c_int),
+    "rumb_butterfly": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp] + [ctypes.c_double] * 4, ctypes.c_int),
+    "rumb_prox": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_double, _vp], ctypes.c_int),
+    "rumb_push_ub64": ([_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_longlong, _vp, _vp, _vp,
+                        ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
+    "rumb_fw_lb64": ([_vp, ctypes.c_int, ctypes.c_longlong, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)],
+                     ctypes.c_int),
+    "rumb_bm_solve": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, ctypes.POINTER(_vp),
+                       ctypes.POINTER(BMResult), _vp, TRACE_FN, _vp], ctypes.c_int),
+    "rumb_bm_state_destroy": ([_vp], ctypes.c_int),
+    "rumb_bm_iterate": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, _vp, _vp, _vp,
+                         ctypes.c_int, ctypes.c_int], ctypes.c_int),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """The loaded librumb.so (raises with the reason when it is missing or fails to load)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError("librumb.so is not built (%s); run rum-testing-gpu_b200/build.py" % LIB_PATH)
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (args, res) in _SIGS.items():
+                f = getattr(L, name)
+                f.argtypes = args
+                f.restype = res
+            _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(4096)
+    load().rumb_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status):
+    if status != OK:
+        msg = last_error()
+        if status == E_OOM:
+            raise OutOfMemory(status, "out of memory: " + msg)
+        raise RumbError(status, msg)
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Context:
+    """One GPU's library context (device memory, stream, graphs, cached tables)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(load().rumb_ctx_create(int(device), ctypes.byref(h)))
+        self.h = h
+        self.device = int(device)
+
+    def close(self):
+        if self.h:
+            load().rumb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        check(load().rumb_ctx_set_stream(self.h, ctypes.c_void_p(int(stream_handle) if stream_handle else 0)))
+
+    def sync(self):
+        check(load().rumb_ctx_sync(self.h))
+
+    def mem_info(self):
+        f, t = ctypes.c_size_t(), ctypes.c_size_t()
+        check(load().rumb_mem_info(self.h, ctypes.byref(f), ctypes.byref(t)))
+        return f.value, t.value
+
+    def cancel(self):
+        load().rumb_cancel(self.h)
+
+    # -------------------------------------------------------------- primitives
+    def butterfly(self, n, v, a, b, c, d):
+        v = np.ascontiguousarray(v)
+        dt = {np.dtype(np.float64): F64, np.dtype(np.float32): F32}[v.dtype]
+        if v.size != n << (n - 1):
+            raise ValueError("slab of n * 2^(n-1) values expected")
+        out = np.empty_like(v)
+        check(load().rumb_butterfly(self.h, n, dt, _p(v), _p(out), a, b, c, d))
+        return out
+
+    def prox(self, n, v, xhat, wmask, beta2):
+        v = np.ascontiguousarray(v)
+        dt = {np.dtype(np.float64): F64, np.dtype(np.float32): F32}[v.dtype]
+        xhat = np.ascontiguousarray(xhat, dtype=v.dtype)
+        wmask = np.ascontiguousarray(wmask, dtype=v.dtype)
+        out = np.empty_like(v)
+        check(load().rumb_prox(self.h, n, dt, _p(v), _p(xhat), _p(wmask), float(beta2), _p(out)))
+        return out
+
+    def push_ub64(self, n, x, menu, alt, p, want_fit=True):
+        x = np.ascontiguousarray(x)
+        dt = {np.dtype(np.float64): F64, np.dtype(np.float32): F32}[x.dtype]
+        menu = np.ascontiguousarray(menu, dtype=np.uint32)
+        alt = np.ascontiguousarray(alt, dtype=np.int32)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        ub = ctypes.c_double()
+        fit = np.empty(p.size) if want_fit else None
+        check(load().rumb_push_ub64(self.h, n, dt, _p(x), p.size, _p(menu), _p(alt), _p(p), ctypes.byref(ub),
+                                    _p(fit) if want_fit else None))
+        return ub.value, fit
+
+    def fw_lb64(self, n, menu, alt, y, p):
+        menu = np.ascontiguousarray(menu, dtype=np.uint32)
+        alt = np.ascontiguousarray(alt, dtype=np.int32)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        lb = ctypes.c_double()
+        check(load().rumb_fw_lb64(self.h, n, p.size, _p(menu), _p(alt), _p(y), _p(p), ctypes.byref(lb)))
+        return lb.value
+
+    # -------------------------------------------------------------- BM-ADMM
+    @staticmethod
+    def bm_params(beta, alpha=1.95, precond_p=math.sqrt(2.0), check=50, lb_every=1, max_iter=10 ** 7,
+                  abs_tol=1e-5, rel_tol=1e-4, time_limit=0.0, ub_target=None, lb_target=None, dtype="float64",
+                  use_graph=True, stall_checks=3, stall_rtol=1e-3):
+        P = BMParams()
+        P.beta, P.alpha, P.precond_p = float(beta), float(alpha), float(precond_p)
+        P.check, P.lb_every, P.max_iter = int(check), int(lb_every), int(max_iter)
+        P.abs_tol = -1.0 if abs_tol is None else float(abs_tol)
+        P.rel_tol = -1.0 if rel_tol is None else float(rel_tol)
+        P.time_limit = float(time_limit or 0.0)
+        P.ub_target = math.nan if ub_target is None else float(ub_target)
+        P.lb_target = math.nan if lb_target is None else float(lb_target)
+        P.dtype = DTYPES[dtype] if isinstance(dtype, str) else int(dtype)
+        P.use_graph = int(bool(use_graph))
+        P.stall_checks, P.stall_rtol = int(stall_checks), float(stall_rtol)
+        return P
+
+    @staticmethod
+    def bm_problem(n, menu, alt, p):
+        """(BMProblem, keep-alive arrays) from host rows."""
+        menu = np.ascontiguousarray(menu, dtype=np.uint32)
+        alt = np.ascontiguousarray(alt, dtype=np.int32)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        pr = BMProblem(int(n), p.size, _p(menu), _p(alt), _p(p), 0)
+        return pr, (menu, alt, p)
+
+    def bm_solve(self, problem, params, warm=None, keep=False, want_fit=True, trace=None):
+        """(result dict, p_fit or None, kept state handle or None)."""
+        pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
+        res = BMResult()
+        fit = np.empty(pr.mp) if want_fit else None
+        kept = ctypes.c_void_p()
+        rows = []
+        if trace is not None:
+            def cb(_u, it, wall, phi, ub, lb):
+                rows.append((int(it), float(wall), float(phi), float(ub), float(lb)))
+            fn = TRACE_FN(cb)
+        else:
+            fn = TRACE_FN()
+        st = load().rumb_bm_solve(self.h, ctypes.byref(pr), ctypes.byref(params), warm.h if warm else None,
+                                  ctypes.byref(kept) if keep else None, ctypes.byref(res),
+                                  _p(fit) if want_fit else None, fn, None)
+        check(st)
+        out = {f: getattr(res, f) for f, _ in BMResult._fields_}
+        out["stop_reason"] = STOP.get(res.stop, "unknown")
+        if trace is not None:
+            trace.extend(rows)
+        return out, fit, (BMState(kept) if keep and kept.value else None)
+
+    def bm_iterate(self, problem, params, state, iters, cold_start=False):
+        pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
+        dt = np.float64 if params.dtype == F64 else np.float32
+        m2 = pr.n << (pr.n - 1)
+        st = {}
+        for k in ("x2", "s", "y", "z"):
+            st[k] = np.ascontiguousarray(state[k], dtype=dt).copy() if state is not None else np.zeros(m2, dt)
+        check(load().rumb_bm_iterate(self.h, ctypes.byref(pr), ctypes.byref(params), _p(st["x2"]), _p(st["s"]),
+                                     _p(st["y"]), _p(st["z"]), int(iters), int(bool(cold_start))))
+        return st
+
+
+class BMState:
+    """A kept ADMM state on the device (freed with the object)."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def close(self):
+        if self.h:
+            load().rumb_bm_state_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
