@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark: certified BM-ADMM solves per second at n = 18 (1 % menu density), abs gap 1e-5.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--dtype float64|mixed] [--impl rumb|reference]
+
+Workload "n18_d1pct_k50": every menu of 18 alternatives with >= 2 members kept with probability
+0.01 (2,627 menus, 23,650 observed cells), p_hat from a Dirichlet(1) mixture of 50 random linear
+orders with Multinomial(500) noise per menu, seed 0 (rumb.instances). A step is one certified
+solve from the cold start: float64 upper and lower bound every 50 iterations until ub - lb <=
+1e-5 (rel_tol off), i.e. the reference's RUM.calculate_distance(method="bm_admm") bracket.
+
+value   solves/s with the instance already in HBM (device pointers), all ranks summed
+e2e     the same through the C ABI from host buffers: rows uploaded and p_fit read back per solve
+roofline, for the kernel with the largest time share in an eager profile of 20 iterations:
+        algorithmic bytes per launch / its CUDA-event launch time, against MEASURED_PEAKS.json
+cpu_baseline   the oracle (C restatement of the reference's iteration and certificate) on the host,
+        a bounded sample of iterations scaled to solves/s by this run's iteration count
+
+--impl reference times the reference's CPU path -- the oracle port, all host threads -- on the
+same workload and prints its line with "impl": "reference".
+
+Multi-GPU: a single solve does not shard (the prox couples every alternative of a menu each
+iteration), so N GPUs run N replicas of the solve (weak scaling, no collective on the data path);
+NCCL carries only the barrier and the max-over-ranks step time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rum-testing-gpu_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = "n18_d1pct_k50"
+METRIC = "n=18 BM-ADMM certified solves/s at abs gap 1e-5"
+ABS_TOL = 1e-5
+CHECK = 50
+# Iterations of the float64 certified solve of this seeded workload (the float64 library path
+# and the oracle follow the same trajectory; checked at n = 10 by tests/test_gpu_bm.py); the
+# reference arm, which runs only a sample, scales by it.
+CERT_ITERS_F64 = None
+# DRAM bytes per launch of the dominant kernel, from the ncu capture summarised under profiles/
+NCU_TRAFFIC = {}
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def instance():
+    from rumb.instances import config_instance
+    n, menu, alt, p = config_instance(WORKLOAD, seed=0)
+    return n, menu.astype(np.uint32), alt.astype(np.int32), p.astype(np.float64)
+
+
+def beta_rule(mp):
+    from rumb.params import bm_beta_default
+    return bm_beta_default(mp)
+
+
+# ------------------------------------------------------------------ CPU paths (oracle)
+def cpu_sample(n, menu, alt, p, threads, iters_per_solve, checks_per_solve, sample_iters):
+    """(solves/s, description, threads used): the oracle's iteration and float64 check, timed on a
+    bounded sample and scaled to one certified solve."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    used = O.set_threads(threads)
+    bm = O.BMOracle(n, menu, alt, p, beta=beta_rule(p.size))
+    bm.iterate(1)
+    t0 = time.perf_counter()
+    bm.iterate(sample_iters)
+    t_it = (time.perf_counter() - t0) / sample_iters
+    t0 = time.perf_counter()
+    O.push_ub64(n, bm.x2, bm.obs, bm.p)
+    O.fw_lb64(n, bm.obs, bm.x2[bm.obs], bm.p)
+    t_chk = time.perf_counter() - t0
+    per_solve = iters_per_solve * t_it + checks_per_solve * t_chk
+    desc = ("%d float64 ADMM iterations + 1 float64 check (push + lower bound) of %s on %d thread(s): "
+            "%.1f ms/iteration, %.1f ms/check, scaled to %d iterations and %d checks per certified solve"
+            % (sample_iters, WORKLOAD, used, 1e3 * t_it, 1e3 * t_chk, iters_per_solve, checks_per_solve))
+    return 1.0 / per_solve, desc, used
+
+
+def run_reference(args, rank):
+    """The reference arm: the reference's CPU path (the oracle port) with every host thread."""
+    if rank != 0:
+        return
+    n, menu, alt, p = instance()
+    iters = CERT_ITERS_F64 or 10000
+    checks = iters // CHECK
+    vals = []
+    desc, used = "", 0
+    for i in range(args.warmup + args.steps):
+        v, desc, used = cpu_sample(n, menu, alt, p, 0, iters, checks, sample_iters=10)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "cells": int(p.size), "abs_tol": ABS_TOL, "check": CHECK,
+                       "iters_per_solve": iters},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": used, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
+    ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from rumb import _lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    n, menu, alt, p = instance()
+    mp = p.size
+    beta = beta_rule(mp)
+    ctx = _lib.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    d_menu = torch.from_numpy(menu.view(np.int32)).cuda()
+    d_alt = torch.from_numpy(alt).cuda()
+    d_p = torch.from_numpy(p).cuda()
+    prob_dev = _lib.BMProblem(n, mp, d_menu.data_ptr(), d_alt.data_ptr(), d_p.data_ptr(), 1)
+    prob_host = ctx.bm_problem(n, menu, alt, p)
+    par = ctx.bm_params(beta, check=CHECK, abs_tol=ABS_TOL, rel_tol=None, dtype=args.dtype, max_iter=10 ** 7,
+                        time_limit=600)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")       # > 126 MB of L2
+
+    def solve(dev):
+        if dev:
+            r, _, _ = ctx.bm_solve((prob_dev, None), par, want_fit=False)
+        else:
+            r, _, _ = ctx.bm_solve(prob_host, par, want_fit=True)
+        return r
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(dev, k):
+        ms, res = [], None
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = solve(dev)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms, res
+
+    for _ in range(args.warmup):
+        last = solve(True)
+    barrier()
+    with ClockSampler(local) as clk:
+        ms_dev, res = timed(True, args.steps)
+        barrier()
+    clocks = clk.summary()
+    barrier()
+    ms_e2e, res_e2e = timed(False, args.steps)
+    barrier()
+    step_ms = sum(ms_dev) / len(ms_dev)
+    e2e_ms = sum(ms_e2e) / len(ms_e2e)
+    if world > 1:
+        t = torch.tensor([step_ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, e2e_ms = float(t[0]), float(t[1])
+
+    # roofline of the dominant kernel (eager profile, CUDA events per launch on the library's stream)
+    prof = ctx.bm_profile((prob_dev, None), par, iters=20)
+    launches = sum(k["launches"] for k in prof if k["name"].startswith(("bfly", "prox")))
+    top = max(prof, key=lambda k: k["total_ms"])
+    tot = sum(k["total_ms"] for k in prof)
+    per_launch_ms = top["total_ms"] / top["launches"]
+    peak, peak_kind = load_peaks()
+    achieved = top["bytes_per_launch"] / (per_launch_ms * 1e-3) / 1e9
+    iter_launches = launches / 20.0
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu:
+        v, desc, used = cpu_sample(n, menu, alt, p, 1, int(res["iters"]), int(res["n_push"]), sample_iters=40)
+        cpu = {"value": v, "unit": "solves/s", "cores": used, "kind": "port", "sample": desc}
+    value = world * 1e3 / step_ms
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"float64": "f64", "mixed": "f32+f64", "float32": "f32"}[args.dtype],
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "cells": int(mp), "menus": int(np.unique(menu).size),
+                   "abs_tol": ABS_TOL, "rel_tol": None, "check": CHECK, "beta": beta,
+                   "iters_per_solve": int(res["iters"]), "checks_per_solve": int(res["n_push"]),
+                   "ub": res["ub"], "lb": res["lb"], "state_dtype": args.dtype,
+                   "l2": "flushed (256 MB write) before every timed solve; state slabs exceed L2",
+                   "parallelism": "replicas x%d" % world},
+        "e2e": {"value": world * 1e3 / e2e_ms, "unit": "solves/s", "h2d_bytes_per_step": int(mp * 16),
+                "d2h_bytes_per_step": int(mp * 8 + 64 * res_e2e["n_push"] + 104)},
+        "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "share": top["total_ms"] / tot if tot > 0 else None,
+                     "bytes_per_launch": top["bytes_per_launch"], "launch_ms": per_launch_ms,
+                     "traffic": NCU_TRAFFIC.get(top["name"])},
+        "kernels": [{"name": k["name"], "share": round(k["total_ms"] / tot, 4),
+                     "us_per_launch": round(1e3 * k["total_ms"] / k["launches"], 2),
+                     "gbs": round(k["bytes_per_launch"] / (k["total_ms"] / k["launches"] * 1e-3) / 1e9, 1)}
+                    for k in sorted(prof, key=lambda k: -k["total_ms"])[:8]],
+        "gpu_launches": int(round(iter_launches * res["iters"] + 2 * n * res["n_push"] * 1.5)),
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

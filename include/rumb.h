@@ -22,6 +22,10 @@
  *   rumb_push_ub64           push_to_ub64 (solver/common/transforms.py:94-98)
  *   rumb_fw_lb64             fw_lb_rows_gpu (solver/common/transforms.py:101-114)
  *   rumb_mem_info            machine.gpu_free_bytes (solver/machine.py:156-159)
+ *   rumb_cg_pricer_create    StreamPricer.__init__ / the mask sweep's scaffolding
+ *                            (solver/flow_cg/pricing_stream.py:270-299, solver/flow_cg/solver.py:69-77)
+ *   rumb_cg_price            StreamPricer.price (solver/flow_cg/pricing_stream.py:407-412) and the mask
+ *                            sweep + backtrace (solver/flow_cg/solver.py:169-200)
  */
 #ifndef RUMB_H
 #define RUMB_H
@@ -67,6 +71,7 @@ extern "C" {
 
 typedef struct rumb_ctx rumb_ctx;
 typedef struct rumb_bm_state rumb_bm_state;
+typedef struct rumb_cg_pricer rumb_cg_pricer;
 
 RUMB_API int rumb_version(void);
 /* copies the calling thread's last error message (NUL-terminated, truncated to len) */
@@ -153,6 +158,44 @@ RUMB_API int rumb_bm_state_destroy(rumb_bm_state *st);
  * = 0. For iterate-level parity checks. */
 RUMB_API int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, void *x2,
                     void *s, void *y, void *z, int iters, int cold_start);
+
+/* ---------------------------------------------------------------- Flow-CG pricing */
+/* pricing storage of the lattice values */
+#define RUMB_PRICE_MASK 0 /* float32 per subset (2^n values, n <= 30) */
+#define RUMB_PRICE_F32 1  /* rank-indexed, two live layers, float32 */
+#define RUMB_PRICE_U16 2  /* rank-indexed, 16-bit mantissa per rank + float32 (offset, step) per 1024 ranks */
+#define RUMB_PRICE_U24 3  /* rank-indexed, 24-bit mantissa per rank + float32 (offset, step) per 1024 ranks */
+
+/* A pricer over the rows (menu bitmask, alternative) in x-major order: offsets[x]..offsets[x+1]
+ * are alternative x's rows (offsets has n+1 entries, offsets[n] = mp). k_pred: predecessors are
+ * kept for layers >= k_pred and the rest is solved on the sub-lattice (<= 0: n - 10).
+ * fma_decode: decode block-scaled values as fma(q, step, offset) (1) or multiply-then-add (0). */
+RUMB_API int rumb_cg_pricer_create(rumb_ctx *ctx, int n, long long mp, const uint64_t *menus,
+                                   const int64_t *offsets, int mode, int k_pred, int fma_decode,
+                                   rumb_cg_pricer **out);
+/* One pricing call on float32 row scores (host memory, or device memory of the pricer's GPU when
+ * on_device = 1): vmax = the longest path value (float64 decode of the stored top value),
+ * rank_pos[n] = the priced ranking (rank_pos[a] = position of a, 0 = best), margin = the
+ * quantization margin (0 for float32 storage), layer_step[n+1] (may be NULL) = each layer's
+ * largest quantization step. */
+RUMB_API int rumb_cg_price(rumb_cg_pricer *pricer, const float *scores, int on_device, double *vmax,
+                           int32_t *rank_pos, double *margin, float *layer_step);
+RUMB_API int rumb_cg_pricer_destroy(rumb_cg_pricer *pricer);
+
+/* ---------------------------------------------------------------- profiling */
+typedef struct {
+    char name[64];            /* kernel and launch shape */
+    long long launches;
+    double total_ms;          /* CUDA-event time summed over the launches */
+    double bytes_per_launch;  /* algorithmic bytes one launch must move */
+} rumb_kernel_stat;
+
+/* Runs `iters` ADMM iterations from the cold start (plus one float64 check when
+ * par->lb_every > 0) with an event pair around every kernel launch, and reports per kernel:
+ * launches, total time and algorithmic bytes per launch. Fills at most cap entries. This is the
+ * library's counterpart of the reference's per-phase timers (solver/flow_cg/solver.py:174-188). */
+RUMB_API int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int iters,
+                             rumb_kernel_stat *stats, int cap, int *count);
 
 #ifdef __cplusplus
 }

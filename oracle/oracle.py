@@ -69,8 +69,16 @@ def lib():
         L.ora_price_stream.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ullp, _fp,
                                        _llp, _dp, _ip, _dp, _fp]
         L.ora_ranking_column.argtypes = [ctypes.c_int, ctypes.c_longlong, _ullp, _ip, _ip, _u8p]
+        L.ora_set_threads.argtypes = [ctypes.c_int]
+        L.ora_get_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
+
+
+def set_threads(t):
+    """Threads of the oracle's parallel loops (0 = every core); results do not depend on it."""
+    lib().ora_set_threads(int(t))
+    return lib().ora_get_threads()
 
 
 def _ptr(a, t):

@@ -21,9 +21,30 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 typedef long long ll;
 typedef unsigned long long ull;
+
+/* thread count of the parallel loops (every loop writes disjoint outputs, so results do not
+ * depend on it) */
+void ora_set_threads(int t) {
+#ifdef _OPENMP
+    omp_set_num_threads(t > 0 ? t : omp_get_num_procs());
+#else
+    (void)t;
+#endif
+}
+
+int ora_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
 
 /* ------------------------------------------------------------------ slab layout */
 
@@ -59,6 +80,7 @@ void ora_slab_index(int n, ll mp, const ull *menu, const ll *alt, ll *idx) {
         T *blk = v + (ll)x * Nloc;                                                          \
         for (int j = 0; j < n - 1; ++j) {                                                   \
             ll h = 1LL << j;                                                                \
+            _Pragma("omp parallel for schedule(static) if (Nloc >= 4096)")                  \
             for (ll base = 0; base < Nloc; base += 2 * h)                                   \
                 for (ll i = base; i < base + h; ++i) {                                      \
                     T X = blk[i], Y = blk[i + h];                                           \
@@ -78,8 +100,9 @@ void ora_bfly_f32(int n, float *v, float a, float b, float c, float d) { BFLY_BO
 #define PROX_BODY(T)                                                                        \
     ll Nloc = 1LL << (n - 1);                                                               \
     ull full = (1ULL << n);                                                                 \
-    T vals[64]; ll pos_arr[64]; double srt[64];                                              \
+    _Pragma("omp parallel for schedule(dynamic, 1024) if (full >= 4096)")                  \
     for (ull S = 1; S < full; ++S) {                                                        \
+        T vals[64]; ll pos_arr[64]; double srt[64];                                         \
         int k = __builtin_popcountll(S);                                                    \
         ull SS = S; int kk = 0; T w0 = (T)0; int mixed = 0; int single = 0;                 \
         while (SS) {                                                                        \
@@ -152,22 +175,28 @@ void ora_prox_f32(int n, const float *in, float *out, const float *xhat, const f
     T *Ax = scratch + 4 * m2, *x2n = scratch + 5 * m2, *xk = w;                             \
     T one = (T)1;                                                                           \
     for (int it = 0; it < iters; ++it) {                                                    \
+        _Pragma("omp parallel for schedule(static)")                                        \
         for (ll i = 0; i < m2; ++i) w[i] = y[i] - b1 * s[i];                                \
         memcpy(AT, w, (size_t)m2 * sizeof(T));                                              \
         BF(n, AT, (T)1, (T)0, (T)-1, p);                                                    \
+        _Pragma("omp parallel for schedule(static)")                                        \
         for (ll i = 0; i < m2; ++i) rhs[i] = (z[i] + b2 * x2[i] - AT[i]) * ib1;             \
         memcpy(x, rhs, (size_t)m2 * sizeof(T));                                             \
         BF(n, x, (T)co[0], (T)co[1], (T)co[2], (T)co[3]);                                   \
+        _Pragma("omp parallel for schedule(static)")                                        \
         for (ll i = 0; i < m2; ++i) x[i] *= inv_gl[i % Nloc];                               \
         BF(n, x, (T)co[4], (T)co[5], (T)co[6], (T)co[7]);                                   \
         memcpy(Ax, x, (size_t)m2 * sizeof(T));                                              \
         BF(n, Ax, (T)1, (T)-1, (T)0, p);                                                    \
+        _Pragma("omp parallel for schedule(static)")                                        \
         for (ll i = 0; i < m2; ++i) xk[i] = alpha * x[i] + (one - alpha) * x2[i] - ib2 * z[i]; \
         PX(n, xk, x2n, xhat, wmask, b2);                                                    \
+        _Pragma("omp parallel for schedule(static)")                                        \
         for (ll i = 0; i < m2; ++i) {                                                       \
             T xo = alpha * x[i] + (one - alpha) * x2[i];                                    \
             z[i] -= b2 * (xo - x2n[i]);                                                     \
         }                                                                                   \
+        _Pragma("omp parallel for schedule(static)")                                        \
         for (ll i = 0; i < m2; ++i) {                                                       \
             T axor = -alpha * Ax[i] - (one - alpha) * s[i];                                 \
             T sn = ib1 * y[i] - axor; sn = sn > (T)0 ? sn : (T)0;                           \
@@ -212,7 +241,9 @@ void ora_make_feasible64(int n, const double *q, double *rf, double eps) {
     double *mass = (double *)calloc((size_t)N, sizeof(double));
     ll *order = (ll *)malloc((size_t)N * sizeof(ll));
     ll *bounds = (ll *)malloc(((size_t)n + 2) * sizeof(ll));
+    #pragma omp parallel for schedule(static)
     for (ll i = 0; i < m2; ++i) w[i] = (q[i] > 0.0 ? q[i] : 0.0) + eps;
+    #pragma omp parallel for schedule(static)
     for (ll D = 0; D < N; ++D) {
         double sum = 0.0;
         for (int x = 0; x < n; ++x) {
@@ -223,7 +254,8 @@ void ora_make_feasible64(int n, const double *q, double *rf, double eps) {
     }
     ora_layers(n, order, bounds);
     mass[0] = 1.0;
-    for (int c = 1; c <= n; ++c)
+    for (int c = 1; c <= n; ++c) {
+        #pragma omp parallel for schedule(static)
         for (ll i = bounds[c]; i < bounds[c + 1]; ++i) {
             ll C = order[i];
             double sum = 0.0;
@@ -237,6 +269,8 @@ void ora_make_feasible64(int n, const double *q, double *rf, double eps) {
             }
             mass[C] = sum;
         }
+    }
+    #pragma omp parallel for schedule(static)
     for (ll a = 0; a < m2; ++a) {
         ll x = a / Nloc, rest = a - x * Nloc;
         ll T = (ll)expand_bit((ull)rest, (int)x);
@@ -255,7 +289,8 @@ double ora_longest_path64(int n, const double *R) {
     ll *bounds = (ll *)malloc(((size_t)n + 2) * sizeof(ll));
     ora_layers(n, order, bounds);
     dp[0] = 0.0;
-    for (int c = 1; c <= n; ++c)
+    for (int c = 1; c <= n; ++c) {
+        #pragma omp parallel for schedule(static)
         for (ll i = bounds[c]; i < bounds[c + 1]; ++i) {
             ll C = order[i];
             double best = -1e300;
@@ -269,6 +304,7 @@ double ora_longest_path64(int n, const double *R) {
             }
             dp[C] = best;
         }
+    }
     double out = dp[N - 1];
     free(dp); free(order); free(bounds);
     return out;

@@ -7,6 +7,7 @@
 
 #include "bm.cuh"
 #include "ctx.cuh"
+#include "pricer.cuh"
 
 namespace rumb {
 static thread_local std::string g_last_error;
@@ -186,6 +187,59 @@ int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_pa
     if (!x2 || !s || !y || !z) rumb::fail(RUMB_E_INVAL, "state buffers must not be NULL");
     if (iters < 0) rumb::fail(RUMB_E_INVAL, "iters must be >= 0");
     return rumb::bm_iterate(ctx->c, prob, par, x2, s, y, z, iters, cold_start);
+    RUMB_API_END
+}
+
+int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int iters,
+                    rumb_kernel_stat *stats, int cap, int *count) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    if (iters < 1) rumb::fail(RUMB_E_INVAL, "iters must be >= 1");
+    return rumb::bm_profile(ctx->c, prob, par, iters, stats, cap, count);
+    RUMB_API_END
+}
+
+int rumb_cg_pricer_create(rumb_ctx *ctx, int n, long long mp, const uint64_t *menus, const int64_t *offsets,
+                          int mode, int k_pred, int fma_decode, rumb_cg_pricer **out) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    if (!out) rumb::fail(RUMB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    ctx->c.join_in();
+    rumb_cg_pricer *h = new rumb_cg_pricer();
+    try {
+        h->p = rumb::pricer_create(ctx->c, n, mp, menus, offsets, mode, k_pred, fma_decode);
+    } catch (...) {
+        delete h;
+        throw;
+    }
+    h->device = ctx->c.device;
+    ctx->c.join_out();
+    *out = h;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_price(rumb_cg_pricer *pr, const float *scores, int on_device, double *vmax, int32_t *rank_pos,
+                  double *margin, float *layer_step) {
+    RUMB_API_BEGIN
+    if (!pr || !pr->p) rumb::fail(RUMB_E_INVAL, "pricer is NULL");
+    if (!scores || !vmax || !rank_pos || !margin) rumb::fail(RUMB_E_INVAL, "NULL output");
+    rumb::DeviceGuard dg(pr->device);
+    rumb::pricer_price(pr->p, scores, on_device, vmax, rank_pos, margin, layer_step);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_pricer_destroy(rumb_cg_pricer *pr) {
+    RUMB_API_BEGIN
+    if (!pr) return RUMB_OK;
+    {
+        rumb::DeviceGuard dg(pr->device);
+        rumb::pricer_destroy(pr->p);
+    }
+    delete pr;
+    return RUMB_OK;
     RUMB_API_END
 }
 

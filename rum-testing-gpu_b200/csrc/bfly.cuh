@@ -17,6 +17,8 @@
 // accesses are conflict-free. Prologue / epilogue functors fuse the elementwise ADMM steps into
 // the first load and the last store of a transform.
 #pragma once
+#include <cstdio>
+
 #include "common.cuh"
 
 namespace rumb {
@@ -211,8 +213,18 @@ inline void bf_launch_pass(const BfArgs<T, TI> &A, int n, cudaStream_t st) {
     }
     ll tiles = A.Nloc >> (A.s == 0 ? A.B : A.B + 5);
     size_t smem = (size_t)sizeof(T) << (A.s == 0 ? A.B : A.B + 5);
+    if (g_prof) {
+        double S = (double)A.Nloc * n;
+        double bytes = S * (sizeof(TI) + sizeof(T));
+        if (A.pro == PRO_W) bytes += S * sizeof(T);              // two inputs instead of one
+        if (A.epi == EPI_RHS) bytes += 2.0 * S * sizeof(T);
+        char nm[64];
+        snprintf(nm, sizeof nm, "bfly_pass<%s>[s=%d,B=%d]", sizeof(T) == 8 ? "f64" : "f32", A.s, A.B);
+        prof_begin(nm, bytes, st);
+    }
     bfly_pass<T, TI><<<(unsigned)(tiles * n), BF_THREADS, smem, st>>>(A);
     RUMB_LAUNCH("bfly_pass");
+    prof_end(st);
 }
 
 // Full transform in -> out. pro applies to the first pass's load, epi to the last pass's store;

@@ -169,10 +169,17 @@ static void launch_prox_n(const ProxArgs<T> &P, cudaStream_t st) {
     const int TB = 128;
     unsigned grid = grid_for(P.nmenus, TB);
     int n = P.n;
+    if (g_prof) {
+        double S = (double)P.Nloc * n, e = sizeof(T);
+        double bytes = (MODE == PROX_ITER ? 10.0 : 2.0) * S * e + S / 8.0;
+        prof_begin(MODE == PROX_ITER ? (e == 8 ? "prox_fused<f64>" : "prox_fused<f32>")
+                                     : (e == 8 ? "prox_only<f64>" : "prox_only<f32>"), bytes, st);
+    }
 #define RUMB_PROX_CASE(NN)                                          \
     if (n <= NN) {                                                  \
         prox_kernel<T, NN, MODE><<<grid, TB, 0, st>>>(P);           \
         RUMB_LAUNCH("prox_kernel");                                 \
+        prof_end(st);                                               \
         return;                                                     \
     }
     RUMB_PROX_CASE(8)
@@ -952,6 +959,79 @@ int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, voi
     };
     if (par->dtype == RUMB_F64) run(double());
     else run(float());
+    c.join_out();
+    return RUMB_OK;
+}
+
+thread_local Prof *g_prof = nullptr;
+
+// Runs `iters` iterations eagerly from the cold start with an event pair around every launch;
+// returns per-kernel-name launches, total milliseconds and algorithmic bytes per launch.
+int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int iters, rumb_kernel_stat *stats,
+               int cap, int *count) {
+    check_problem(pr);
+    check_params(par);
+    if (!stats || !count || cap < 1) fail(RUMB_E_INVAL, "profile: stats buffer");
+    int n = pr->n;
+    cudaStream_t st = c.own;
+    c.join_in();
+    CertWork &CW = cert_work(c);
+    CW.ensure(n, pr->mp);
+    DevProblem D;
+    upload_problem(*pr, D, st);
+    BmCoef C = make_coef(n, par->beta, par->alpha, par->precond_p);
+    Prof prof;
+    prof.st = st;
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        BmWork<T> &W = bm_work<T>(c);
+        W.ensure(n);
+        setup_obs<T>(c, CW, &W, *pr, D, st);
+        std::vector<T> dg(C.diag.begin(), C.diag.end());
+        RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        enqueue_cold_start<T>(W, C, n, st);
+        for (int i = 0; i < 3; ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        g_prof = &prof;
+        try {
+            for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
+            if (par->lb_every > 0) {
+                enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
+                enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+            }
+        } catch (...) {
+            g_prof = nullptr;
+            throw;
+        }
+        g_prof = nullptr;
+        RUMB_CUDA(cudaStreamSynchronize(st));
+    };
+    if (par->dtype == RUMB_F64) run(double());
+    else run(float());
+    std::vector<std::string> names;
+    std::map<std::string, rumb_kernel_stat> agg;
+    for (auto &r : prof.recs) {
+        float ms = 0.f;
+        if (r.b) cudaEventElapsedTime(&ms, r.a, r.b);
+        cudaEventDestroy(r.a);
+        if (r.b) cudaEventDestroy(r.b);
+        auto it = agg.find(r.name);
+        if (it == agg.end()) {
+            rumb_kernel_stat k{};
+            snprintf(k.name, sizeof k.name, "%s", r.name.c_str());
+            k.bytes_per_launch = r.bytes;
+            it = agg.emplace(r.name, k).first;
+            names.push_back(r.name);
+        }
+        it->second.launches += 1;
+        it->second.total_ms += ms;
+    }
+    int k = 0;
+    for (auto &nm : names) {
+        if (k >= cap) break;
+        stats[k++] = agg[nm];
+    }
+    *count = k;
     c.join_out();
     return RUMB_OK;
 }

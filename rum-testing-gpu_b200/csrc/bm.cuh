@@ -13,4 +13,6 @@ int push_ub64_host(Ctx &c, int n, int dtype, const void *x, ll mp, const uint32_
                    const double *p, double *ub, double *p_fit);
 int fw_lb64_host(Ctx &c, int n, ll mp, const uint32_t *menu, const int32_t *alt, const double *y, const double *p,
                  double *lb);
+int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int iters, rumb_kernel_stat *stats,
+               int cap, int *count);
 }  // namespace rumb

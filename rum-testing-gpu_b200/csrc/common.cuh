@@ -81,6 +81,34 @@ inline int num_sms(int dev) {
     return v > 0 ? v : 148;
 }
 
+// ---------------------------------------------------------------- launch profiler
+// When a profiler is installed on the calling thread (rumb_bm_profile), every kernel launch site
+// brackets its launch with CUDA events and reports its algorithmic bytes; otherwise these are
+// no-ops.
+struct ProfRec {
+    std::string name;
+    cudaEvent_t a, b;
+    double bytes;
+};
+struct Prof {
+    cudaStream_t st = nullptr;
+    std::vector<ProfRec> recs;
+};
+extern thread_local Prof *g_prof;
+
+inline void prof_begin(const std::string &name, double bytes, cudaStream_t st) {
+    if (!g_prof || st != g_prof->st) return;
+    ProfRec r{name, nullptr, nullptr, bytes};
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, st);
+    g_prof->recs.push_back(r);
+}
+inline void prof_end(cudaStream_t st) {
+    if (!g_prof || st != g_prof->st || g_prof->recs.empty()) return;
+    cudaEventRecord(g_prof->recs.back().b, st);
+}
+
 inline unsigned grid_for(ll n, int block) {
     ll g = (n + block - 1) / block;
     if (g < 1) g = 1;

@@ -1,0 +1,473 @@
+// Flow-CG pricing on the GPU (sm_100a): the Bellman-Ford longest path over the subset lattice,
+//     V[D] = max over x in D of V[D \ {x}] + w(x, D),  w(x, D) = sum of the scores of x's rows whose
+//     menu is a subset of D (a sequential float32 sum in row order),
+// and the ranking it picks, bit for bit as the reference computes them.
+//
+// Reference behaviour (mingxiz/rum-testing-gpu):
+//   stream sweep   solver/flow_cg/pricing_stream.py:61-182 (BODY, f32/u16/u24 storage), :302-345
+//   backtrace      solver/flow_cg/pricing_stream.py:348-405 (pred layers, sub-lattice mask DP)
+//   mask sweep     solver/flow_cg/bf_pricing.py:8-47, solver/flow_cg/solver.py:169-200
+//
+// What must match exactly, and how it is kept:
+//   * w(x, D) adds x's rows in their x-major order, one float32 add at a time.
+//   * stream: candidates over x descending with `>=` (ties -> lowest x); mask: x ascending with
+//     `>` (ties -> lowest x). Both are computed here as one warp-uniform loop over x so that all
+//     lanes read the same row at the same time (a broadcast), with the lane's own predicate.
+//   * quantization blocks are 1024 consecutive ranks: one CTA of 1024 threads per block, block
+//     min / max (exact, order-free), step = (max - min) / levels and q = rintf((v - min) / step)
+//     with IEEE division; the previous layer is decoded as fma(q, step, min) (fma_decode = 1,
+//     the contraction the reference's JIT compiler applies to m + q * e) or as a rounded multiply
+//     then add (fma_decode = 0).
+//   * the sub-lattice DP after the descent uses the original menus and row order restricted to
+//     the node reached, which is what the reference's relabelled sub-problem adds up.
+#include <cstring>
+
+#include "ctx.cuh"
+#include "pricer.cuh"
+
+namespace rumb {
+
+constexpr int PB = 1024;       // ranks per quantization block = threads per CTA
+constexpr int MAXN_PR = 40;
+
+struct PricerArgs {
+    int n, k;
+    ull count;                 // ranks in this layer
+    const ull *binom;          // C(b, t) at b*(n+1)+t
+    const ull *menus;          // x-major rows
+    const float *scores;
+    const ll *offsets;         // n+1
+    int mode;                  // 1 f32, 2 u16, 3 u24
+    int fma_decode;
+    // previous layer
+    const float *vprev_f;
+    const uint16_t *vprev_h;
+    const uint8_t *lprev;
+    const float *mprev, *eprev;
+    // current layer
+    float *vcur_f;
+    uint16_t *vcur_h;
+    uint8_t *lcur;
+    float *mcur, *ecur;
+    uint8_t *pred;             // nullptr when this layer keeps no predecessors
+    unsigned int *layer_step;  // float bits, atomicMax (steps are >= 0)
+};
+
+__device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
+    if (A.mode == 1) return A.vprev_f[rp];
+    unsigned int q = A.vprev_h[rp];
+    if (A.mode == 3) q = (q << 8) | (unsigned int)A.lprev[rp];
+    float qf = (float)q, m = A.mprev[rp / PB], e = A.eprev[rp / PB];
+    if (A.fma_decode) return __fmaf_rn(qf, e, m);
+    return __fadd_rn(m, __fmul_rn(qf, e));
+}
+
+__global__ void __launch_bounds__(PB) stream_layer_kernel(PricerArgs A) {
+    __shared__ float smin[PB / 32], smax[PB / 32];
+    const int n = A.n, k = A.k;
+    const ull r = (ull)blockIdx.x * PB + threadIdx.x;
+    const bool valid = r < A.count;
+    // colex unranking of r into D (elements ascending)
+    ull D = 0;
+    if (valid) {
+        ull rr = r;
+        int b = n - 1;
+        for (int t = k; t >= 1; --t) {
+            while (A.binom[b * (n + 1) + t] > rr) --b;
+            D |= 1ULL << b;
+            rr -= A.binom[b * (n + 1) + t];
+            --b;
+        }
+    }
+    float best = 0.0f;
+    int bestx = 0;
+    bool seen = false;
+    ull suf = 0, remain = r;
+    int t = k;                                      // elements of D at or above x still to visit
+    for (int x = n - 1; x >= 0; --x) {
+        bool in = valid && ((D >> x) & 1ULL);
+        // sequential float32 sum of x's rows with menu subset of D (warp-uniform row loop)
+        float w = 0.0f;
+        const ll lo = A.offsets[x], hi = A.offsets[x + 1];
+        if (__any_sync(0xffffffffu, in)) {
+            for (ll i = lo; i < hi; ++i) {
+                ull Dp = __ldg(A.menus + i);
+                float sc = __ldg(A.scores + i);
+                if (in && (Dp & D) == Dp) w = __fadd_rn(w, sc);
+            }
+        }
+        if (in) {
+            --t;                                    // x is element t of D (0-based, ascending)
+            remain -= A.binom[x * (n + 1) + (t + 1)];
+            ull rp = remain + suf;
+            suf += A.binom[x * (n + 1) + t];
+            float vp = decode_prev(A, rp);
+            float cand = __fadd_rn(vp, w);
+            if (!seen || cand >= best) { best = cand; seen = true; bestx = x; }
+        }
+    }
+    if (valid && A.pred) A.pred[r] = (uint8_t)bestx;
+    if (A.mode == 1) {
+        if (valid) A.vcur_f[r] = best;
+        return;
+    }
+    // block min / max over the valid ranks
+    float tmin = valid ? best : 3.0e38f, tmax = valid ? best : -3.0e38f;
+    for (int o = 16; o > 0; o >>= 1) {
+        tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+        tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) { smin[threadIdx.x >> 5] = tmin; smax[threadIdx.x >> 5] = tmax; }
+    __syncthreads();
+    float bmin = smin[0], bmax = smax[0];
+    for (int i = 1; i < PB / 32; ++i) { bmin = fminf(bmin, smin[i]); bmax = fmaxf(bmax, smax[i]); }
+    const float levels = A.mode == 2 ? 65535.0f : 16777215.0f;
+    float step = __fdiv_rn(__fsub_rn(bmax, bmin), levels);
+    if (threadIdx.x == 0) {
+        A.mcur[blockIdx.x] = bmin;
+        A.ecur[blockIdx.x] = step;
+        atomicMax(A.layer_step, __float_as_uint(step));
+    }
+    if (!valid) return;
+    float q = (step > 0.0f) ? rintf(__fdiv_rn(__fsub_rn(best, bmin), step)) : 0.0f;
+    q = fminf(fmaxf(q, 0.0f), levels);
+    unsigned int qi = (unsigned int)q;
+    if (A.mode == 2) {
+        A.vcur_h[r] = (uint16_t)qi;
+    } else {
+        A.vcur_h[r] = (uint16_t)(qi >> 8);
+        A.lcur[r] = (uint8_t)(qi & 255u);
+    }
+}
+
+// Mask-indexed layer: thread per node of layer c (node ids from the popcount-ordered table).
+__global__ void mask_layer_kernel(const int *nodes, ll ns, const ull *menus, const float *scores, const ll *offsets,
+                                  int n, float *V, uint8_t *pred) {
+    ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    bool valid = i < ns;
+    ull D = valid ? (ull)(unsigned)nodes[i] : 0ULL;
+    float best = 0.0f;
+    bool seen = false;
+    int bx = 0;
+    for (int x = 0; x < n; ++x) {
+        bool in = valid && ((D >> x) & 1ULL);
+        float w = 0.0f;
+        if (__any_sync(0xffffffffu, in)) {
+            for (ll j = offsets[x]; j < offsets[x + 1]; ++j) {
+                ull Dp = __ldg(menus + j);
+                float sc = __ldg(scores + j);
+                if (in && (Dp & D) == Dp) w = __fadd_rn(w, sc);
+            }
+        }
+        if (in) {
+            float cand = __fadd_rn(V[D ^ (1ULL << x)], w);
+            if (!seen || cand > best) { best = cand; seen = true; bx = x; }
+        }
+    }
+    if (valid) {
+        V[D] = best;
+        pred[D] = (uint8_t)bx;
+    }
+}
+
+__device__ ull colex_rank_dev(ull mask, const ull *binom, int n) {
+    ull r = 0;
+    int t = 0;
+    for (int b = 0; b < n; ++b)
+        if ((mask >> b) & 1ULL) {
+            ++t;
+            r += binom[b * (n + 1) + t];
+        }
+    return r;
+}
+
+// Result block written by the device backtrace (one small D2H copy per price call).
+struct PriceOut {
+    float vtop;            // f32 value at the full set (f32 / mask modes)
+    float mtop, etop;      // u16 / u24: offset and step of the top block
+    unsigned int qtop;     // u16 / u24: quantized top value
+    int rank_pos[MAXN_PR];
+    int error;
+};
+
+// Descent through the stored predecessor layers (stream modes), then the mask DP on the
+// sub-lattice of the node reached; one CTA. V/pred scratch: 2^K entries (K = k_pred).
+__global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *const *preds, const ull *menus,
+                                 const float *scores, const ll *offsets, float *Vs, uint8_t *Ps, PriceOut *out,
+                                 const float *vtop_f, const uint16_t *vtop_h, const uint8_t *ltop, const float *mtop,
+                                 const float *etop, int mode) {
+    __shared__ ull sD;
+    __shared__ int elems[MAXN_PR];
+    __shared__ int spos;
+    if (threadIdx.x == 0) {
+        ull D = (n >= 64) ? ~0ULL : ((1ULL << n) - 1ULL);
+        int pos = 0;
+        for (int k = n; k > k_pred; --k) {
+            ull r = colex_rank_dev(D, binom, n);
+            int x = preds[k][r];
+            out->rank_pos[x] = pos++;
+            D ^= 1ULL << x;
+        }
+        int K = 0;
+        for (int b = 0; b < n; ++b)
+            if ((D >> b) & 1ULL) elems[K++] = b;
+        sD = D;
+        spos = pos;
+        if (mode == 1) out->vtop = vtop_f[0];
+        else if (mode >= 2) {
+            unsigned int q = vtop_h[0];
+            if (mode == 3) q = (q << 8) | ltop[0];
+            out->qtop = q;
+            out->mtop = mtop[0];
+            out->etop = etop[0];
+        }
+    }
+    __syncthreads();
+    const ull D = sD;
+    const int K = __popcll(D);
+    const ull Nsub = 1ULL << K;
+    for (ull s = threadIdx.x; s < Nsub; s += blockDim.x) { Vs[s] = 0.0f; Ps[s] = 0; }
+    __syncthreads();
+    for (int c = 1; c <= K; ++c) {
+        for (ull s = threadIdx.x; s < Nsub; s += blockDim.x) {
+            if (__popcll(s) != c) continue;
+            ull Dorig = 0;
+            for (int j = 0; j < K; ++j)
+                if ((s >> j) & 1ULL) Dorig |= 1ULL << elems[j];
+            float best = 0.0f;
+            bool seen = false;
+            int bj = 0;
+            for (int j = 0; j < K; ++j) {
+                if (!((s >> j) & 1ULL)) continue;
+                int x = elems[j];
+                float w = 0.0f;
+                for (ll i = offsets[x]; i < offsets[x + 1]; ++i) {
+                    ull Dp = menus[i];
+                    if ((Dp & Dorig) == Dp) w = __fadd_rn(w, scores[i]);
+                }
+                float cand = __fadd_rn(Vs[s ^ (1ULL << j)], w);
+                if (!seen || cand > best) { best = cand; seen = true; bj = j; }
+            }
+            Vs[s] = best;
+            Ps[s] = (uint8_t)bj;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ull Dm = Nsub - 1;
+        int pos = spos;
+        for (int i = 0; i < K; ++i) {
+            int j = Ps[Dm];
+            out->rank_pos[elems[j]] = pos + i;
+            Dm ^= 1ULL << j;
+        }
+        if (mode == 0) out->vtop = Vs[Nsub - 1];
+        out->error = 0;
+    }
+}
+
+// Mask mode: the whole lattice is solved; descend pred from the full set.
+__global__ void mask_readout_kernel(int n, const float *V, const uint8_t *pred, PriceOut *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ull D = (1ULL << n) - 1ULL;
+    out->vtop = V[D];
+    for (int i = 0; i < n; ++i) {
+        int x = pred[D];
+        out->rank_pos[x] = i;
+        D ^= 1ULL << x;
+    }
+    out->error = 0;
+}
+
+// ----------------------------------------------------------------- host object
+struct Pricer {
+    Ctx *c = nullptr;
+    int n = 0, mode = 0, k_pred = 0, fma_decode = 1;
+    ll mp = 0;
+    std::vector<ull> counts;
+    DevBuf menus, scores, offsets, binom;
+    DevBuf v[2], l[2], m[2], e[2];          // stream layers
+    std::vector<std::unique_ptr<DevBuf>> pred;   // per layer >= k_pred
+    DevBuf pred_ptrs;                       // device array of pred pointers (n+1)
+    DevBuf layer_step;                      // n+1 uints (float bits)
+    DevBuf Vs, Ps;                          // sub-lattice / mask scratch
+    DevBuf out;                             // PriceOut
+    std::vector<ll> host_offsets;
+};
+
+static std::vector<ull> binom_host(int n) {
+    std::vector<ull> t((size_t)(n + 1) * (n + 1), 0);
+    for (int b = 0; b <= n; ++b) {
+        t[b * (n + 1)] = 1;
+        for (int k = 1; k <= b; ++k)
+            t[b * (n + 1) + k] = t[(b - 1) * (n + 1) + k - 1] + (k <= b - 1 ? t[(b - 1) * (n + 1) + k] : 0);
+    }
+    return t;
+}
+
+Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t *offsets, int mode, int k_pred,
+                      int fma_decode) {
+    if (mode < 0 || mode > 3) fail(RUMB_E_INVAL, "pricer mode must be 0 (mask), 1 (f32), 2 (u16) or 3 (u24)");
+    if (n < 1 || n > 39) fail(RUMB_E_INVAL, "pricing handles 1 <= n <= 39");
+    if (mode == 0 && n > 30) fail(RUMB_E_INVAL, "mask pricing handles n <= 30");
+    if (mp < 0 || (mp > 0 && !menus) || !offsets) fail(RUMB_E_INVAL, "menus / offsets must not be NULL");
+    std::vector<ll> off(offsets, offsets + n + 1);
+    if (off[0] != 0 || off[n] != mp) fail(RUMB_E_INVAL, "offsets must run from 0 to mp");
+    for (int x = 0; x < n; ++x) {
+        if (off[x + 1] < off[x]) fail(RUMB_E_INVAL, "offsets must be nondecreasing");
+        for (ll i = off[x]; i < off[x + 1]; ++i)
+            if (!((menus[i] >> x) & 1ULL) || (n < 64 && (menus[i] >> n) != 0))
+                fail(RUMB_E_INVAL, "row's menu does not contain its alternative or exceeds n");
+    }
+    std::unique_ptr<Pricer> P(new Pricer());
+    P->c = &c;
+    P->n = n;
+    P->mp = mp;
+    P->mode = mode;
+    P->fma_decode = fma_decode ? 1 : 0;
+    int kp = k_pred > 0 ? k_pred : n - 10;
+    P->k_pred = kp < 1 ? 1 : (kp > n ? n : kp);
+    if (mode != 0 && P->k_pred > 22) fail(RUMB_E_INVAL, "k_pred > 22 needs a sub-lattice larger than this pricer keeps");
+    P->host_offsets = off;
+    std::vector<ull> bt = binom_host(n);
+    for (int k = 0; k <= n; ++k) P->counts.push_back(bt[n * (n + 1) + k]);
+    cudaStream_t st = c.own;
+    P->menus.ensure((size_t)std::max<ll>(mp, 1) * 8);
+    P->scores.ensure((size_t)std::max<ll>(mp, 1) * 4);
+    P->offsets.ensure((size_t)(n + 1) * 8);
+    P->binom.ensure(bt.size() * 8);
+    if (mp) RUMB_CUDA(cudaMemcpyAsync(P->menus.ptr, menus, (size_t)mp * 8, cudaMemcpyHostToDevice, st));
+    RUMB_CUDA(cudaMemcpyAsync(P->offsets.ptr, off.data(), (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st));
+    RUMB_CUDA(cudaMemcpyAsync(P->binom.ptr, bt.data(), bt.size() * 8, cudaMemcpyHostToDevice, st));
+    P->out.ensure(sizeof(PriceOut));
+    P->layer_step.ensure((size_t)(n + 1) * 4);
+    if (mode == 0) {
+        ull N = 1ULL << n;
+        P->Vs.ensure((size_t)N * 4);
+        P->Ps.ensure((size_t)N);
+    } else {
+        ull cap = 0;
+        for (ull v : P->counts) cap = v > cap ? v : cap;
+        ull nblk = (cap + PB - 1) / PB;
+        for (int i = 0; i < 2; ++i) {
+            P->v[i].ensure((size_t)cap * (mode == 1 ? 4 : 2));
+            if (mode == 3) P->l[i].ensure((size_t)cap);
+            P->m[i].ensure((size_t)nblk * 4);
+            P->e[i].ensure((size_t)nblk * 4);
+        }
+        std::vector<uint8_t *> ptrs(n + 1, nullptr);
+        P->pred.resize(n + 1);
+        for (int k = P->k_pred; k <= n; ++k) {
+            P->pred[k].reset(new DevBuf());
+            P->pred[k]->ensure((size_t)P->counts[k]);
+            ptrs[k] = P->pred[k]->as<uint8_t>();
+        }
+        P->pred_ptrs.ensure((size_t)(n + 1) * sizeof(void *));
+        RUMB_CUDA(cudaMemcpyAsync(P->pred_ptrs.ptr, ptrs.data(), (size_t)(n + 1) * sizeof(void *),
+                                  cudaMemcpyHostToDevice, st));
+        ull Nsub = 1ULL << P->k_pred;
+        P->Vs.ensure((size_t)Nsub * 4);
+        P->Ps.ensure((size_t)Nsub);
+    }
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    return P.release();
+}
+
+void pricer_destroy(Pricer *P) { delete P; }
+
+int pricer_device(const Pricer *P) { return P->c->device; }
+
+void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vmax, int32_t *rank_pos, double *margin,
+                  float *layer_step_out) {
+    Ctx &c = *P->c;
+    cudaStream_t st = c.own;
+    int n = P->n;
+    const float *scores = scores_host;
+    if (!on_device) {
+        if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->scores.ptr, scores_host, (size_t)P->mp * 4, cudaMemcpyHostToDevice, st));
+        scores = P->scores.as<float>();
+    }
+    const ull *menus = P->menus.as<ull>();
+    const ll *offs = P->offsets.as<ll>();
+    RUMB_CUDA(cudaMemsetAsync(P->layer_step.ptr, 0, (size_t)(n + 1) * 4, st));
+    if (P->mode == 0) {
+        RUMB_CUDA(cudaMemsetAsync(P->Vs.ptr, 0, ((size_t)1 << n) * 4, st));
+        RUMB_CUDA(cudaMemsetAsync(P->Ps.ptr, 0, (size_t)1 << n, st));
+        std::vector<ll> bounds;
+        const int *nodes = c.layer_table(n, bounds);
+        for (int cc = 1; cc <= n; ++cc) {
+            ll lo = bounds[cc], ns = bounds[cc + 1] - lo;
+            mask_layer_kernel<<<grid_for(ns, 256), 256, 0, st>>>(nodes + lo, ns, menus, scores, offs, n,
+                                                                  P->Vs.as<float>(), P->Ps.as<uint8_t>());
+            RUMB_LAUNCH("mask_layer_kernel");
+        }
+    } else {
+        int cur = 0, prev = 1;
+        // layer 0: V = 0 (offset 0, step 0, q 0)
+        RUMB_CUDA(cudaMemsetAsync(P->v[prev].ptr, 0, P->mode == 1 ? 4 : 2, st));
+        if (P->mode == 3) RUMB_CUDA(cudaMemsetAsync(P->l[prev].ptr, 0, 1, st));
+        RUMB_CUDA(cudaMemsetAsync(P->m[prev].ptr, 0, 4, st));
+        RUMB_CUDA(cudaMemsetAsync(P->e[prev].ptr, 0, 4, st));
+        for (int k = 1; k <= n; ++k) {
+            PricerArgs A{};
+            A.n = n;
+            A.k = k;
+            A.count = P->counts[k];
+            A.binom = P->binom.as<ull>();
+            A.menus = menus;
+            A.scores = scores;
+            A.offsets = offs;
+            A.mode = P->mode;
+            A.fma_decode = P->fma_decode;
+            A.vprev_f = P->v[prev].as<float>();
+            A.vprev_h = P->v[prev].as<uint16_t>();
+            A.lprev = P->l[prev].as<uint8_t>();
+            A.mprev = P->m[prev].as<float>();
+            A.eprev = P->e[prev].as<float>();
+            A.vcur_f = P->v[cur].as<float>();
+            A.vcur_h = P->v[cur].as<uint16_t>();
+            A.lcur = P->l[cur].as<uint8_t>();
+            A.mcur = P->m[cur].as<float>();
+            A.ecur = P->e[cur].as<float>();
+            A.pred = k >= P->k_pred ? P->pred[k]->as<uint8_t>() : nullptr;
+            A.layer_step = P->layer_step.as<unsigned int>() + k;
+            unsigned grid = (unsigned)((A.count + PB - 1) / PB);
+            stream_layer_kernel<<<grid, PB, 0, st>>>(A);
+            RUMB_LAUNCH("stream_layer_kernel");
+            std::swap(cur, prev);
+        }
+        backtrace_kernel<<<1, 1024, 0, st>>>(n, P->k_pred, P->binom.as<ull>(), P->pred_ptrs.as<uint8_t *>(), menus,
+                                             scores, offs, P->Vs.as<float>(), P->Ps.as<uint8_t>(),
+                                             P->out.as<PriceOut>(), P->v[prev].as<float>(), P->v[prev].as<uint16_t>(),
+                                             P->l[prev].as<uint8_t>(), P->m[prev].as<float>(), P->e[prev].as<float>(),
+                                             P->mode);
+        RUMB_LAUNCH("backtrace_kernel");
+    }
+    if (P->mode == 0) {
+        mask_readout_kernel<<<1, 32, 0, st>>>(n, P->Vs.as<float>(), P->Ps.as<uint8_t>(), P->out.as<PriceOut>());
+        RUMB_LAUNCH("mask_readout_kernel");
+    }
+    PriceOut h;
+    std::vector<unsigned int> steps(n + 1);
+    RUMB_CUDA(cudaMemcpyAsync(&h, P->out.ptr, sizeof(PriceOut), cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaMemcpyAsync(steps.data(), P->layer_step.ptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    double ms = 0.0;
+    for (int k = 1; k <= n; ++k) {
+        float f;
+        std::memcpy(&f, &steps[k], 4);
+        ms += (double)f;
+        if (layer_step_out) layer_step_out[k] = f;
+    }
+    if (layer_step_out) layer_step_out[0] = 0.0f;
+    for (int x = 0; x < n; ++x) rank_pos[x] = h.rank_pos[x];
+    if (P->mode <= 1) {
+        *vmax = (double)h.vtop;
+        *margin = 0.0;
+    } else {
+        *vmax = (double)h.mtop + (double)h.qtop * (double)h.etop;
+        *margin = P->mode == 2 ? 0.5 * ms : ms;
+    }
+}
+
+}  // namespace rumb

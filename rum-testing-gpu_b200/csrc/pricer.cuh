@@ -1,0 +1,18 @@
+// Internal interface of the Flow-CG pricer translation unit.
+#pragma once
+#include "ctx.cuh"
+
+namespace rumb {
+struct Pricer;
+Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t *offsets, int mode, int k_pred,
+                      int fma_decode);
+void pricer_destroy(Pricer *P);
+void pricer_price(Pricer *P, const float *scores, int on_device, double *vmax, int32_t *rank_pos, double *margin,
+                  float *layer_step_out);
+int pricer_device(const Pricer *P);
+}  // namespace rumb
+
+struct rumb_cg_pricer {
+    rumb::Pricer *p = nullptr;
+    int device = 0;
+};

@@ -52,6 +52,11 @@ class BMResult(ctypes.Structure):
                 ("device_ms", ctypes.c_double)]
 
 
+class KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 64), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
+                ("bytes_per_launch", ctypes.c_double)]
+
+
 TRACE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
                             ctypes.c_double, ctypes.c_double)
 
@@ -74,6 +79,13 @@ _SIGS = {
     "rumb_bm_solve": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, ctypes.POINTER(_vp),
                        ctypes.POINTER(BMResult), _vp, TRACE_FN, _vp], ctypes.c_int),
     "rumb_bm_state_destroy": ([_vp], ctypes.c_int),
+    "rumb_bm_profile": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), ctypes.c_int,
+                         ctypes.POINTER(KernelStat), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "rumb_cg_pricer_create": ([_vp, ctypes.c_int, ctypes.c_longlong, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "rumb_cg_price": ([_vp, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _vp,
+                       ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
+    "rumb_cg_pricer_destroy": ([_vp], ctypes.c_int),
     "rumb_bm_iterate": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, _vp, _vp, _vp,
                          ctypes.c_int, ctypes.c_int], ctypes.c_int),
 }
@@ -244,6 +256,17 @@ class Context:
             trace.extend(rows)
         return out, fit, (BMState(kept) if keep and kept.value else None)
 
+    def bm_profile(self, problem, params, iters=20):
+        """[dict(name, launches, total_ms, bytes_per_launch)] over `iters` eager iterations."""
+        pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
+        cap = 64
+        arr = (KernelStat * cap)()
+        cnt = ctypes.c_int()
+        check(load().rumb_bm_profile(self.h, ctypes.byref(pr), ctypes.byref(params), int(iters), arr, cap,
+                                     ctypes.byref(cnt)))
+        return [dict(name=arr[i].name.decode(), launches=arr[i].launches, total_ms=arr[i].total_ms,
+                     bytes_per_launch=arr[i].bytes_per_launch) for i in range(cnt.value)]
+
     def bm_iterate(self, problem, params, state, iters, cold_start=False):
         pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
         dt = np.float64 if params.dtype == F64 else np.float32
@@ -254,6 +277,54 @@ class Context:
         check(load().rumb_bm_iterate(self.h, ctypes.byref(pr), ctypes.byref(params), _p(st["x2"]), _p(st["s"]),
                                      _p(st["y"]), _p(st["z"]), int(iters), int(bool(cold_start))))
         return st
+
+
+PRICE_MODES = {"mask": 0, "f32": 1, "u16": 2, "u24": 3}
+
+
+class Pricer:
+    """Flow-CG pricer on one GPU (rows in x-major order; see rumb_cg_pricer_create)."""
+
+    def __init__(self, ctx, n, menus, offsets, mode="u24", k_pred=None, fma_decode=True):
+        menus = np.ascontiguousarray(menus, dtype=np.uint64)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        h = ctypes.c_void_p()
+        check(load().rumb_cg_pricer_create(ctx.h, int(n), menus.size, _p(menus), _p(offsets), PRICE_MODES[mode],
+                                           0 if k_pred is None else int(k_pred), int(bool(fma_decode)),
+                                           ctypes.byref(h)))
+        self.h, self.n, self.mp, self.mode, self.ctx = h, int(n), menus.size, mode, ctx
+
+    def price(self, scores, want_steps=False):
+        """(vmax, rank_pos int32[n], margin[, layer_step float32[n+1]]) for float32 scores."""
+        scores = np.ascontiguousarray(scores, dtype=np.float32)
+        if scores.size != self.mp:
+            raise ValueError("expected %d scores" % self.mp)
+        vmax, margin = ctypes.c_double(), ctypes.c_double()
+        rank = np.zeros(self.n, dtype=np.int32)
+        steps = np.zeros(self.n + 1, dtype=np.float32)
+        check(load().rumb_cg_price(self.h, _p(scores), 0, ctypes.byref(vmax), _p(rank), ctypes.byref(margin),
+                                   _p(steps)))
+        if want_steps:
+            return vmax.value, rank, margin.value, steps
+        return vmax.value, rank, margin.value
+
+    def price_device(self, scores_ptr):
+        vmax, margin = ctypes.c_double(), ctypes.c_double()
+        rank = np.zeros(self.n, dtype=np.int32)
+        check(load().rumb_cg_price(self.h, ctypes.c_void_p(int(scores_ptr)), 1, ctypes.byref(vmax), _p(rank),
+                                   ctypes.byref(margin), None))
+        return vmax.value, rank, margin.value
+
+    def close(self):
+        if self.h:
+            load().rumb_cg_pricer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class BMState:

@@ -1,0 +1,113 @@
+"""Flow-CG pricing on the GPU through the C ABI: bit-exact against the oracle (values, rankings,
+quantization steps) in every storage mode, and column-for-column equal CG trajectories."""
+import numpy as np
+import pytest
+
+import oracle as O
+import paper_instances as PI
+from rumb import _lib
+from rumb.instances import config_instance
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    yield "pair6", PI.gen_pairwise(6)[0], 6
+    yield "pair8", PI.gen_pairwise(8)[0], 8
+    yield "med12", PI.gen_medium(12, mult=3)[0], 12
+    yield "pair16", PI.gen_pairwise(16)[0], 16
+    yield "med16", PI.gen_medium(16, mult=2)[0], 16
+    n, m, a, p = config_instance("n18_d05pct_k50")
+    yield "n18_d05pct", np.column_stack([m, a, p]).astype(np.float64), n
+
+
+CASES = list(_cases())
+
+
+@pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("mode", ["mask", "f32", "u16", "u24"])
+def test_pricer_bit_exact_against_oracle(ctx, name, cd, n, mode):
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+    rng = np.random.RandomState(7)
+    trials = 2 if n >= 16 else 3
+    for trial in range(trials):
+        scores = (rng.randn(menus.size) * (2.0 if trial == 0 else 0.05)).astype(np.float32)
+        if trial == trials - 1:
+            scores = (p32 - p32.mean()).astype(np.float32)      # residual-like scores
+        if mode == "mask":
+            v_ref, r_ref = O.price_mask(n, menus, scores, offsets)
+            m_ref = 0.0
+        else:
+            v_ref, r_ref, m_ref, steps_ref = O.price_stream(n, menus, scores, offsets, mode=mode)
+        v, r, m, steps = pr.price(scores, want_steps=True)
+        assert v == v_ref, (trial, v, v_ref)
+        np.testing.assert_array_equal(r, r_ref)
+        if mode in ("u16", "u24"):
+            np.testing.assert_array_equal(steps, steps_ref)
+            assert m == m_ref
+    pr.close()
+
+
+def test_mask_and_f32_stream_identical(ctx):
+    cd, mp = PI.gen_medium(14, mult=4)
+    menus, alts, p32, offsets, _ = O.cg_layout(14, cd[:, 0], cd[:, 1], cd[:, 2])
+    a = _lib.Pricer(ctx, 14, menus, offsets, mode="mask")
+    b = _lib.Pricer(ctx, 14, menus, offsets, mode="f32", k_pred=6)
+    rng = np.random.RandomState(3)
+    for _ in range(4):
+        s = rng.randn(menus.size).astype(np.float32)
+        va, ra, _ = a.price(s)
+        vb, rb, _ = b.price(s)
+        assert va == vb and np.array_equal(ra, rb)
+
+
+@pytest.mark.parametrize("mode", ["u24", "u16", "f32"])
+def test_cg_trajectory_matches_oracle(ctx, mode):
+    from rumb import flow_cg
+    cd, mp = PI.gen_medium(12, mult=4)
+    n = 12
+    prob = flow_cg.CGProblem(ctx, n, cd[:, 0], cd[:, 1], mode)
+    mine = flow_cg.solve_cg(prob, cd[:, 2], max_iters=120, gap_abs_tol=1e-6, record_columns=True)
+    ref = O.cg_solve(n, cd[:, 0], cd[:, 1], cd[:, 2], mode=mode, max_iters=120, gap_abs_tol=1e-6)
+    assert len(mine["picked"]) == len(ref["columns"])
+    for i, (a, b) in enumerate(zip(mine["picked"], ref["columns"])):
+        assert np.array_equal(a, b), "column %d differs" % i
+    assert mine["distance"] == ref["ub"] and mine["lb"] == ref["lb"]
+
+
+def test_cg_columns_on_config3_residuals(ctx):
+    """n = 18, 0.5 % density: the GPU loop's residual scores at several iterations, priced again by
+    the oracle, give the same columns."""
+    from rumb import flow_cg
+    n, m, a, p = config_instance("n18_d05pct_k50")
+    for mode in ("u24", "u16"):
+        prob = flow_cg.CGProblem(ctx, n, m, a, mode)
+        seen = []
+
+        class Spy:
+            def __init__(self, inner):
+                self.inner = inner
+
+            def price(self, s):
+                out = self.inner.price(s)
+                if len(seen) in (0, 5, 20):
+                    seen.append((s.copy(), out))
+                else:
+                    seen.append(None)
+                return out
+
+        prob.pricer = Spy(prob.pricer)
+        flow_cg.solve_cg(prob, p, max_iters=25, gap_abs_tol=1e-9)
+        menus, alts, p32, offsets, _ = O.cg_layout(n, m, a, p)
+        for item in seen:
+            if item is None:
+                continue
+            s, (v, r, mg) = item
+            v_ref, r_ref, m_ref, _ = O.price_stream(n, menus, s, offsets, mode=mode)
+            assert v == v_ref and np.array_equal(r, r_ref) and mg == m_ref
+
+
+def test_pricer_rejects_bad_rows(ctx):
+    with pytest.raises(_lib.RumbError):
+        _lib.Pricer(ctx, 4, np.array([3, 4], dtype=np.uint64), np.array([0, 1, 2, 2, 2]), mode="u24")

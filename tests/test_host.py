@@ -1,0 +1,139 @@
+"""Host logic without a GPU: input checks and messages of the RUM class, planning with a fake
+device-memory query (the reference's stub-profile pattern, tests/test_cpu.py:215-279), the
+Flow-CG master pieces against the reference's golden vectors, and the seeded generators."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from rumb import rum_solver, flow_cg, defaults
+from rumb.instances import config_instance, mixture_instance, panel_instance, dsr_instance
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture
+def fake_gpu(monkeypatch):
+    monkeypatch.setattr(rum_solver, "gpu_free_bytes", lambda device=0: 150 * 2 ** 30)
+
+
+def test_input_errors():
+    R = rum_solver.RUM
+    with pytest.raises(ValueError, match="no observations"):
+        R([], [], [])
+    with pytest.raises(ValueError, match="empty menu"):
+        R([0, 3], [0, 1], [0.5, 0.5])
+    with pytest.raises(ValueError, match="not in its menu"):
+        R([3, 3], [0, 2], [0.5, 0.5])
+    with pytest.raises(ValueError, match="appears more than once"):
+        R([3, 3], [0, 0], [0.5, 0.5])
+    with pytest.raises(ValueError, match="outside"):
+        R([3, 3], [0, 1], [0.5, 1.5])
+    with pytest.raises(ValueError, match="must hold integers"):
+        R([3.5, 3], [0, 1], [0.5, 0.5])
+    with pytest.raises(ValueError, match="num_alternatives"):
+        R([3, 3], [0, 1], [0.5, 0.5], num_alternatives=1)
+    with pytest.warns(UserWarning, match="summing to more than 1"):
+        R([3, 3], [0, 1], [0.7, 0.7])
+
+
+def test_method_args_and_planning(fake_gpu):
+    n, m, a, p = config_instance("n10_all_k20")
+    rum = rum_solver.RUM(m, a, p)
+    with pytest.raises(ValueError, match="unknown method_args"):
+        rum._plan("bm_admm", {"bogus": 1})
+    with pytest.raises(ValueError, match="needs a named method"):
+        rum._plan(None, {"check": 10})
+    with pytest.raises(ValueError, match="unknown method"):
+        rum._plan("ip_cg", None)
+    name, _, args = rum._plan("bm_admm", {"check": 25})
+    assert name == "bm_admm" and args["check"] == 25 and args["dtype"] == "float64"
+    assert args["beta"] == pytest.approx(2.534415507522252)
+    name, _, args = rum._plan("flow_cg", {"pricing": "stream_u16"})
+    assert args["_engine"] == "u16" and args["pricing"] == "stream"
+    with pytest.raises(ValueError, match="contradicts"):
+        rum._plan("flow_cg", {"pricing": "stream_u16", "dtype": "uint24"})
+    with pytest.raises(ValueError, match="mask pricing stores float32"):
+        rum._plan("flow_cg", {"pricing": "mask", "dtype": "uint16"})
+    with pytest.raises(ValueError):
+        rum._plan("bm_admm", {"dtype": "float16"})
+
+
+def test_choose_method_density_rule(fake_gpu):
+    assert rum_solver.choose_method(10, 5110)[0] == "flow_cg"
+    assert rum_solver.choose_method(18, 23650)[0] == "bm_admm"          # 1 % >= 0.5 %
+    assert rum_solver.choose_method(18, 5000)[0] == "flow_cg"           # 0.2 %
+    assert rum_solver.choose_method(12, 20000)[0] == "bm_admm"
+
+
+def test_planner_memory_refusal(monkeypatch):
+    monkeypatch.setattr(rum_solver, "gpu_free_bytes", lambda device=0: 2 ** 30)
+    with pytest.raises(RuntimeError, match="needs .* GB of GPU memory"):
+        rum_solver._plan_bm_admm(24, 1000, dict(defaults.METHOD_ARGS["bm_admm"]))
+    # the automatic choice falls back to flow_cg
+    assert rum_solver.choose_method(24, 4 * 10 ** 6)[0] == "flow_cg"
+
+
+def test_races_and_weights_refused():
+    n, m, a, p = config_instance("n10_all_k20")
+    rum = rum_solver.RUM(m, a, p)
+    with pytest.raises(ValueError, match="races"):
+        rum.calculate_distance(opt=1.0)
+    with pytest.raises(RuntimeError, match="unweighted"):
+        rum.calculate_distance(vcov=2 * np.eye(p.size))
+
+
+def test_threshold_on_rest_rows():
+    assert rum_solver._on_rest(None, 0.3, True) is None
+    assert rum_solver._on_rest(0.5, 0.3, True) == 0.0
+    assert rum_solver._on_rest(0.5, 0.3, False) is None
+    assert rum_solver._on_rest(1.0, 0.36, True) == pytest.approx(0.8)
+    with pytest.raises(ValueError):
+        rum_solver._on_rest(math.inf, 0.0, True)
+
+
+def test_master_pieces_against_reference():
+    g = np.load(os.path.join(GOLD, "qp.npz"))
+    for t in range(4):
+        lam, A = flow_cg.solve_qp_native(g["Q_%d" % t], g["h_%d" % t])
+        np.testing.assert_allclose(lam, g["lam_%d" % t], atol=1e-12)
+        np.testing.assert_array_equal(flow_cg.project_simplex(g["ps_y_%d" % t]), g["ps_x_%d" % t])
+    c = np.load(os.path.join(GOLD, "columns.npz"))
+    for t in range(5):
+        col = flow_cg.ranking_column(c["menus"].astype(np.uint64), c["alts"], c["rank_%d" % t], 18)
+        np.testing.assert_array_equal(col, c["col_%d" % t])
+
+
+def test_gram_and_pout_maintainers():
+    rng = np.random.default_rng(1)
+    M = 300
+    ph = rng.random(M)
+    g = flow_cg.GramMaintainer(M, ph, max_K=10)
+    po = flow_cg.PoutMaintainer(M)
+    cols = [(rng.random(M) < 0.4).astype(np.uint8) for _ in range(6)]
+    for c in cols:
+        g.add_column(c.astype(np.float64))
+        po.add_column(c)
+    V = np.stack(cols, axis=1).astype(np.float64)
+    Q, h = g.view()
+    np.testing.assert_array_equal(Q, V.T @ V)
+    np.testing.assert_allclose(h, V.T @ ph, rtol=1e-14)
+    lam = rng.dirichlet(np.ones(6))
+    po.apply_delta(lam)
+    np.testing.assert_allclose(po.p_out, V @ lam, atol=1e-14)
+
+
+def test_generators_shapes_and_determinism():
+    n, m, a, p = config_instance("n10_all_k20")
+    assert np.unique(m).size == 1013 and m.size == 5110
+    sums = np.bincount(np.unique(m, return_inverse=True)[1], weights=p)
+    np.testing.assert_allclose(sums, 1.0)
+    m1, a1, p1 = mixture_instance(12, 0.2, 5, 100, seed=4)
+    m2, a2, p2 = mixture_instance(12, 0.2, 5, 100, seed=4)
+    assert np.array_equal(m1, m2) and np.array_equal(p1, p2)
+    panel, (mm, aa, pp) = panel_instance(12, 0.1, 40, 5, 4, seed=1)
+    assert panel["menu"].size == 200 and set(np.unique(panel["respondent"])) == set(range(40))
+    panel, (mm, aa, pp) = dsr_instance(10, 20, 30, 4, seed=1)
+    assert mm.size == 20 and (aa == 0).all() and ((mm & 1) == 1).all()
