@@ -278,7 +278,8 @@ def main():
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": n, "cells": int(mp), "menus": int(np.unique(menu).size),
                    "abs_tol": ABS_TOL, "rel_tol": None, "check": CHECK, "beta": beta,
-                   "iters_per_solve": int(res["iters"]), "checks_per_solve": int(res["n_push"]),
+                   "iters_per_solve": int(res["iters"]), "iters_float32": int(res["iters_f32"]),
+                   "checks_per_solve": int(res["n_push"]),
                    "ub": res["ub"], "lb": res["lb"], "state_dtype": args.dtype,
                    "l2": "flushed (256 MB write) before every timed solve; state slabs exceed L2",
                    "parallelism": "replicas x%d" % world},

@@ -22,6 +22,8 @@
 #include <cstring>
 
 #include "bfly.cuh"
+#include "xform.cuh"
+#include "prox.cuh"
 #include "bm.cuh"
 #include "ctx.cuh"
 
@@ -34,8 +36,8 @@ struct ProxArgs {
     ll Nloc, nmenus;
     const T *v;         // PROX mode input
     T *out;             // PROX mode output
-    const T *x, *Ax;    // ITER mode inputs
-    T *x2, *z, *s, *y;  // ITER mode state (updated in place)
+    const T *x;         // ITER mode input
+    T *x2, *z;          // ITER mode state (updated in place)
     const T *xhat;
     const uint32_t *obsbits;
     T alpha, b1, b2, ib1, ib2;
@@ -74,13 +76,7 @@ __global__ void __launch_bounds__(128) prox_kernel(ProxArgs<T> P) {
                 T xi = P.x[pos], x2i = P.x2[pos], zi = P.z[pos];
                 T xo = P.alpha * xi + (one - P.alpha) * x2i;
                 v = xo - P.ib2 * zi;
-                q[i] = xo;
-                T ax = P.Ax[pos], si = P.s[pos], yi = P.y[pos];
-                T axor = -P.alpha * ax - (one - P.alpha) * si;
-                T sn = P.ib1 * yi - axor;
-                sn = sn > (T)0 ? sn : (T)0;
-                P.y[pos] = yi - P.b1 * (axor + sn);
-                P.s[pos] = sn;
+                q[i] = zi - P.b2 * xo;                 // z' = z - b2 (xo - u) = q + b2 u
             } else {
                 v = P.v[pos];
             }
@@ -155,7 +151,7 @@ __global__ void __launch_bounds__(128) prox_kernel(ProxArgs<T> P) {
                 u = yv > 0.0 ? (T)yv : (T)0;
             }
             if (MODE == PROX_ITER) {
-                P.z[pos] = P.z[pos] - P.b2 * (q[i] - u);
+                P.z[pos] = q[i] + P.b2 * u;
                 P.x2[pos] = u;
             } else {
                 P.out[pos] = u;
@@ -171,7 +167,7 @@ static void launch_prox_n(const ProxArgs<T> &P, cudaStream_t st) {
     int n = P.n;
     if (g_prof) {
         double S = (double)P.Nloc * n, e = sizeof(T);
-        double bytes = (MODE == PROX_ITER ? 10.0 : 2.0) * S * e + S / 8.0;
+        double bytes = (MODE == PROX_ITER ? 5.0 : 2.0) * S * e + S / 8.0;
         prof_begin(MODE == PROX_ITER ? (e == 8 ? "prox_fused<f64>" : "prox_fused<f32>")
                                      : (e == 8 ? "prox_only<f64>" : "prox_only<f32>"), bytes, st);
     }
@@ -351,6 +347,19 @@ __global__ void convert_kernel(const TI *in, TO *out, ll m) {
     if (i < m) out[i] = (TO)in[i];
 }
 
+// s/y update of the reference's fuse_sy (solver/bm_admm/solver.py:47-51), small-n path
+template <class T>
+__global__ void sy_update_kernel(const T *Ax, T *s, T *y, ll m, T alpha, T b1, T ib1) {
+    ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    T one = (T)1;
+    T axor = -alpha * Ax[i] - (one - alpha) * s[i];
+    T sn = ib1 * y[i] - axor;
+    sn = sn > (T)0 ? sn : (T)0;
+    y[i] -= b1 * (axor + sn);
+    s[i] = sn;
+}
+
 // ----------------------------------------------------------------- layers (host build, cached)
 const int *Ctx::layer_table(int n, std::vector<ll> &bounds) {
     auto it = layers.find(n);
@@ -373,6 +382,29 @@ const int *Ctx::layer_table(int n, std::vector<ll> &bounds) {
     layer_bounds[n] = b;
     bounds = b;
     return buf->as<int>();
+}
+
+// Generic full transform in -> out (K_PLAIN passes; the certificate's Mobius, zeta and
+// subset-sum butterflies). in may be float32 while out is float64 (the first pass converts).
+template <class T, class TI>
+static void xf_transform(int n, const TI *in, T *out, Co<T> k, cudaStream_t st) {
+    if (n - 1 < 5) {
+        bf_transform<T, TI>(n, in, out, k.a, k.b, k.c, k.d, st);
+        return;
+    }
+    std::vector<XfShape> plan = xf_plan(n - 1);
+    ll Nloc = 1LL << (n - 1);
+    for (size_t i = 0; i < plan.size(); ++i) {
+        if (i == 0) {
+            XfArgs<T, TI> A{};
+            A.in = in; A.out = out; A.k1 = k; A.Nloc = Nloc; A.s0 = plan[i].s0; A.B = plan[i].B;
+            xf_launch<T, TI, K_PLAIN>(A, plan[i], n, st);
+        } else {
+            XfArgs<T, T> A{};
+            A.in = out; A.out = out; A.k1 = k; A.Nloc = Nloc; A.s0 = plan[i].s0; A.B = plan[i].B;
+            xf_launch<T, T, K_PLAIN>(A, plan[i], n, st);
+        }
+    }
 }
 
 // ----------------------------------------------------------------- certificate workspace
@@ -412,7 +444,7 @@ static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t s
     ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
     const double eps = 1e-12;
     double *qa = W.qa.as<double>(), *qb = W.qb.as<double>();
-    bf_transform<double, T>(n, x2, qa, 1.0, -1.0, 0.0, 1.0, st);          // Mobius
+    xf_transform<double, T>(n, x2, qa, Co<double>{1.0, -1.0, 0.0, 1.0}, st);     // Mobius
     outw_kernel<<<grid_for(N, 256), 256, 0, st>>>(qa, W.outw.as<double>(), n, Nloc, eps);
     RUMB_LAUNCH("outw_kernel");
     std::vector<ll> bounds;
@@ -429,7 +461,7 @@ static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t s
     extract_kernel<<<grid_for(m2, 256), 256, 0, st>>>(qa, W.outw.as<double>(), W.mass.as<double>(), qb, n, Nloc,
                                                       eps);
     RUMB_LAUNCH("extract_kernel");
-    bf_transform<double, double>(n, qb, qa, 1.0, 1.0, 0.0, 1.0, st);      // zeta -> x_ub in qa
+    xf_transform<double, double>(n, qb, qa, Co<double>{1.0, 1.0, 0.0, 1.0}, st);  // zeta -> x_ub in qa
     ub_eval_kernel<<<1, RED_THREADS, 0, st>>>(qa, W.obs.as<ll>(), W.p.as<double>(), W.mp,
                                               W.pfit_cur.as<double>(), W.res.as<double>());
     RUMB_LAUNCH("ub_eval_kernel");
@@ -450,7 +482,7 @@ static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_
                                                    with_lb ? g : nullptr, W.res.as<double>());
     RUMB_LAUNCH("obs_stats_kernel");
     if (!with_lb) return;
-    bf_transform<double, double>(n, g, g, 1.0, 0.0, 1.0, 1.0, st);        // subset sums
+    xf_transform<double, double>(n, g, g, Co<double>{1.0, 0.0, 1.0, 1.0}, st);    // subset sums
     std::vector<ll> bounds;
     const int *nodes = c.layer_table(n, bounds);
     double *dp = W.dp.as<double>();
@@ -469,7 +501,7 @@ static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_
 // ================================================================= ADMM workspace
 template <class T>
 struct BmWork : public BmWorkBase {
-    DevBuf x2, s, y, z, x, Ax, t1, t2, xhat, obsbits, diag;
+    DevBuf x2, s, y, z, x, Ax, t1, t2, xhat, obsbits, diag, err, menu_obs;
     int n = 0;
     void ensure(int n_) {
         n = n_;
@@ -477,7 +509,9 @@ struct BmWork : public BmWorkBase {
         size_t sb = (size_t)m2 * sizeof(T);
         for (DevBuf *b : {&x2, &s, &y, &z, &x, &Ax, &t1, &t2, &xhat}) b->ensure(sb);
         obsbits.ensure((size_t)((m2 + 31) / 32) * 4);
+        menu_obs.ensure((size_t)4 << n);
         diag.ensure(64 * sizeof(T));
+        err.ensure(16);
     }
 };
 
@@ -513,8 +547,9 @@ static Eigen eigen2(double p) {
 
 struct BmCoef {
     double b1, b2, ib1, ib2, alpha, p;
-    double Qt[4], Q[4];
+    double Qt[4], Q[4], AQ[4];
     std::vector<double> diag;   // by popcount, nb + 1 entries
+    int lo_bits = 12;           // transform window split (tuned)
 };
 
 static BmCoef make_coef(int n, double beta, double alpha, double p) {
@@ -526,6 +561,8 @@ static BmCoef make_coef(int n, double beta, double alpha, double p) {
     Eigen E = eigen2(p);
     C.Qt[0] = E.Q[0][0]; C.Qt[1] = E.Q[1][0]; C.Qt[2] = E.Q[0][1]; C.Qt[3] = E.Q[1][1];
     C.Q[0] = E.Q[0][0]; C.Q[1] = E.Q[0][1]; C.Q[2] = E.Q[1][0]; C.Q[3] = E.Q[1][1];
+    // A Q with A = [[1, -1], [0, p]] (the raw A butterfly, solver/bm_admm/solver.py:247)
+    C.AQ[0] = C.Q[0] - C.Q[2]; C.AQ[1] = C.Q[1] - C.Q[3]; C.AQ[2] = p * C.Q[2]; C.AQ[3] = p * C.Q[3];
     int nb = n - 1;
     double gamma = 1.0;                                  // beta2 / beta1
     for (int pc = 0; pc <= nb; ++pc) {
@@ -537,25 +574,117 @@ static BmCoef make_coef(int n, double beta, double alpha, double p) {
 }
 
 template <class T>
-static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
+static void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st) {
+    size_t smem = prox_tile_smem<T>(P.n);
+    unsigned grid = (unsigned)(1LL << (P.n - PT_M));
+#define RUMB_PT_CASE(NN)                                                                                   \
+    if (P.n <= NN) {                                                                                       \
+        static bool attr = false;                                                                          \
+        if (!attr) {                                                                                       \
+            RUMB_CUDA(cudaFuncSetAttribute(prox_tile_kernel<T, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                           (int)prox_tile_smem<T>(NN)));                                   \
+            attr = true;                                                                                   \
+        }                                                                                                  \
+        prox_tile_kernel<T, NN><<<grid, PT_THREADS, smem, st>>>(P);                                        \
+        RUMB_LAUNCH("prox_tile_kernel");                                                                   \
+        return;                                                                                            \
+    }
+    RUMB_PT_CASE(30)
+#undef RUMB_PT_CASE
+    fail(RUMB_E_INVAL, "prox: n > 30");
+}
+
+// The reference's one_iter (solver/bm_admm/solver.py:240-254) for n <= 5: separate butterflies.
+template <class T>
+static void enqueue_iteration_small(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
     T *x2 = W.x2.template as<T>(), *s = W.s.template as<T>(), *y = W.y.template as<T>(), *z = W.z.template as<T>();
     T *x = W.x.template as<T>(), *Ax = W.Ax.template as<T>(), *t1 = W.t1.template as<T>(), *t2 = W.t2.template as<T>();
     T p = (T)C.p;
-    // rhs = (z + b2 x2 - A'(y - b1 s)) / b1
     bf_transform<T, T>(n, t1, t1, (T)1, (T)0, (T)-1, p, st, PRO_W, y, s, (T)C.b1, EPI_RHS, z, x2, (T)C.b2,
                        (T)C.ib1);
-    // x = Q diag Q^T rhs
     bf_transform<T, T>(n, t1, t2, (T)C.Qt[0], (T)C.Qt[1], (T)C.Qt[2], (T)C.Qt[3], st, PRO_PLAIN, nullptr, nullptr,
                        (T)0, EPI_DIAG, nullptr, nullptr, (T)0, (T)0, W.diag.template as<T>());
     bf_transform<T, T>(n, t2, x, (T)C.Q[0], (T)C.Q[1], (T)C.Q[2], (T)C.Q[3], st);
-    // Ax
     bf_transform<T, T>(n, x, Ax, (T)1, (T)-1, (T)0, p, st);
-    // fused prox + z + s/y + x2
+    sy_update_kernel<T><<<grid_for((ll)n << (n - 1), 256), 256, 0, st>>>(Ax, s, y, (ll)n << (n - 1), (T)C.alpha,
+                                                                       (T)C.b1, (T)C.ib1);
+    RUMB_LAUNCH("sy_update_kernel");
+}
+
+// One ADMM iteration: 4 register-tiled transform passes (or 1 for n <= 13, more for n >= 21)
+// and the fused prox.
+template <class T>
+static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
+    T *x2 = W.x2.template as<T>(), *s = W.s.template as<T>(), *y = W.y.template as<T>(), *z = W.z.template as<T>();
+    T *x = W.x.template as<T>(), *Ax = W.Ax.template as<T>(), *t1 = W.t1.template as<T>(), *t2 = W.t2.template as<T>();
+    if (n - 1 < 5) {
+        enqueue_iteration_small<T>(W, C, n, st);
+    } else {
+        T p = (T)C.p;
+        Co<T> kA{(T)1, (T)0, (T)-1, p};                                    // A' (sign folded)
+        Co<T> kQt{(T)C.Qt[0], (T)C.Qt[1], (T)C.Qt[2], (T)C.Qt[3]};
+        Co<T> kQ{(T)C.Q[0], (T)C.Q[1], (T)C.Q[2], (T)C.Q[3]};
+        Co<T> kAQ{(T)C.AQ[0], (T)C.AQ[1], (T)C.AQ[2], (T)C.AQ[3]};      // A Q, A = [[1,-1],[0,p]]
+        std::vector<XfShape> plan = xf_plan(n - 1, C.lo_bits);
+        XfArgs<T, T> base{};
+        base.Nloc = 1LL << (n - 1);
+        base.b1 = (T)C.b1; base.b2 = (T)C.b2; base.ib1 = (T)C.ib1; base.alpha = (T)C.alpha;
+        base.diag = W.diag.template as<T>();
+        auto at = [&](const XfShape &sh) { XfArgs<T, T> A = base; A.s0 = sh.s0; A.B = sh.B; return A; };
+        const size_t m = plan.size() - 1;                                  // high windows
+        if (m == 0) {
+            XfArgs<T, T> A = at(plan[0]);
+            A.y = y; A.s = s; A.z = z; A.x2 = x2; A.out = x; A.s_io = s; A.y_io = y;
+            A.k1 = kA; A.k2 = kQt; A.k3 = kQ; A.k4 = kAQ;
+            xf_launch<T, T, K_FULL>(A, plan[0], n, st);
+        } else {
+            { XfArgs<T, T> A = at(plan[0]); A.y = y; A.s = s; A.out = t1; A.k1 = kA;
+              xf_launch<T, T, K_P1>(A, plan[0], n, st); }
+            for (size_t i = 1; i < m; ++i) {
+                XfArgs<T, T> A = at(plan[i]); A.in = t1; A.out = t1; A.k1 = kA;
+                xf_launch<T, T, K_PLAIN>(A, plan[i], n, st);
+            }
+            { XfArgs<T, T> A = at(plan[m]); A.in = t1; A.out = t2; A.z = z; A.x2 = x2; A.k1 = kA; A.k2 = kQt;
+              xf_launch<T, T, K_P2>(A, plan[m], n, st); }
+            for (size_t i = 1; i < m; ++i) {
+                XfArgs<T, T> A = at(plan[i]); A.in = t2; A.out = t2; A.k1 = kQt;
+                xf_launch<T, T, K_PLAIN>(A, plan[i], n, st);
+            }
+            { XfArgs<T, T> A = at(plan[0]); A.in = t2; A.out = x; A.out2 = Ax; A.k1 = kQt; A.k2 = kQ; A.k3 = kAQ;
+              xf_launch<T, T, K_P3>(A, plan[0], n, st); }
+            for (size_t i = 1; i < m; ++i) {
+                XfArgs<T, T> A = at(plan[i]); A.in = x; A.in2 = Ax; A.out = x; A.out2 = Ax; A.k1 = kQ; A.k3 = kAQ;
+                xf_launch<T, T, K_DUAL>(A, plan[i], n, st);
+            }
+            { XfArgs<T, T> A = at(plan[m]); A.in = x; A.in2 = Ax; A.out = x; A.s_io = s; A.y_io = y; A.k1 = kQ;
+              A.k3 = kAQ;
+              xf_launch<T, T, K_P4>(A, plan[m], n, st); }
+        }
+    }
+    // fused prox + z + x2
+    if (n >= PT_M + 1) {
+        ProxTileArgs<T> P{};
+        P.n = n;
+        P.Nloc = 1LL << (n - 1);
+        P.x = x; P.x2 = x2; P.z = z;
+        P.xhat = W.xhat.template as<T>();
+        P.menu_obs = W.menu_obs.template as<uint32_t>();
+        P.alpha = (T)C.alpha; P.b2 = (T)C.b2; P.ib2 = (T)C.ib2;
+        P.inv_c0 = (T)(1.0 / C.b2); P.inv_c1 = (T)(1.0 / (C.b2 + 2.0));
+        P.err = W.err.template as<unsigned int>();
+        if (g_prof) {
+            double S = (double)P.Nloc * n, e = sizeof(T);
+            prof_begin(e == 8 ? "prox_tile<f64>" : "prox_tile<f32>", 5.0 * S * e + 4.0 * (1LL << n), st);
+        }
+        launch_prox_tile<T>(P, st);
+        prof_end(st);
+        return;
+    }
     ProxArgs<T> P{};
     P.n = n;
     P.Nloc = 1LL << (n - 1);
     P.nmenus = (1LL << n) - 1;
-    P.x = x; P.Ax = Ax; P.x2 = x2; P.z = z; P.s = s; P.y = y;
+    P.x = x; P.x2 = x2; P.z = z;
     P.xhat = W.xhat.template as<T>();
     P.obsbits = W.obsbits.template as<uint32_t>();
     P.alpha = (T)C.alpha; P.b1 = (T)C.b1; P.b2 = (T)C.b2; P.ib1 = (T)C.ib1; P.ib2 = (T)C.ib2;
@@ -576,6 +705,38 @@ static void enqueue_cold_start(BmWork<T> &W, const BmCoef &C, int n, cudaStream_
     P.b2 = (T)C.b2;
     launch_prox_n<T, PROX_ONLY>(P, st);
     for (DevBuf *b : {&W.s, &W.y, &W.z}) RUMB_CUDA(cudaMemsetAsync(b->ptr, 0, (size_t)m2 * sizeof(T), st));
+}
+
+// Picks the low-window size of the transform passes by timing a few iterations of each candidate
+// on the workspace (cached per context, n and dtype). The state is reset by the caller.
+template <class T>
+static int tune_lo_bits(Ctx &c, BmWork<T> &W, BmCoef C, int n, cudaStream_t st) {
+    auto key = std::make_pair(n, (int)sizeof(T));
+    auto it = c.lo_bits.find(key);
+    if (it != c.lo_bits.end()) return it->second;
+    int best = 12;
+    if (n - 1 > 10) {
+        float best_ms = 1e30f;
+        cudaEvent_t a, b;
+        RUMB_CUDA(cudaEventCreate(&a));
+        RUMB_CUDA(cudaEventCreate(&b));
+        for (int lb : {10, 11, 12}) {
+            if (lb > n - 1) continue;
+            C.lo_bits = lb;
+            for (int i = 0; i < 2; ++i) enqueue_iteration<T>(W, C, n, st);
+            RUMB_CUDA(cudaEventRecord(a, st));
+            for (int i = 0; i < 6; ++i) enqueue_iteration<T>(W, C, n, st);
+            RUMB_CUDA(cudaEventRecord(b, st));
+            RUMB_CUDA(cudaEventSynchronize(b));
+            float ms = 0.f;
+            RUMB_CUDA(cudaEventElapsedTime(&ms, a, b));
+            if (ms < best_ms) { best_ms = ms; best = lb; }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    c.lo_bits[key] = best;
+    return best;
 }
 
 // ----------------------------------------------------------------- problem upload
@@ -627,6 +788,10 @@ static void setup_obs(Ctx &c, CertWork &CW, BmWork<T> *W, const rumb_bm_problem 
                                                               CW.obs.as<ll>(), xhat, bits, bad.as<int>());
     RUMB_LAUNCH("obs_setup_kernel");
     RUMB_CUDA(cudaMemcpyAsync(CW.p.ptr, D.d_p, (size_t)pr.mp * 8, cudaMemcpyDeviceToDevice, st));
+    if (W) {
+        menu_obs_kernel<<<grid_for(1LL << n, 256), 256, 0, st>>>(bits, n, Nloc, W->menu_obs.template as<uint32_t>());
+        RUMB_LAUNCH("menu_obs_kernel");
+    }
     int hbad = 0;
     RUMB_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, st));
     RUMB_CUDA(cudaStreamSynchronize(st));
@@ -801,7 +966,10 @@ static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const r
             enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
         }
         RUMB_CUDA(cudaMemcpyAsync(res, CW.res.ptr, sizeof(res), cudaMemcpyDeviceToHost, st));
+        unsigned int dev_err = 0;
+        RUMB_CUDA(cudaMemcpyAsync(&dev_err, W.err.ptr, 4, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaStreamSynchronize(st));
+        if (dev_err) fail(RUMB_E_TIMEOUT, "a kernel's bounded wait for its TMA copies gave up");
         L.push_s += secs(tp, Clock::now());
         L.checks++;
         L.phi = std::sqrt(res[R_PHI2]);
@@ -861,10 +1029,22 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
     if (!use32 || par->dtype == RUMB_MIXED) { W64 = &bm_work<double>(c); W64->ensure(n); }
     if (W32) setup_obs<float>(c, CW, W32, *pr, D, st);
     if (W64) setup_obs<double>(c, CW, W64, *pr, D, st);
+    if (W32) RUMB_CUDA(cudaMemsetAsync(W32->err.ptr, 0, 16, st));
+    if (W64) RUMB_CUDA(cudaMemsetAsync(W64->err.ptr, 0, 16, st));
     std::vector<float> d32(C.diag.begin(), C.diag.end());
     if (W32) RUMB_CUDA(cudaMemcpyAsync(W32->diag.ptr, d32.data(), d32.size() * 4, cudaMemcpyHostToDevice, st));
     if (W64) RUMB_CUDA(cudaMemcpyAsync(W64->diag.ptr, C.diag.data(), C.diag.size() * 8, cudaMemcpyHostToDevice, st));
-    // initial state
+    // transform split (tuned once per context, n and dtype), then the initial state
+    BmCoef C64 = C;
+    if (W32) {
+        enqueue_cold_start<float>(*W32, C, n, st);
+        C.lo_bits = tune_lo_bits<float>(c, *W32, C, n, st);
+    }
+    if (W64) {
+        enqueue_cold_start<double>(*W64, C64, n, st);
+        C64.lo_bits = tune_lo_bits<double>(c, *W64, C64, n, st);
+    }
+    if (!W32) C.lo_bits = C64.lo_bits;
     if (use32) {
         if (warm) copy_state_in<float>(*W32, *warm, m2, st);
         else enqueue_cold_start<float>(*W32, C, n, st);
@@ -888,7 +1068,7 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
         if (!done) {
             promote_state(*W32, *W64, m2, st);
             final_dtype64 = true;
-            run_leg<double>(c, CW, *W64, C, *pr, *par, L, t0, false, trace, user);
+            run_leg<double>(c, CW, *W64, C64, *pr, *par, L, t0, false, trace, user);
         }
     } else {
         run_leg<double>(c, CW, *W64, C, *pr, *par, L, t0, false, trace, user);
@@ -939,6 +1119,7 @@ int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, voi
         BmWork<T> &W = bm_work<T>(c);
         W.ensure(n);
         setup_obs<T>(c, CW, &W, *pr, D, st);
+        RUMB_CUDA(cudaMemsetAsync(W.err.ptr, 0, 16, st));
         std::vector<T> dg(C.diag.begin(), C.diag.end());
         RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
         size_t sb = (size_t)m2 * sizeof(T);
@@ -955,7 +1136,10 @@ int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, voi
         RUMB_CUDA(cudaMemcpyAsync(s, W.s.ptr, sb, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaMemcpyAsync(y, W.y.ptr, sb, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaMemcpyAsync(z, W.z.ptr, sb, cudaMemcpyDeviceToHost, st));
+        unsigned int dev_err = 0;
+        RUMB_CUDA(cudaMemcpyAsync(&dev_err, W.err.ptr, 4, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaStreamSynchronize(st));
+        if (dev_err) fail(RUMB_E_TIMEOUT, "a kernel's bounded wait for its TMA copies gave up");
     };
     if (par->dtype == RUMB_F64) run(double());
     else run(float());
@@ -987,8 +1171,11 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         BmWork<T> &W = bm_work<T>(c);
         W.ensure(n);
         setup_obs<T>(c, CW, &W, *pr, D, st);
+        RUMB_CUDA(cudaMemsetAsync(W.err.ptr, 0, 16, st));
         std::vector<T> dg(C.diag.begin(), C.diag.end());
         RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        enqueue_cold_start<T>(W, C, n, st);
+        C.lo_bits = tune_lo_bits<T>(c, W, C, n, st);
         enqueue_cold_start<T>(W, C, n, st);
         for (int i = 0; i < 3; ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
         RUMB_CUDA(cudaStreamSynchronize(st));
@@ -1057,9 +1244,10 @@ int butterfly_host(Ctx &c, int n, int dtype, const void *in, void *out, double a
     c.join_in();
     RUMB_CUDA(cudaMemcpyAsync(S.a.ptr, in, (size_t)m2 * es, cudaMemcpyHostToDevice, st));
     if (dtype == RUMB_F64)
-        bf_transform<double, double>(n, S.a.as<double>(), S.a.as<double>(), a, b, cc, d, st);
+        xf_transform<double, double>(n, S.a.as<double>(), S.a.as<double>(), Co<double>{a, b, cc, d}, st);
     else
-        bf_transform<float, float>(n, S.a.as<float>(), S.a.as<float>(), (float)a, (float)b, (float)cc, (float)d, st);
+        xf_transform<float, float>(n, S.a.as<float>(), S.a.as<float>(),
+                                   Co<float>{(float)a, (float)b, (float)cc, (float)d}, st);
     RUMB_CUDA(cudaMemcpyAsync(out, S.a.ptr, (size_t)m2 * es, cudaMemcpyDeviceToHost, st));
     RUMB_CUDA(cudaStreamSynchronize(st));
     c.join_out();

@@ -27,6 +27,7 @@ struct Ctx {
     std::unique_ptr<BmWorkBase> bm64, bm32;     // BM-ADMM workspaces
     std::unique_ptr<BmWorkBase> cert;           // float64 certificate workspace
     std::unique_ptr<BmWorkBase> scratch;        // primitive calls' scratch
+    std::map<std::pair<int, int>, int> lo_bits; // tuned low-window size per (n, state bytes)
 
     // Make the context's stream wait for the caller's stream (call start) ...
     void join_in() {
