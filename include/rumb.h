@@ -128,8 +128,9 @@ typedef struct {
     double lb_target;    /* stop once lb >= lb_target (NaN: none) */
     int dtype;           /* RUMB_F64, RUMB_F32 or RUMB_MIXED */
     int use_graph;       /* 1: replay each check interval as one CUDA graph */
-    int stall_checks;    /* RUMB_MIXED: checks without progress before float64 takes over */
-    double stall_rtol;   /* RUMB_MIXED: relative progress that counts */
+    int stall_checks;    /* RUMB_MIXED: window of checks over which the gap must keep shrinking */
+    double stall_rtol;   /* RUMB_MIXED: float64 takes over once the gap shrank by less than this
+                            fraction over the last stall_checks checks */
 } rumb_bm_params;
 
 typedef struct {

@@ -440,7 +440,11 @@ static CertWork &cert_work(Ctx &c) {
 
 // UB part of a check: x2 (dtype T) -> q = Mobius -> push -> zeta -> ub_now, pfit; running best.
 template <class T>
-static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t st) {
+static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t st, const double *p_ovr = nullptr,
+                         double *res_ovr = nullptr) {
+    const double *pp = p_ovr ? p_ovr : W.p.as<double>();
+    double *rr = res_ovr ? res_ovr : W.res.as<double>();
+    const bool commit = res_ovr == nullptr;            // batched draws keep no p_fit
     ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
     const double eps = 1e-12;
     double *qa = W.qa.as<double>(), *qb = W.qb.as<double>();
@@ -462,24 +466,27 @@ static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t s
                                                       eps);
     RUMB_LAUNCH("extract_kernel");
     xf_transform<double, double>(n, qb, qa, Co<double>{1.0, 1.0, 0.0, 1.0}, st);  // zeta -> x_ub in qa
-    ub_eval_kernel<<<1, RED_THREADS, 0, st>>>(qa, W.obs.as<ll>(), W.p.as<double>(), W.mp,
-                                              W.pfit_cur.as<double>(), W.res.as<double>());
+    ub_eval_kernel<<<1, RED_THREADS, 0, st>>>(qa, W.obs.as<ll>(), pp, W.mp, W.pfit_cur.as<double>(), rr);
     RUMB_LAUNCH("ub_eval_kernel");
-    ub_commit_kernel<<<grid_for(W.mp, 256), 256, 0, st>>>(W.pfit_cur.as<double>(), W.pfit_best.as<double>(), W.mp,
-                                                         W.res.as<double>());
-    RUMB_LAUNCH("ub_commit_kernel");
-    ub_best_kernel<<<1, 32, 0, st>>>(W.res.as<double>());
+    if (commit) {
+        ub_commit_kernel<<<grid_for(W.mp, 256), 256, 0, st>>>(W.pfit_cur.as<double>(), W.pfit_best.as<double>(), W.mp,
+                                                             rr);
+        RUMB_LAUNCH("ub_commit_kernel");
+    }
+    ub_best_kernel<<<1, 32, 0, st>>>(rr);
     RUMB_LAUNCH("ub_best_kernel");
 }
 
 // phi (and the LB's residual sums); with_lb also scatters g and runs the longest path.
 template <class T>
-static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_lb, cudaStream_t st) {
+static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_lb, cudaStream_t st,
+                             const double *p_ovr = nullptr, double *res_ovr = nullptr) {
+    const double *pp = p_ovr ? p_ovr : W.p.as<double>();
+    double *rr = res_ovr ? res_ovr : W.res.as<double>();
     ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
     double *g = W.qb.as<double>();
     if (with_lb) RUMB_CUDA(cudaMemsetAsync(g, 0, (size_t)m2 * 8, st));
-    obs_stats_kernel<T><<<1, RED_THREADS, 0, st>>>(x2, W.obs.as<ll>(), W.p.as<double>(), W.mp,
-                                                   with_lb ? g : nullptr, W.res.as<double>());
+    obs_stats_kernel<T><<<1, RED_THREADS, 0, st>>>(x2, W.obs.as<ll>(), pp, W.mp, with_lb ? g : nullptr, rr);
     RUMB_LAUNCH("obs_stats_kernel");
     if (!with_lb) return;
     xf_transform<double, double>(n, g, g, Co<double>{1.0, 0.0, 1.0, 1.0}, st);    // subset sums
@@ -494,7 +501,7 @@ static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_
         lpath_layer_kernel<<<grid_for(ns, 256), 256, 0, st>>>(g, dp, nodes + lo, ns, n, Nloc);
         RUMB_LAUNCH("lpath_layer_kernel");
     }
-    lb_final_kernel<<<1, 1, 0, st>>>(dp, N, W.res.as<double>());
+    lb_final_kernel<<<1, 1, 0, st>>>(dp, N, rr);
     RUMB_LAUNCH("lb_final_kernel");
 }
 
@@ -574,9 +581,9 @@ static BmCoef make_coef(int n, double beta, double alpha, double p) {
 }
 
 template <class T>
-static void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st) {
+static void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots = 1) {
     size_t smem = prox_tile_smem<T>(P.n);
-    unsigned grid = (unsigned)(1LL << (P.n - PT_M));
+    dim3 grid((unsigned)(1LL << (P.n - PT_M)), (unsigned)slots);
 #define RUMB_PT_CASE(NN)                                                                                   \
     if (P.n <= NN) {                                                                                       \
         static bool attr = false;                                                                          \
@@ -611,15 +618,36 @@ static void enqueue_iteration_small(BmWork<T> &W, const BmCoef &C, int n, cudaSt
     RUMB_LAUNCH("sy_update_kernel");
 }
 
-// One ADMM iteration: 4 register-tiled transform passes (or 1 for n <= 13, more for n >= 21)
-// and the fused prox.
+// Device pointers of one or more draws' ADMM state (slots of bstride elements, grid.y = slot).
 template <class T>
-static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
-    T *x2 = W.x2.template as<T>(), *s = W.s.template as<T>(), *y = W.y.template as<T>(), *z = W.z.template as<T>();
-    T *x = W.x.template as<T>(), *Ax = W.Ax.template as<T>(), *t1 = W.t1.template as<T>(), *t2 = W.t2.template as<T>();
-    if (n - 1 < 5) {
-        enqueue_iteration_small<T>(W, C, n, st);
-    } else {
+struct IterPtrs {
+    T *x2, *s, *y, *z, *x, *Ax, *t1, *t2;
+    const T *xhat, *diag;
+    const uint32_t *menu_obs;
+    unsigned int *err;
+    int slots = 1;
+    ll bstride = 0;
+    const int *active = nullptr;
+};
+
+template <class T>
+static IterPtrs<T> iter_ptrs(BmWork<T> &W) {
+    IterPtrs<T> P;
+    P.x2 = W.x2.template as<T>(); P.s = W.s.template as<T>(); P.y = W.y.template as<T>(); P.z = W.z.template as<T>();
+    P.x = W.x.template as<T>(); P.Ax = W.Ax.template as<T>(); P.t1 = W.t1.template as<T>(); P.t2 = W.t2.template as<T>();
+    P.xhat = W.xhat.template as<T>(); P.diag = W.diag.template as<T>();
+    P.menu_obs = W.menu_obs.template as<uint32_t>();
+    P.err = W.err.template as<unsigned int>();
+    return P;
+}
+
+// One ADMM iteration: 4 register-tiled transform passes (or 1 for n <= 13, more for n >= 21)
+// and the fused prox, for every slot of I (n >= 8).
+template <class T>
+static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n, cudaStream_t st) {
+    T *x2 = I.x2, *s = I.s, *y = I.y, *z = I.z, *x = I.x, *Ax = I.Ax, *t1 = I.t1, *t2 = I.t2;
+    const int K = I.slots;
+    {
         T p = (T)C.p;
         Co<T> kA{(T)1, (T)0, (T)-1, p};                                    // A' (sign folded)
         Co<T> kQt{(T)C.Qt[0], (T)C.Qt[1], (T)C.Qt[2], (T)C.Qt[3]};
@@ -629,57 +657,69 @@ static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t
         XfArgs<T, T> base{};
         base.Nloc = 1LL << (n - 1);
         base.b1 = (T)C.b1; base.b2 = (T)C.b2; base.ib1 = (T)C.ib1; base.alpha = (T)C.alpha;
-        base.diag = W.diag.template as<T>();
+        base.diag = I.diag;
+        base.bstride = I.bstride;
+        base.active = I.active;
         auto at = [&](const XfShape &sh) { XfArgs<T, T> A = base; A.s0 = sh.s0; A.B = sh.B; return A; };
         const size_t m = plan.size() - 1;                                  // high windows
         if (m == 0) {
             XfArgs<T, T> A = at(plan[0]);
             A.y = y; A.s = s; A.z = z; A.x2 = x2; A.out = x; A.s_io = s; A.y_io = y;
             A.k1 = kA; A.k2 = kQt; A.k3 = kQ; A.k4 = kAQ;
-            xf_launch<T, T, K_FULL>(A, plan[0], n, st);
+            xf_launch<T, T, K_FULL>(A, plan[0], n, st, K);
         } else {
             { XfArgs<T, T> A = at(plan[0]); A.y = y; A.s = s; A.out = t1; A.k1 = kA;
-              xf_launch<T, T, K_P1>(A, plan[0], n, st); }
+              xf_launch<T, T, K_P1>(A, plan[0], n, st, K); }
             for (size_t i = 1; i < m; ++i) {
                 XfArgs<T, T> A = at(plan[i]); A.in = t1; A.out = t1; A.k1 = kA;
-                xf_launch<T, T, K_PLAIN>(A, plan[i], n, st);
+                xf_launch<T, T, K_PLAIN>(A, plan[i], n, st, K);
             }
             { XfArgs<T, T> A = at(plan[m]); A.in = t1; A.out = t2; A.z = z; A.x2 = x2; A.k1 = kA; A.k2 = kQt;
-              xf_launch<T, T, K_P2>(A, plan[m], n, st); }
+              xf_launch<T, T, K_P2>(A, plan[m], n, st, K); }
             for (size_t i = 1; i < m; ++i) {
                 XfArgs<T, T> A = at(plan[i]); A.in = t2; A.out = t2; A.k1 = kQt;
-                xf_launch<T, T, K_PLAIN>(A, plan[i], n, st);
+                xf_launch<T, T, K_PLAIN>(A, plan[i], n, st, K);
             }
             { XfArgs<T, T> A = at(plan[0]); A.in = t2; A.out = x; A.out2 = Ax; A.k1 = kQt; A.k2 = kQ; A.k3 = kAQ;
-              xf_launch<T, T, K_P3>(A, plan[0], n, st); }
+              xf_launch<T, T, K_P3>(A, plan[0], n, st, K); }
             for (size_t i = 1; i < m; ++i) {
                 XfArgs<T, T> A = at(plan[i]); A.in = x; A.in2 = Ax; A.out = x; A.out2 = Ax; A.k1 = kQ; A.k3 = kAQ;
-                xf_launch<T, T, K_DUAL>(A, plan[i], n, st);
+                xf_launch<T, T, K_DUAL>(A, plan[i], n, st, K);
             }
             { XfArgs<T, T> A = at(plan[m]); A.in = x; A.in2 = Ax; A.out = x; A.s_io = s; A.y_io = y; A.k1 = kQ;
               A.k3 = kAQ;
-              xf_launch<T, T, K_P4>(A, plan[m], n, st); }
+              xf_launch<T, T, K_P4>(A, plan[m], n, st, K); }
         }
     }
     // fused prox + z + x2
+    ProxTileArgs<T> P{};
+    P.n = n;
+    P.Nloc = 1LL << (n - 1);
+    P.x = x; P.x2 = x2; P.z = z;
+    P.xhat = I.xhat;
+    P.menu_obs = I.menu_obs;
+    P.alpha = (T)C.alpha; P.b2 = (T)C.b2; P.ib2 = (T)C.ib2;
+    P.inv_c0 = (T)(1.0 / C.b2); P.inv_c1 = (T)(1.0 / (C.b2 + 2.0));
+    P.err = I.err;
+    P.bstride = I.bstride;
+    P.active = I.active;
+    if (g_prof) {
+        double S = (double)P.Nloc * n * K, e = sizeof(T);
+        prof_begin(e == 8 ? "prox_tile<f64>" : "prox_tile<f32>", 5.0 * S * e + 4.0 * (1LL << n), st);
+    }
+    launch_prox_tile<T>(P, st, K);
+    prof_end(st);
+}
+
+template <class T>
+static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
     if (n >= PT_M + 1) {
-        ProxTileArgs<T> P{};
-        P.n = n;
-        P.Nloc = 1LL << (n - 1);
-        P.x = x; P.x2 = x2; P.z = z;
-        P.xhat = W.xhat.template as<T>();
-        P.menu_obs = W.menu_obs.template as<uint32_t>();
-        P.alpha = (T)C.alpha; P.b2 = (T)C.b2; P.ib2 = (T)C.ib2;
-        P.inv_c0 = (T)(1.0 / C.b2); P.inv_c1 = (T)(1.0 / (C.b2 + 2.0));
-        P.err = W.err.template as<unsigned int>();
-        if (g_prof) {
-            double S = (double)P.Nloc * n, e = sizeof(T);
-            prof_begin(e == 8 ? "prox_tile<f64>" : "prox_tile<f32>", 5.0 * S * e + 4.0 * (1LL << n), st);
-        }
-        launch_prox_tile<T>(P, st);
-        prof_end(st);
+        enqueue_iteration_ptrs<T>(iter_ptrs<T>(W), C, n, st);
         return;
     }
+    // small lattices: separate butterflies and the thread-per-menu prox
+    enqueue_iteration_small<T>(W, C, n, st);
+    T *x2 = W.x2.template as<T>(), *z = W.z.template as<T>(), *x = W.x.template as<T>();
     ProxArgs<T> P{};
     P.n = n;
     P.Nloc = 1LL << (n - 1);
@@ -913,8 +953,7 @@ struct LoopState {
     double ub = INFINITY, lb = 0.0, phi = NAN;
     int stop = RUMB_STOP_MAX_ITER;
     double push_s = 0.0;
-    double best_prog = -INFINITY;
-    int n_flat = 0;
+    std::vector<double> gaps;   // mixed mode: the bracket's gap at every check
 };
 
 template <class T>
@@ -985,14 +1024,11 @@ static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const r
         if (par.abs_tol >= 0 && gap <= par.abs_tol) { L.stop = RUMB_STOP_GAP_ABS; return true; }
         if (par.rel_tol >= 0 && L.lb > 0 && gap / L.lb <= par.rel_tol) { L.stop = RUMB_STOP_GAP_REL; return true; }
         if (stall_exit) {
-            // progress = -ub (falls); a float32 state stops improving at its rounding floor
-            double prog = -L.ub;
-            if (L.best_prog == -INFINITY || prog > L.best_prog * (1.0 + (L.best_prog > 0 ? 1 : -1) * par.stall_rtol)) {
-                L.best_prog = prog;
-                L.n_flat = 0;
-            } else if (++L.n_flat >= par.stall_checks) {
-                return false;
-            }
+            // A float32 state's bracket stops closing at its rounding floor: hand over to float64
+            // once the gap has shrunk by less than stall_rtol over the last stall_checks checks.
+            L.gaps.push_back(gap);
+            size_t W = (size_t)(par.stall_checks > 0 ? par.stall_checks : 1);
+            if (L.gaps.size() > W && gap > (1.0 - par.stall_rtol) * L.gaps[L.gaps.size() - 1 - W]) return false;
         }
     }
     L.stop = RUMB_STOP_MAX_ITER;

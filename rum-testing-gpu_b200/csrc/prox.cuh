@@ -78,6 +78,8 @@ struct ProxTileArgs {
     T alpha, b2, ib2;
     T inv_c0, inv_c1;           // 1 / b2 and 1 / (b2 + 2): the curvatures of unobserved / observed
     unsigned int *err;
+    ll bstride;                 // batched draws: elements between draws' slabs (grid.y = slot)
+    const int *active;          // batched draws: slot flags (nullptr: every slot runs)
 };
 
 // Largest tile (elements per array): m 2^(m-1) + (n - m) 2^m.
@@ -109,6 +111,14 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
     extern __shared__ __align__(128) unsigned char pt_smem[];
     uint64_t *mbar = reinterpret_cast<uint64_t *>(pt_smem);
     int *roff = reinterpret_cast<int *>(pt_smem + 16);     // run offsets (elements), n <= 30
+    if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
+    {
+        const ll boff = (ll)blockIdx.y * P.bstride;
+        P.x += boff;
+        P.x2 += boff;
+        P.z += boff;
+        P.xhat += boff;
+    }
     const int n = P.n, tid = threadIdx.x, lane = tid & 31;
     const ll Nloc = P.Nloc;
     const ll E_max = prox_tile_elems(n);

@@ -148,6 +148,8 @@ struct XfArgs {
     T b1, b2, ib1, alpha;
     ll Nloc;
     int s0, B;          // window
+    ll bstride;         // batched draws: elements between consecutive draws' slabs (grid.y = draw slot)
+    const int *active;  // batched draws: slot flags (nullptr: every slot runs)
 };
 
 template <class T, int L, int RB, int WB>
@@ -174,12 +176,14 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
     const ll tile = blockIdx.x;
     const int s0 = A.s0, B = A.B;
     const ll Nloc = A.Nloc;
+    if (A.active && !A.active[blockIdx.y]) return;          // a retired slot (uniform per CTA)
+    const ll boff = (ll)blockIdx.y * A.bstride;
     T v[R];
     if (KIND == K_P4 || KIND == K_DUAL) {
         T u[R], ss[KIND == K_P4 ? R : 1], yy[KIND == K_P4 ? R : 1];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
             v[j] = (T)A.in[g];
             u[j] = A.in2[g];
         }
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
 #pragma unroll
             for (int j = 0; j < R; ++j) {
                 int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
-                ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+                ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
                 ss[j] = A.s_io[g];
                 yy[j] = A.y_io[g];
             }
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
             A.out[g] = v[j];
             if (KIND == K_DUAL) {
                 A.out2[g] = u[j];
@@ -217,7 +221,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
     T zz[(KIND == K_P2 || KIND == K_FULL) ? R : 1], xx[(KIND == K_P2 || KIND == K_FULL) ? R : 1];
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-        ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+        ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
         if (KIND == K_P1 || KIND == K_FULL) v[j] = A.y[g] - A.b1 * A.s[g];
         else v[j] = (T)A.in[g];
     }
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
             zz[j] = A.z[g];
             xx[j] = A.x2[g];
         }
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
-            A.out[xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane)] = v[j];
+            A.out[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane)] = v[j];
         }
         return;
     }
@@ -248,14 +252,14 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
         if (KIND == K_P2) {
 #pragma unroll
             for (int j = 0; j < R; ++j)
-                A.out[xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane)] = v[j];
+                A.out[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane)] = v[j];
             return;
         }
         // K_FULL: diag, then Q and (A Q) forward, x and the s/y update (layout A -> B)
         T u[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
             v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
             u[j] = v[j];
         }
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
             A.out[g] = v[j];
             T ax = u[j], sv = A.s_io[g], yv = A.y_io[g];
             T one = (T)1;
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
             v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
             u[j] = v[j];
         }
@@ -289,7 +293,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
         xf_backward<T, L, RB, WB>(u, sm, w, lane, A.k3);
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            ll g = xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
             A.out[g] = v[j];
             A.out2[g] = u[j];
         }
@@ -326,7 +330,7 @@ inline std::vector<XfShape> xf_plan(int nb, int lo_bits = 12) {
 }
 
 template <class T, class TI, int L, int RB, int WB, int KIND>
-inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st) {
+inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st, int slots = 1) {
     static bool attr = false;
     size_t smem = (size_t)sizeof(T) << (RB + WB + 5);
     if (!attr) {
@@ -336,7 +340,7 @@ inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st) {
     }
     ll tiles = (A.Nloc >> (L ? A.B : A.B + 5)) * n;
     if (g_prof) {
-        double S = (double)A.Nloc * n, e = sizeof(T), ei = sizeof(TI);
+        double S = (double)A.Nloc * n * slots, e = sizeof(T), ei = sizeof(TI);
         double bytes = S * e;                                          // one output
         switch (KIND) {
             case K_PLAIN: bytes += S * ei; break;
@@ -352,16 +356,16 @@ inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st) {
         snprintf(nm, sizeof nm, "xform<%s,%s>[s=%d,B=%d]", sizeof(T) == 8 ? "f64" : "f32", kn[KIND], A.s0, A.B);
         prof_begin(nm, bytes, st);
     }
-    xform_pass<T, TI, L, RB, WB, KIND><<<(unsigned)tiles, 32 << WB, smem, st>>>(A);
+    xform_pass<T, TI, L, RB, WB, KIND><<<dim3((unsigned)tiles, (unsigned)slots), 32 << WB, smem, st>>>(A);
     RUMB_LAUNCH("xform_pass");
     prof_end(st);
 }
 
 template <class T, class TI, int KIND>
-inline void xf_launch(const XfArgs<T, TI> &A, const XfShape &sh, int n, cudaStream_t st) {
+inline void xf_launch(const XfArgs<T, TI> &A, const XfShape &sh, int n, cudaStream_t st, int slots = 1) {
 #define XF_CASE(LL, RBB, WBB)                                                     \
     if (sh.L == LL && sh.RB == RBB && sh.WB == WBB) {                             \
-        xf_launch_one<T, TI, LL, RBB, WBB, KIND>(A, n, st);                        \
+        xf_launch_one<T, TI, LL, RBB, WBB, KIND>(A, n, st, slots);                 \
         return;                                                                   \
     }
     XF_CASE(1, 0, 0) XF_CASE(1, 1, 0) XF_CASE(1, 1, 1) XF_CASE(1, 2, 1) XF_CASE(1, 2, 2) XF_CASE(1, 3, 2)

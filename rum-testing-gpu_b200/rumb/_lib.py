@@ -210,7 +210,7 @@ class Context:
     @staticmethod
     def bm_params(beta, alpha=1.95, precond_p=math.sqrt(2.0), check=50, lb_every=1, max_iter=10 ** 7,
                   abs_tol=1e-5, rel_tol=1e-4, time_limit=0.0, ub_target=None, lb_target=None, dtype="float64",
-                  use_graph=True, stall_checks=3, stall_rtol=1e-3):
+                  use_graph=True, stall_checks=20, stall_rtol=0.05):
         P = BMParams()
         P.beta, P.alpha, P.precond_p = float(beta), float(alpha), float(precond_p)
         P.check, P.lb_every, P.max_iter = int(check), int(lb_every), int(max_iter)
