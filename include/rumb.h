@@ -68,6 +68,7 @@ extern "C" {
 #define RUMB_STOP_UB_TARGET 5
 #define RUMB_STOP_LB_TARGET 6
 #define RUMB_STOP_CANCEL 7
+#define RUMB_STOP_STALL 8    /* float32 state (RUMB_F32, stall_checks > 0): the bracket stopped closing */
 
 typedef struct rumb_ctx rumb_ctx;
 typedef struct rumb_bm_state rumb_bm_state;
@@ -128,9 +129,11 @@ typedef struct {
     double lb_target;    /* stop once lb >= lb_target (NaN: none) */
     int dtype;           /* RUMB_F64, RUMB_F32 or RUMB_MIXED */
     int use_graph;       /* 1: replay each check interval as one CUDA graph */
-    int stall_checks;    /* RUMB_MIXED: window of checks over which the gap must keep shrinking */
-    double stall_rtol;   /* RUMB_MIXED: float64 takes over once the gap shrank by less than this
-                            fraction over the last stall_checks checks */
+    int stall_checks;    /* float32 state: window of checks over which the gap must keep shrinking
+                            (RUMB_F32 with 0: no stall test) */
+    double stall_rtol;   /* float32 state: once the gap shrank by less than this fraction over the
+                            last stall_checks checks, RUMB_MIXED hands over to float64 and
+                            RUMB_F32 stops with RUMB_STOP_STALL */
 } rumb_bm_params;
 
 typedef struct {
@@ -159,6 +162,33 @@ RUMB_API int rumb_bm_state_destroy(rumb_bm_state *st);
  * = 0. For iterate-level parity checks. */
 RUMB_API int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, void *x2,
                     void *s, void *y, void *z, int iters, int cold_start);
+
+/* ---------------------------------------------------------------- batched draws */
+typedef struct {
+    int slots;            /* draws resident at once; 0 = as many as fit mem_fraction of free memory */
+    double mem_fraction;  /* share of free device memory the slots may take (0 = 0.8) */
+    double draw_time;     /* seconds per draw (<= 0: none) */
+} rumb_batch_params;
+
+typedef struct {
+    int slots;            /* draws resident at once */
+    double bytes_per_slot;
+    long long total_iters;/* slot-iterations run */
+    double setup_s, solve_s, device_ms;
+    int lo_bits;          /* transform split used */
+} rumb_batch_info;
+
+/* B draws of one menu structure (prob->menu, prob->alt; prob->p is the structure's reference
+ * point and is not solved), each to the certified bracket of par (abs_tol / rel_tol / max_iter,
+ * dtype RUMB_F32 or RUMB_F64; a float32 draw whose gap stops shrinking ends with RUMB_STOP_STALL),
+ * with per-draw thresholds below[b] (stop once ub <= below) and above[b] (stop once lb >= above),
+ * NaN or NULL for none. P is B x mp row-major (host). Every draw starts from warm (e.g. the kept
+ * state of p_hat's solve) or from the cold start. res[B] receives each draw's bracket.
+ * The bootstrap's per-draw solves (solver/inference/bootstrap.py:308-335) run here together. */
+RUMB_API int rumb_bm_solve_batch(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par,
+                                 const rumb_batch_params *bp, int B, const double *P, const double *below,
+                                 const double *above, const rumb_bm_state *warm, rumb_bm_result *res,
+                                 rumb_batch_info *info);
 
 /* ---------------------------------------------------------------- Flow-CG pricing */
 /* pricing storage of the lattice values */

@@ -85,6 +85,8 @@ int rumb_ctx_destroy(rumb_ctx *ctx) {
         cudaStreamSynchronize(ctx->c.own);
         ctx->c.bm64.reset();
         ctx->c.bm32.reset();
+        ctx->c.batch64.reset();
+        ctx->c.batch32.reset();
         ctx->c.cert.reset();
         ctx->c.scratch.reset();
         ctx->c.layers.clear();
@@ -187,6 +189,15 @@ int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_pa
     if (!x2 || !s || !y || !z) rumb::fail(RUMB_E_INVAL, "state buffers must not be NULL");
     if (iters < 0) rumb::fail(RUMB_E_INVAL, "iters must be >= 0");
     return rumb::bm_iterate(ctx->c, prob, par, x2, s, y, z, iters, cold_start);
+    RUMB_API_END
+}
+
+int rumb_bm_solve_batch(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par,
+                        const rumb_batch_params *bp, int B, const double *P, const double *below, const double *above,
+                        const rumb_bm_state *warm, rumb_bm_result *res, rumb_batch_info *info) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::bm_solve_batch(ctx->c, prob, par, bp, B, P, below, above, warm, res, info);
     RUMB_API_END
 }
 

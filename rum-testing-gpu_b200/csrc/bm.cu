@@ -20,6 +20,7 @@
 // active-set iteration in registers instead of an insertion sort.
 #include <chrono>
 #include <cstring>
+#include <string>
 
 #include "bfly.cuh"
 #include "xform.cuh"
@@ -1100,11 +1101,15 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
     LoopState L;
     bool final_dtype64 = !use32;
     if (use32) {
-        bool done = run_leg<float>(c, CW, *W32, C, *pr, *par, L, t0, par->dtype == RUMB_MIXED, trace, user);
-        if (!done) {
+        // a float32 state stops at its rounding floor: mixed hands over to float64, float32 ends
+        bool stall_exit = par->dtype == RUMB_MIXED || par->stall_checks > 0;
+        bool done = run_leg<float>(c, CW, *W32, C, *pr, *par, L, t0, stall_exit, trace, user);
+        if (!done && par->dtype == RUMB_MIXED) {
             promote_state(*W32, *W64, m2, st);
             final_dtype64 = true;
             run_leg<double>(c, CW, *W64, C64, *pr, *par, L, t0, false, trace, user);
+        } else if (!done) {
+            L.stop = RUMB_STOP_STALL;
         }
     } else {
         run_leg<double>(c, CW, *W64, C, *pr, *par, L, t0, false, trace, user);
@@ -1257,6 +1262,284 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
     *count = k;
     c.join_out();
     return RUMB_OK;
+}
+
+// ================================================================= batched draws
+// Many draws of one menu structure (the bootstrap's perturbed points) solved together: K slots of
+// ADMM state live side by side (slot k at k * S), one CUDA graph advances every active slot by a
+// check interval (grid.y = slot, retired slots skip their CTAs), each active slot then gets its
+// float64 check, and the host retires finished draws and refills their slots from the queue.
+// Slots are admitted by device memory: K = min(B, mem_fraction * free / bytes per slot).
+
+__global__ void scatter_rows_kernel(const ll *obs, const double *p, ll mp, double *p_dst, float *xf, double *xd) {
+    ll j = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (j >= mp) return;
+    double v = p[j];
+    p_dst[j] = v;
+    if (xf) xf[obs[j]] = (float)v;
+    if (xd) xd[obs[j]] = v;
+}
+
+template <class T>
+struct BatchWork : public BmWorkBase {
+    DevBuf x2, s, y, z, x, Ax, t1, t2, xhat;   // K slabs each
+    DevBuf obsbits, menu_obs, diag, err, active, p, res;
+    int K = 0, n = 0;
+    ll mp = 0;
+    void ensure(int n_, ll mp_, int K_) {
+        n = n_; mp = mp_; K = K_;
+        ll m2 = (ll)n << (n - 1);
+        size_t sb = (size_t)m2 * sizeof(T) * (size_t)K;
+        for (DevBuf *b : {&x2, &s, &y, &z, &x, &Ax, &t1, &t2, &xhat}) b->ensure(sb);
+        obsbits.ensure((size_t)((m2 + 31) / 32) * 4);
+        menu_obs.ensure((size_t)4 << n);
+        diag.ensure(64 * sizeof(T));
+        err.ensure(16);
+        active.ensure((size_t)K * 4);
+        p.ensure((size_t)K * (size_t)mp * 8);
+        res.ensure((size_t)K * R_SLOTS * 8);
+    }
+};
+
+template <class T>
+static size_t batch_slot_bytes(int n, ll mp) {
+    ll m2 = (ll)n << (n - 1);
+    return (size_t)9 * (size_t)m2 * sizeof(T) + (size_t)mp * 8 + R_SLOTS * 8;
+}
+
+template <class T>
+static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_batch_params *bp,
+                            int B, const double *P, const double *below, const double *above, const rumb_bm_state *warm,
+                            rumb_bm_result *out, rumb_batch_info *info) {
+    const int n = pr->n;
+    const ll mp = pr->mp, m2 = (ll)n << (n - 1);
+    cudaStream_t st = c.own;
+    auto t0 = Clock::now();
+    // slots by memory
+    size_t fr = 0, tot = 0;
+    RUMB_CUDA(cudaMemGetInfo(&fr, &tot));
+    double frac = (bp && bp->mem_fraction > 0) ? bp->mem_fraction : 0.8;
+    size_t per = batch_slot_bytes<T>(n, mp);
+    CertWork &CW = cert_work(c);
+    CW.ensure(n, mp);
+    RUMB_CUDA(cudaMemGetInfo(&fr, &tot));
+    ll fit = (ll)((double)fr * frac / (double)per);
+    int K = (bp && bp->slots > 0) ? bp->slots : (int)std::min<ll>(fit, 256);
+    K = std::max(1, std::min(K, B));
+    if ((ll)K > fit && fit >= 1) K = (int)fit;
+    if (fit < 1) fail(RUMB_E_OOM, "one draw's state does not fit the free device memory");
+    std::unique_ptr<BmWorkBase> &slot = sizeof(T) == 8 ? c.batch64 : c.batch32;
+    if (!slot) slot.reset(new BatchWork<T>());
+    BatchWork<T> &W = *static_cast<BatchWork<T> *>(slot.get());
+    W.ensure(n, mp, K);
+    // shared structure: observed positions, bits, per-menu masks, diagonal
+    DevProblem D;
+    upload_problem(*pr, D, st);
+    BmCoef C = make_coef(n, par->beta, par->alpha, par->precond_p);
+    {
+        DevBuf bad;
+        bad.ensure(4);
+        RUMB_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, st));
+        RUMB_CUDA(cudaMemsetAsync(W.xhat.ptr, 0, (size_t)m2 * sizeof(T) * K, st));
+        RUMB_CUDA(cudaMemsetAsync(W.obsbits.ptr, 0, (size_t)((m2 + 31) / 32) * 4, st));
+        obs_setup_kernel<T><<<grid_for(mp, 256), 256, 0, st>>>(D.d_menu, D.d_alt, D.d_p, mp, n, 1LL << (n - 1),
+                                                               CW.obs.as<ll>(), W.xhat.template as<T>(),
+                                                               W.obsbits.template as<uint32_t>(), bad.as<int>());
+        RUMB_LAUNCH("obs_setup_kernel");
+        menu_obs_kernel<<<grid_for(1LL << n, 256), 256, 0, st>>>(W.obsbits.template as<uint32_t>(), n, 1LL << (n - 1),
+                                                               W.menu_obs.template as<uint32_t>());
+        RUMB_LAUNCH("menu_obs_kernel");
+        int hbad = 0;
+        RUMB_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        if (hbad) fail(RUMB_E_INVAL, "an observed row's alternative is not in its menu, or its menu is a singleton");
+        std::vector<T> dg(C.diag.begin(), C.diag.end());
+        RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        RUMB_CUDA(cudaMemsetAsync(W.err.ptr, 0, 16, st));
+    }
+    IterPtrs<T> I;
+    I.x2 = W.x2.template as<T>(); I.s = W.s.template as<T>(); I.y = W.y.template as<T>(); I.z = W.z.template as<T>();
+    I.x = W.x.template as<T>(); I.Ax = W.Ax.template as<T>(); I.t1 = W.t1.template as<T>(); I.t2 = W.t2.template as<T>();
+    I.xhat = W.xhat.template as<T>(); I.diag = W.diag.template as<T>();
+    I.menu_obs = W.menu_obs.template as<uint32_t>();
+    I.err = W.err.template as<unsigned int>();
+    I.slots = K;
+    I.bstride = m2;
+    I.active = W.active.template as<int>();
+    // the transform split tuned on slot 0's single-draw workspace when not known yet
+    {
+        auto key = std::make_pair(n, (int)sizeof(T));
+        if (c.lo_bits.count(key)) C.lo_bits = c.lo_bits[key];
+    }
+    DevBuf pbuf;                                    // the draws' rows, uploaded once
+    pbuf.ensure((size_t)B * (size_t)mp * 8);
+    RUMB_CUDA(cudaMemcpyAsync(pbuf.ptr, P, (size_t)B * (size_t)mp * 8, cudaMemcpyHostToDevice, st));
+    std::vector<int> act(K, 0), draw_of(K, -1);
+    std::vector<ll> it_of(K, 0);
+    std::vector<double> ub_of(K, INFINITY), lb_of(K, 0.0), phi_of(K, NAN);
+    std::vector<int> nlb_of(K, 0), npush_of(K, 0);
+    std::vector<Clock::time_point> t_of(K);
+    std::vector<std::vector<double>> gaps_of(K);
+    int next = 0, done = 0;
+    ll total_iters = 0;
+    auto admit = [&](int k) {
+        if (next >= B) { act[k] = 0; draw_of[k] = -1; return; }
+        int b = next++;
+        draw_of[k] = b; act[k] = 1; it_of[k] = 0; ub_of[k] = INFINITY; lb_of[k] = 0.0; phi_of[k] = NAN;
+        nlb_of[k] = 0; npush_of[k] = 0; gaps_of[k].clear();
+        t_of[k] = Clock::now();
+        double *pk = W.p.template as<double>() + (size_t)k * mp;
+        T *xk = W.xhat.template as<T>() + (size_t)k * m2;
+        scatter_rows_kernel<<<grid_for(mp, 256), 256, 0, st>>>(CW.obs.as<ll>(), pbuf.as<double>() + (size_t)b * mp, mp,
+                                                               pk, sizeof(T) == 4 ? (float *)xk : nullptr,
+                                                               sizeof(T) == 8 ? (double *)xk : nullptr);
+        RUMB_LAUNCH("scatter_rows_kernel");
+        double *rk = W.res.template as<double>() + (size_t)k * R_SLOTS;
+        set_doubles_kernel<<<1, 32, 0, st>>>(rk, R_SLOTS, 0.0);
+        set_doubles_kernel<<<1, 32, 0, st>>>(rk + R_UB_BEST, 1, INFINITY);
+        RUMB_LAUNCH("set_doubles");
+        T *dst[4] = {I.x2 + (size_t)k * m2, I.s + (size_t)k * m2, I.y + (size_t)k * m2, I.z + (size_t)k * m2};
+        if (warm) {
+            const DevBuf *src[4] = {&warm->x2, &warm->s, &warm->y, &warm->z};
+            for (int i = 0; i < 4; ++i) {
+                if ((warm->dtype == RUMB_F64) == (sizeof(T) == 8))
+                    RUMB_CUDA(cudaMemcpyAsync(dst[i], src[i]->ptr, (size_t)m2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
+                else if (warm->dtype == RUMB_F64)
+                    convert_kernel<double, T><<<grid_for(m2, 256), 256, 0, st>>>(src[i]->as<double>(), dst[i], m2);
+                else
+                    convert_kernel<float, T><<<grid_for(m2, 256), 256, 0, st>>>(src[i]->as<float>(), dst[i], m2);
+            }
+            RUMB_LAUNCH("warm copy");
+        } else {
+            ProxArgs<T> Pa{};
+            Pa.n = n; Pa.Nloc = 1LL << (n - 1); Pa.nmenus = (1LL << n) - 1;
+            Pa.v = xk; Pa.out = dst[0]; Pa.xhat = xk;
+            Pa.obsbits = W.obsbits.template as<uint32_t>();
+            Pa.b2 = (T)C.b2;
+            launch_prox_n<T, PROX_ONLY>(Pa, st);
+            for (int i = 1; i < 4; ++i) RUMB_CUDA(cudaMemsetAsync(dst[i], 0, (size_t)m2 * sizeof(T), st));
+        }
+    };
+    for (int k = 0; k < K; ++k) admit(k);
+    RUMB_CUDA(cudaMemcpyAsync(W.active.ptr, act.data(), (size_t)K * 4, cudaMemcpyHostToDevice, st));
+    std::vector<ll> bounds;
+    c.layer_table(n, bounds);
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    auto t_setup = Clock::now();
+    const int chunk = graph_chunk(par->check);
+    Graph g_iter;
+    g_iter.capture(st, [&] { for (int i = 0; i < chunk; ++i) enqueue_iteration_ptrs<T>(I, C, n, st); });
+    std::vector<double> res((size_t)K * R_SLOTS);
+    cudaEvent_t e0, e1;
+    RUMB_CUDA(cudaEventCreate(&e0));
+    RUMB_CUDA(cudaEventCreate(&e1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } eg{e0, e1};
+    RUMB_CUDA(cudaEventRecord(e0, st));
+    while (done < B) {
+        if (c.cancel.load()) fail(RUMB_E_CANCEL, "cancelled");
+        if (par->time_limit > 0 && secs(t0, Clock::now()) > par->time_limit) break;
+        for (int i = 0; i < par->check / chunk; ++i) g_iter.launch(st);
+        int nact = 0;
+        for (int k = 0; k < K; ++k) {
+            if (!act[k]) continue;
+            ++nact;
+            it_of[k] += par->check;
+            const T *x2k = I.x2 + (size_t)k * m2;
+            const double *pk = W.p.template as<double>() + (size_t)k * mp;
+            double *rk = W.res.template as<double>() + (size_t)k * R_SLOTS;
+            bool want_lb = (npush_of[k] % par->lb_every) == 0;
+            enqueue_stats_lb<T>(c, CW, n, x2k, want_lb, st, pk, rk);
+            enqueue_push<T>(c, CW, n, x2k, st, pk, rk);
+        }
+        total_iters += (ll)nact * par->check;
+        RUMB_CUDA(cudaMemcpyAsync(res.data(), W.res.ptr, res.size() * 8, cudaMemcpyDeviceToHost, st));
+        unsigned int dev_err = 0;
+        RUMB_CUDA(cudaMemcpyAsync(&dev_err, W.err.ptr, 4, cudaMemcpyDeviceToHost, st));
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        if (dev_err) fail(RUMB_E_TIMEOUT, "a kernel's bounded wait for its TMA copies gave up");
+        bool changed = false;
+        for (int k = 0; k < K; ++k) {
+            if (!act[k]) continue;
+            const double *r = &res[(size_t)k * R_SLOTS];
+            bool want_lb = (npush_of[k] % par->lb_every) == 0;
+            npush_of[k]++;
+            phi_of[k] = std::sqrt(r[R_PHI2]);
+            ub_of[k] = r[R_UB_BEST];
+            if (want_lb) { nlb_of[k]++; if (r[R_LB_NOW] > lb_of[k]) lb_of[k] = r[R_LB_NOW]; }
+            int b = draw_of[k];
+            int stop = 0;
+            double gap = ub_of[k] - lb_of[k];
+            double bl = below ? below[b] : NAN, ab = above ? above[b] : NAN;
+            if (std::isfinite(bl) && ub_of[k] <= bl) stop = RUMB_STOP_UB_TARGET;
+            else if (std::isfinite(ab) && lb_of[k] >= ab) stop = RUMB_STOP_LB_TARGET;
+            else if (par->abs_tol >= 0 && gap <= par->abs_tol) stop = RUMB_STOP_GAP_ABS;
+            else if (par->rel_tol >= 0 && lb_of[k] > 0 && gap / lb_of[k] <= par->rel_tol) stop = RUMB_STOP_GAP_REL;
+            else if (it_of[k] >= par->max_iter) stop = RUMB_STOP_MAX_ITER;
+            else if (bp && bp->draw_time > 0 && secs(t_of[k], Clock::now()) > bp->draw_time) stop = RUMB_STOP_TIME;
+            else if (par->stall_checks > 0) {
+                // a float32 state's bracket stops closing at its rounding floor
+                gaps_of[k].push_back(gap);
+                size_t Wn = (size_t)par->stall_checks;
+                if (sizeof(T) == 4 && gaps_of[k].size() > Wn &&
+                    gap > (1.0 - par->stall_rtol) * gaps_of[k][gaps_of[k].size() - 1 - Wn])
+                    stop = RUMB_STOP_STALL;
+            }
+            if (!stop) continue;
+            rumb_bm_result &o = out[b];
+            o.lb = lb_of[k]; o.ub = ub_of[k]; o.phi = phi_of[k]; o.iters = it_of[k];
+            o.iters_f32 = sizeof(T) == 4 ? it_of[k] : 0; o.stop = stop; o.n_push = npush_of[k]; o.n_lb = nlb_of[k];
+            o.setup_s = 0.0; o.solve_s = secs(t_of[k], Clock::now()); o.push_s = 0.0;
+            o.per_iter_ms = 0.0; o.device_ms = 0.0;
+            ++done;
+            admit(k);
+            changed = true;
+        }
+        if (changed) RUMB_CUDA(cudaMemcpyAsync(W.active.ptr, act.data(), (size_t)K * 4, cudaMemcpyHostToDevice, st));
+    }
+    // draws left when the time ran out
+    for (int k = 0; k < K; ++k) {
+        if (!act[k] || draw_of[k] < 0) continue;
+        rumb_bm_result &o = out[draw_of[k]];
+        o.lb = lb_of[k]; o.ub = ub_of[k]; o.phi = phi_of[k]; o.iters = it_of[k];
+        o.iters_f32 = sizeof(T) == 4 ? it_of[k] : 0; o.stop = RUMB_STOP_TIME; o.n_push = npush_of[k];
+        o.n_lb = nlb_of[k]; o.solve_s = secs(t_of[k], Clock::now());
+    }
+    for (int b = next; b < B; ++b) {
+        out[b] = rumb_bm_result{};
+        out[b].ub = INFINITY;
+        out[b].stop = RUMB_STOP_TIME;
+    }
+    RUMB_CUDA(cudaEventRecord(e1, st));
+    RUMB_CUDA(cudaEventSynchronize(e1));
+    float dms = 0.f;
+    RUMB_CUDA(cudaEventElapsedTime(&dms, e0, e1));
+    if (info) {
+        info->slots = K;
+        info->bytes_per_slot = (double)per;
+        info->total_iters = total_iters;
+        info->setup_s = secs(t0, t_setup);
+        info->solve_s = secs(t_setup, Clock::now());
+        info->device_ms = dms;
+        info->lo_bits = C.lo_bits;
+    }
+    return RUMB_OK;
+}
+
+int bm_solve_batch(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_batch_params *bp, int B,
+                   const double *P, const double *below, const double *above, const rumb_bm_state *warm,
+                   rumb_bm_result *out, rumb_batch_info *info) {
+    check_problem(pr);
+    check_params(par);
+    if (pr->n < PT_M + 1) fail(RUMB_E_INVAL, "batched draws need n >= 8");
+    if (B < 1 || !P || !out) fail(RUMB_E_INVAL, "B >= 1 draws, P and the results are required");
+    if (warm && warm->n != pr->n) fail(RUMB_E_INVAL, "warm state was kept for another n");
+    c.cancel.store(0);
+    c.join_in();
+    int r;
+    if (par->dtype == RUMB_F64) r = bm_solve_batch_t<double>(c, pr, par, bp, B, P, below, above, warm, out, info);
+    else r = bm_solve_batch_t<float>(c, pr, par, bp, B, P, below, above, warm, out, info);
+    c.join_out();
+    return r;
 }
 
 // ----------------------------------------------------------------- primitives on host slabs

@@ -15,4 +15,7 @@ int fw_lb64_host(Ctx &c, int n, ll mp, const uint32_t *menu, const int32_t *alt,
                  double *lb);
 int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int iters, rumb_kernel_stat *stats,
                int cap, int *count);
+int bm_solve_batch(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_batch_params *bp, int B,
+                   const double *P, const double *below, const double *above, const rumb_bm_state *warm,
+                   rumb_bm_result *out, rumb_batch_info *info);
 }  // namespace rumb

@@ -25,6 +25,7 @@ struct Ctx {
     std::map<int, std::shared_ptr<DevBuf>> layers;
     std::map<int, std::vector<ll>> layer_bounds;
     std::unique_ptr<BmWorkBase> bm64, bm32;     // BM-ADMM workspaces
+    std::unique_ptr<BmWorkBase> batch64, batch32;  // batched-draw workspaces
     std::unique_ptr<BmWorkBase> cert;           // float64 certificate workspace
     std::unique_ptr<BmWorkBase> scratch;        // primitive calls' scratch
     std::map<std::pair<int, int>, int> lo_bits; // tuned low-window size per (n, state bytes)

@@ -163,38 +163,68 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
     const T one = (T)1, two = (T)2;
     const bool mixed = wb != 0 && wb != S;
     const double cw = (double)P.b2 + 2.0, cu = (double)P.b2, icw = 1.0 / cw, icu = 1.0 / cu;
-    double s1 = 0.0, s2 = 0.0;
+    // The previous iterate's support {i : x2_i > 0} is almost always this iteration's: the
+    // threshold is computed on it first and accepted when it satisfies the projection's
+    // optimality conditions (active t_i > tau, inactive t_i <= tau), which make tau unique;
+    // otherwise Michelot's iteration runs from the full set.
+    uint32_t A0 = 0;
+    double s1 = 0.0, s2 = 0.0, f1 = 0.0, f2 = 0.0;
     // pass 1 over the members (set bits of S): xo, v, q = z - b2 xo (kept in sz); the value the
     // threshold works on goes to sx: the equal-curvature value (b2 v + 2 w xh) / (b2 + 2 w) in the
     // state dtype, or v itself for a menu with observed and unobserved members (then t is
-    // b2 v + 2 xh, rebuilt in double where it is read); plus the first active-set sums
+    // b2 v + 2 xh, rebuilt in double where it is read); sums over the previous support (s) and
+    // over all members (f)
     for (uint32_t SS = S; SS; SS &= SS - 1) {
         const int i = __ffs(SS) - 1;
         const int e = roff[i] + (int)((i < PT_M) ? compress_bit(low, i) : low);
-        T xo = P.alpha * sx[e] + (one - P.alpha) * sx2[e];
+        T x2o = sx2[e];
+        T xo = P.alpha * sx[e] + (one - P.alpha) * x2o;
         T zz = sz[e];
         T v = xo - P.ib2 * zz;
         sz[e] = zz - P.b2 * xo;
         const bool w = (wb >> i) & 1u;
         T xh = (T)0;
         if (w) xh = P.xhat[(ll)i * Nloc + (ll)compress_bit(S ^ (1u << i), i)];
-        double ti;
+        double ti, ic = 1.0;
         if (mixed) {
             sx[e] = v;
             ti = (double)P.b2 * (double)v + (w ? 2.0 * (double)xh : 0.0);
-            double ic = w ? icw : icu;
-            s1 += ti * ic;
-            s2 += ic;
+            ic = w ? icw : icu;
         } else {
             T val = (P.b2 * v + two * (w ? one : (T)0) * xh) * (w ? P.inv_c1 : P.inv_c0);
             sx[e] = val;
-            s1 += (double)val;
-            s2 += 1.0;
+            ti = (double)val;
+        }
+        f1 += mixed ? ti * ic : ti;
+        f2 += ic;
+        if (x2o > (T)0) {
+            A0 |= 1u << i;
+            s1 += mixed ? ti * ic : ti;
+            s2 += ic;
         }
     }
     double tau = 0.0;
-    if (k > 1) {
+    bool ok = false;
+    if (k > 1 && A0 != 0) {
+        tau = (s1 - 1.0) / s2;
+        ok = true;
+        for (uint32_t SS = S; SS; SS &= SS - 1) {
+            const int i = __ffs(SS) - 1;
+            const int e = roff[i] + (int)((i < PT_M) ? compress_bit(low, i) : low);
+            double ti = (double)sx[e];
+            if (mixed) {
+                const bool w = (wb >> i) & 1u;
+                ti = (double)P.b2 * ti +
+                     (w ? 2.0 * (double)P.xhat[(ll)i * Nloc + (ll)compress_bit(S ^ (1u << i), i)] : 0.0);
+            }
+            const bool in = (A0 >> i) & 1u;
+            if (in ? !(ti > tau) : (ti > tau)) { ok = false; break; }
+        }
+    }
+    if (k > 1 && !ok) {
         uint32_t A = S;
+        s1 = f1;
+        s2 = f2;
         tau = (s1 - 1.0) / s2;
         for (int round = 0; round < 32; ++round) {
             uint32_t A2 = 0;

@@ -15,7 +15,8 @@ LIB_PATH = os.path.join(os.path.dirname(HERE), "librumb.so")
 
 OK, E_INVAL, E_OOM, E_CUDA, E_TIMEOUT, E_CANCEL, E_NODEV, E_INTERNAL = range(8)
 F64, F32, MIXED = 0, 1, 2
-STOP = {1: "gap_abs", 2: "gap_rel", 3: "time_limit", 4: "max_iter", 5: "ub_target", 6: "lb_target", 7: "cancel"}
+STOP = {1: "gap_abs", 2: "gap_rel", 3: "time_limit", 4: "max_iter", 5: "ub_target", 6: "lb_target", 7: "cancel",
+        8: "stall"}
 DTYPES = {"float64": F64, "float32": F32, "mixed": MIXED}
 
 
@@ -52,6 +53,16 @@ class BMResult(ctypes.Structure):
                 ("device_ms", ctypes.c_double)]
 
 
+class BatchParams(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("mem_fraction", ctypes.c_double), ("draw_time", ctypes.c_double)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("bytes_per_slot", ctypes.c_double), ("total_iters", ctypes.c_longlong),
+                ("setup_s", ctypes.c_double), ("solve_s", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("lo_bits", ctypes.c_int)]
+
+
 class KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 64), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
                 ("bytes_per_launch", ctypes.c_double)]
@@ -79,6 +90,9 @@ _SIGS = {
     "rumb_bm_solve": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, ctypes.POINTER(_vp),
                        ctypes.POINTER(BMResult), _vp, TRACE_FN, _vp], ctypes.c_int),
     "rumb_bm_state_destroy": ([_vp], ctypes.c_int),
+    "rumb_bm_solve_batch": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), ctypes.POINTER(BatchParams),
+                             ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.POINTER(BMResult), ctypes.POINTER(BatchInfo)],
+                            ctypes.c_int),
     "rumb_bm_profile": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), ctypes.c_int,
                          ctypes.POINTER(KernelStat), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "rumb_cg_pricer_create": ([_vp, ctypes.c_int, ctypes.c_longlong, _vp, _vp, ctypes.c_int, ctypes.c_int,
@@ -255,6 +269,29 @@ class Context:
         if trace is not None:
             trace.extend(rows)
         return out, fit, (BMState(kept) if keep and kept.value else None)
+
+    def bm_solve_batch(self, problem, params, P, below=None, above=None, warm=None, slots=0, mem_fraction=0.8,
+                       draw_time=0.0):
+        """Solves the rows of P (B x mp) together; (list of result dicts, info dict)."""
+        pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        if P.ndim != 2 or P.shape[1] != pr.mp:
+            raise ValueError("P must be (B, %d)" % pr.mp)
+        B = P.shape[0]
+        lo = None if below is None else np.ascontiguousarray(np.broadcast_to(below, (B,)), dtype=np.float64)
+        hi = None if above is None else np.ascontiguousarray(np.broadcast_to(above, (B,)), dtype=np.float64)
+        res = (BMResult * B)()
+        info = BatchInfo()
+        bp = BatchParams(int(slots), float(mem_fraction), float(draw_time))
+        check(load().rumb_bm_solve_batch(self.h, ctypes.byref(pr), ctypes.byref(params), ctypes.byref(bp), B, _p(P),
+                                         _p(lo) if lo is not None else None, _p(hi) if hi is not None else None,
+                                         warm.h if warm else None, res, ctypes.byref(info)))
+        out = []
+        for r in res:
+            d = {f: getattr(r, f) for f, _ in BMResult._fields_}
+            d["stop_reason"] = STOP.get(r.stop, "unknown")
+            out.append(d)
+        return out, {f: getattr(info, f) for f, _ in BatchInfo._fields_}
 
     def bm_profile(self, problem, params, iters=20):
         """[dict(name, launches, total_ms, bytes_per_launch)] over `iters` eager iterations."""

@@ -1,0 +1,245 @@
+"""Hong and Li's bootstrap on the RUM distance, with the draws solved many at a time on the GPU.
+
+    from rumb import RUM
+    from rumb.instances import cells_from_panel
+    menu, alt, p_hat = cells_from_panel(n, panel["menu"], panel["chosen"])
+    boot = RUM(menu, alt, p_hat, num_alternatives=n).bootstrap(panel=panel, B=10000)
+    print(boot.p_value())
+
+The reference's pipeline (solver/inference/bootstrap.py:182-335, solver/inference/hong_li.py,
+solver/inference/draws.py:161-290), with its formulas and decisions:
+
+    certify   p_hat with a Session (one plan for every solve), keeping its state and fit:
+              dist(p_hat) in [L0, U0]; the band tau = s [L0, U0], s = 1 + eps_n r_n
+    screen    every draw P_b = p_hat + eps_n r_n (p_hat_b - p_hat): ||p_fit - P_b|| bounds dist(P_b)
+    solve     the draws still open, warm from p_hat's state, each stopping once it clears the band
+              (ub < tau_lo: below; lb >= tau_hi: above). bm_admm solves them together with
+              rumb_bm_solve_batch (slots admitted by device memory, retired as they finish);
+              flow_cg one at a time through the Session, as the reference does. A float32 or mixed
+              session solves the batch in float32; draws whose bracket stalls undecided are solved
+              again in float64
+    p-value   p = (#above + #undecided) / B
+
+Respondent weights: "multinomial" (R picks with replacement per draw) and "multinomial_reject"
+(redraw a weight row that leaves a menu unseen), drawn from numpy.random.default_rng(seed) in the
+reference's order.
+"""
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import defaults
+
+BELOW, ABOVE, UNDECIDED = 0, 1, 2
+ZERO = 1e-9
+REDRAW_ROUNDS = 10000
+
+
+def scaling(n, r_n=None, eps_n=None):
+    """(r_n, eps_n, s): sqrt(n), n^(-1/3) and 1 + eps_n r_n (solver/inference/hong_li.py:33-45)."""
+    if int(n) != n or n < 1:
+        raise ValueError("n, the sample size, must be a positive integer; got %r" % (n,))
+    r_n = math.sqrt(n) if r_n is None else float(r_n)
+    eps_n = n ** (-1.0 / 3.0) if eps_n is None else float(eps_n)
+    return r_n, eps_n, 1.0 + eps_n * r_n
+
+
+def perturb(p_hat, p_b, r_n, eps_n):
+    return p_hat + (eps_n * r_n) * (p_b - p_hat)
+
+
+def decide(L, U, tau_lo, tau_hi):
+    d = np.full(np.shape(U), UNDECIDED, dtype=np.int8)
+    d[np.asarray(L) >= tau_hi] = ABOVE
+    d[np.asarray(U) < tau_lo] = BELOW
+    return d
+
+
+class Draws:
+    """B resampled p_hat's from a respondent panel (respondent, menu, chosen columns)."""
+
+    def __init__(self, panel, menu, alternative, p_hat, B, weights="multinomial_reject", seed=0):
+        if weights not in ("multinomial", "multinomial_reject"):
+            raise ValueError("weights must be 'multinomial' or 'multinomial_reject'")
+        resp = np.asarray(panel["respondent"])
+        pm = np.asarray(panel["menu"], dtype=np.int64)
+        pc = np.asarray(panel["chosen"], dtype=np.int64)
+        _, codes = np.unique(resp, return_inverse=True)
+        R = int(codes.max()) + 1
+        menu, alternative = np.asarray(menu, dtype=np.int64), np.asarray(alternative, dtype=np.int64)
+        M = menu.size
+        rum_menus, row_menu = np.unique(menu, return_inverse=True)
+        m = np.minimum(np.searchsorted(rum_menus, pm), rum_menus.size - 1)
+        used = rum_menus[m] == pm
+        row_key = row_menu * 64 + alternative
+        order = np.argsort(row_key)
+        key = m * 64 + pc
+        pos = np.minimum(np.searchsorted(row_key[order], key), M - 1)
+        hit = used & (row_key[order][pos] == key)
+        self.offered = sp.csr_array((np.ones(int(used.sum())), (codes[used], m[used])), shape=(R, rum_menus.size))
+        self.chose = sp.csr_array((np.ones(int(hit.sum())), (codes[hit], order[pos[hit]])), shape=(R, M))
+        self.row_menu = row_menu
+        self.p_hat = np.asarray(p_hat, dtype=np.float64)
+        self.B, self.R, self.M, self.weights, self.seed = int(B), R, M, weights, seed
+        rng = np.random.default_rng(seed)
+        W = rng.multinomial(R, np.ones(R) / R, size=self.B).astype(np.float64)
+        self.n_redraws = 0
+        if weights == "multinomial_reject":
+            for _ in range(REDRAW_ROUNDS):
+                bad = np.any(np.asarray((sp.csr_array(W) @ self.offered).todense()) <= 0, axis=1)
+                if not bad.any():
+                    break
+                self.n_redraws += int(bad.sum())
+                W[bad] = rng.multinomial(R, np.ones(R) / R, size=int(bad.sum())).astype(np.float64)
+        self.W = W
+
+    def rows(self, idx):
+        """The draws idx as a (len(idx), M) array: weighted shares, p_hat where a menu went unseen."""
+        Wb = sp.csr_array(self.W[np.asarray(idx, dtype=np.int64)])
+        seen = np.asarray((Wb @ self.offered).todense())[:, self.row_menu]
+        chose = np.asarray((Wb @ self.chose).todense())
+        empty = seen <= 0
+        return np.where(empty, self.p_hat, chose / np.where(empty, 1.0, seen))
+
+
+@dataclass
+class PValue:
+    p: float
+    p_lo: float
+    p_hi: float
+    alpha: float
+    reject: bool
+    certain: bool
+    n_below: int
+    n_above: int
+    n_undecided: int
+    n_screened: int
+    n_solved: int
+    B: int
+    tau: tuple
+    dist_hat: tuple
+    time: float
+    draws_per_s: float
+
+
+class Bootstrap:
+    def __init__(self, rum, n=None, panel=None, replies=None, B=None, weights=None, seed=None, r_n=None, eps_n=None,
+                 method=None, method_args=None, abs_tol=None, rel_tol=None, max_time=None, draw_time=None,
+                 batch_slots=0, verbose=False):
+        d = defaults.BOOTSTRAP
+        if panel is None or replies is not None:
+            raise ValueError("this bootstrap takes a respondent panel (panel=)")
+        self.rum, self.p_hat = rum, rum.choice_probability
+        self.B = int(d["B"] if B is None else B)
+        self.abs_tol = float(d["abs_tol"] if abs_tol is None else abs_tol)
+        self.rel_tol = float(d["rel_tol"] if rel_tol is None else rel_tol)
+        self.max_time = float(d["max_time"] if max_time is None else max_time)
+        self.draw_time = float(d["draw_time"] if draw_time is None else draw_time)
+        self.draws = Draws(panel, rum.menu, rum.alternative, self.p_hat, self.B,
+                           d["weights"] if weights is None else weights, d["seed"] if seed is None else seed)
+        self.n = self.draws.R if n is None else int(n)
+        self.r_n, self.eps_n, self.s = scaling(self.n, r_n, eps_n)
+        self.session = rum.session(method=method, method_args=method_args)
+        self.batch_slots = batch_slots
+        self.L, self.U = np.zeros(self.B), np.full(self.B, np.inf)
+        self.solved = np.zeros(self.B, dtype=bool)
+        self.n_refined = 0          # float32 draws that stalled undecided and finished in float64
+        self.L0 = self.U0 = None
+        self.verbose = verbose
+        self.time = dict(certificate=0.0, screen=0.0, solve=0.0)
+
+    @property
+    def tau(self):
+        return (self.s * self.L0, self.s * self.U0)
+
+    def _certify(self):
+        t0 = time.perf_counter()
+        r = self.session.solve(self.p_hat, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_time=self.max_time,
+                               keep=True)
+        if not math.isfinite(r.ub):
+            raise RuntimeError("p_hat could not be certified: %s (%s)" % (r.status, r.message))
+        self.L0, self.U0 = r.lb, r.ub
+        self.time["certificate"] += time.perf_counter() - t0
+
+    def _screen(self):
+        t0, fit = time.perf_counter(), self.session.fit
+        for lo in range(0, self.B, 256):
+            idx = np.arange(lo, min(self.B, lo + 256))
+            P = perturb(self.p_hat, self.draws.rows(idx), self.r_n, self.eps_n)
+            self.U[idx] = np.minimum(self.U[idx], np.sqrt(np.einsum("ij,ij->i", P - fit, P - fit)))
+        self.n_screened = int((self.U < self.tau[0]).sum())
+        self.time["screen"] += time.perf_counter() - t0
+
+    def solve_draws(self, idx, stops=True):
+        """Solve the draws idx: bm_admm all together (batched), flow_cg one at a time."""
+        t0 = time.perf_counter()
+        idx = np.asarray(idx, dtype=np.int64)
+        if idx.size == 0:
+            return
+        tau_lo, tau_hi = self.tau
+        P = perturb(self.p_hat, self.draws.rows(idx), self.r_n, self.eps_n)
+        rum, s = self.rum, self.session
+        if s.method == "bm_admm" and rum.n >= 8 and rum._single.size == 0:
+            from .rum_solver import context
+            ctx = context()
+            a = s._args
+            g = rum._geom
+            prob = ctx.bm_problem(rum.n, g.menu.astype(np.uint32), g.alternative.astype(np.int32), self.p_hat)
+            dt = "float32" if a["dtype"] in ("float32", "mixed") else "float64"
+            par = ctx.bm_params(a["beta"], alpha=a["alpha"], precond_p=a["precond_p"], check=a["check"],
+                                lb_every=a["lb_every"], max_iter=a["max_iter"], abs_tol=self.abs_tol,
+                                rel_tol=self.rel_tol if self.rel_tol > 0 else None, dtype=dt)
+            below, above = (tau_lo, tau_hi) if stops else (None, None)
+            res, info = ctx.bm_solve_batch(prob, par, P, below=below, above=above, warm=s._kept,
+                                           slots=self.batch_slots, draw_time=self.draw_time)
+            for j, b in enumerate(idx):
+                self.L[b] = max(self.L[b], res[j]["lb"])
+                self.U[b] = min(self.U[b], res[j]["ub"])
+            self.last_batch = info
+            if dt == "float32":
+                # draws whose float32 bracket stalled before a decision finish in float64
+                dec = decide(self.L[idx], self.U[idx], tau_lo, tau_hi)
+                redo = [j for j in range(idx.size) if res[j]["stop_reason"] == "stall" and
+                        (not stops or dec[j] == UNDECIDED)]
+                if redo:
+                    par.dtype = 0
+                    res2, info2 = ctx.bm_solve_batch(prob, par, P[redo], below=below, above=above, warm=s._kept,
+                                                     slots=self.batch_slots, draw_time=self.draw_time)
+                    for j, r in zip(redo, res2):
+                        b = idx[j]
+                        self.L[b], self.U[b] = max(self.L[b], r["lb"]), min(self.U[b], r["ub"])
+                    self.n_refined += len(redo)
+                    self.last_batch_f64 = info2
+        else:
+            for j, b in enumerate(idx):
+                r = s.solve(P[j], abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_time=self.draw_time, warm=True,
+                            below=tau_lo if stops else None, above=tau_hi if stops else None)
+                self.L[b], self.U[b] = max(self.L[b], r.lb), min(self.U[b], r.ub)
+        self.solved[idx] = True
+        self.time["solve"] += time.perf_counter() - t0
+
+    def p_value(self, alpha=0.05, max_draws=None):
+        t0 = time.perf_counter()
+        if self.L0 is None:
+            self._certify()
+            self._screen()
+        if self.U0 > ZERO:
+            dec = decide(self.L, self.U, *self.tau)
+            todo = np.flatnonzero((dec == UNDECIDED) & ~self.solved)
+            if max_draws is not None:
+                todo = todo[:max_draws]
+            if todo.size:
+                self.solve_draws(todo)
+        dec = decide(self.L, self.U, *self.tau)
+        above = int((dec == ABOVE).sum())
+        und = int((dec == UNDECIDED).sum())
+        p_lo, p_hi = above / self.B, (above + und) / self.B
+        solved = int(self.solved.sum())
+        return PValue(p=p_hi, p_lo=p_lo, p_hi=p_hi, alpha=alpha, reject=p_hi <= alpha,
+                      certain=p_hi <= alpha or p_lo > alpha, n_below=int((dec == BELOW).sum()), n_above=above,
+                      n_undecided=und, n_screened=self.n_screened, n_solved=solved, B=self.B, tau=self.tau,
+                      dist_hat=(self.L0, self.U0), time=time.perf_counter() - t0,
+                      draws_per_s=solved / self.time["solve"] if self.time["solve"] > 0 else float("nan"))

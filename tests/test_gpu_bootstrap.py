@@ -1,0 +1,35 @@
+"""The bootstrap's draws solved together (batched slots) reach the same decisions as the same
+draws solved one at a time through the Session (the reference's loop)."""
+import numpy as np
+import pytest
+
+from rumb import RUM
+from rumb import bootstrap as BS
+from rumb.instances import panel_instance
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batched_and_sequential_bootstrap_agree():
+    n = 10
+    panel, (m, a, p) = panel_instance(n, 0.3, 80, 8, 5, seed=7)
+    rum = RUM(m, a, p, num_alternatives=n)
+    b1 = rum.bootstrap(panel=panel, B=24, weights="multinomial", seed=1, method="bm_admm",
+                       method_args={"dtype": "float64"})
+    r1 = b1.p_value()
+    b2 = rum.bootstrap(panel=panel, B=24, weights="multinomial", seed=1, method="bm_admm",
+                       method_args={"dtype": "float64"})
+    b2._certify()
+    b2._screen()
+    todo = np.flatnonzero((BS.decide(b2.L, b2.U, *b2.tau) == BS.UNDECIDED))
+    tau_lo, tau_hi = b2.tau
+    P = BS.perturb(b2.p_hat, b2.draws.rows(todo), b2.r_n, b2.eps_n)
+    for j, b in enumerate(todo):
+        r = b2.session.solve(P[j], abs_tol=b2.abs_tol, rel_tol=b2.rel_tol, warm=True, below=tau_lo, above=tau_hi)
+        b2.L[b], b2.U[b] = max(b2.L[b], r.lb), min(b2.U[b], r.ub)
+    d1 = BS.decide(b1.L, b1.U, *b1.tau)
+    d2 = BS.decide(b2.L, b2.U, *b2.tau)
+    assert np.array_equal(d1, d2)
+    assert r1.n_solved == todo.size
+    # every bracket of the batch contains the one-at-a-time bracket's distance
+    assert np.all(b1.L <= b2.U + 1e-9) and np.all(b2.L <= b1.U + 1e-9)

@@ -137,3 +137,25 @@ def test_generators_shapes_and_determinism():
     assert panel["menu"].size == 200 and set(np.unique(panel["respondent"])) == set(range(40))
     panel, (mm, aa, pp) = dsr_instance(10, 20, 30, 4, seed=1)
     assert mm.size == 20 and (aa == 0).all() and ((mm & 1) == 1).all()
+
+
+def test_bootstrap_draws_and_formulas():
+    from rumb import bootstrap as BS
+    from rumb.instances import panel_instance
+    panel, (m, a, p) = panel_instance(10, 0.2, 60, 6, 4, seed=3)
+    d = BS.Draws(panel, m, a, p, B=20, weights="multinomial", seed=0)
+    rows = d.rows(np.arange(20))
+    assert rows.shape == (20, p.size)
+    # a draw with every respondent weighted once reproduces p_hat
+    d.W[0] = 1.0
+    np.testing.assert_allclose(d.rows([0])[0], p, atol=1e-12)
+    # shares stay shares
+    sums = np.zeros((20, np.unique(m).size))
+    inv = np.unique(m, return_inverse=True)[1]
+    for k in range(20):
+        sums[k] = np.bincount(inv, weights=rows[k])
+    np.testing.assert_allclose(sums, 1.0, atol=1e-12)
+    r_n, eps_n, s = BS.scaling(520)
+    assert r_n == pytest.approx(math.sqrt(520)) and eps_n == pytest.approx(520 ** (-1 / 3))
+    dec = BS.decide([0.0, 3.0, 1.0], [0.5, 4.0, 2.5], 1.0, 2.0)
+    assert list(dec) == [BS.BELOW, BS.ABOVE, BS.UNDECIDED]
