@@ -93,6 +93,15 @@ RUMB_API int rumb_cancel(rumb_ctx *ctx);
  * pair (l, l | 2^j), lo' = a*lo + b*hi, hi' = c*lo + d*hi; dtype RUMB_F64 or RUMB_F32. */
 RUMB_API int rumb_butterfly(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, double a, double b,
                    double c, double d);
+/* rumb_butterfly with no device allocation (no counterpart in the reference). It stages the slab
+ * in a 4 MiB static device array, one per device, instead of the context's scratch, so it holds
+ * n <= 16 in either dtype; a larger slab returns RUMB_E_INVAL. The first call on each device looks
+ * the array up (cudaGetSymbolAddress) and loads the kernels it launches: make that call before any
+ * region where nothing may allocate. Nothing in the array has to start at zero. Every context on a
+ * device shares the array: calls on one device must not overlap (they race; nothing serializes
+ * them). */
+RUMB_API int rumb_butterfly_noalloc(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, double a,
+                                    double b, double c, double d);
 /* out = the per-menu simplex prox of v (all 2^n - 1 menus); xhat holds p_hat at observed entries,
  * wmask is 1 at observed entries and 0 elsewhere. */
 RUMB_API int rumb_prox(rumb_ctx *ctx, int n, int dtype, const void *v, const void *xhat, const void *wmask,

@@ -140,6 +140,14 @@ int rumb_butterfly(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, d
     RUMB_API_END
 }
 
+int rumb_butterfly_noalloc(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, double a, double b,
+                           double c, double d) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::butterfly_noalloc_host(ctx->c, n, dtype, in, out, a, b, c, d);
+    RUMB_API_END
+}
+
 int rumb_prox(rumb_ctx *ctx, int n, int dtype, const void *v, const void *xhat, const void *wmask, double beta2,
               void *out) {
     RUMB_API_BEGIN

@@ -18,6 +18,7 @@
 // copyto). The prox walks menus in mask order, so a warp's members of one alternative are 32
 // consecutive entries of that alternative's block (coalesced), and projects with Michelot's
 // active-set iteration in registers instead of an insertion sort.
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -1568,6 +1569,57 @@ int butterfly_host(Ctx &c, int n, int dtype, const void *in, void *out, double a
         xf_transform<float, float>(n, S.a.as<float>(), S.a.as<float>(),
                                    Co<float>{(float)a, (float)b, (float)cc, (float)d}, st);
     RUMB_CUDA(cudaMemcpyAsync(out, S.a.ptr, (size_t)m2 * es, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    c.join_out();
+    return RUMB_OK;
+}
+
+// ----------------------------------------------------------------- butterfly without allocation
+// butterfly_host stages the slab in the context's scratch, which grows by cudaMalloc/cudaFree.
+// This variant stages it in a static device array of this module instead, so a call reaches no
+// allocator: 4 MiB, which holds the slab up to n = 16 (16 * 2^15 float64 values). The array is
+// per device and shared by every context on it; the host copy overwrites every entry the
+// transform reads, so nothing in it has to start at zero. Two calls on one device that overlap
+// (two threads, two contexts) race on the array; nothing here serializes them.
+static constexpr size_t NOALLOC_SLAB_BYTES = size_t(4) << 20;
+static constexpr int NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) unsigned char g_noalloc_slab[NOALLOC_SLAB_BYTES];
+static std::atomic<void *> g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+// The slab's address on `device`, which must be the current device. Found once per device by
+// cudaGetSymbolAddress (which loads this module on that device if nothing has yet).
+static void *noalloc_slab(int device) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) fail(RUMB_E_INVAL, "butterfly_noalloc: device index above 63");
+    void *p = g_noalloc_addr[device].load(std::memory_order_acquire);
+    if (p) return p;
+    RUMB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_slab));
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 255)) fail(RUMB_E_INTERNAL, "butterfly_noalloc: slab address");
+    g_noalloc_addr[device].store(p, std::memory_order_release);
+    return p;
+}
+
+int butterfly_noalloc_host(Ctx &c, int n, int dtype, const void *in, void *out, double a, double b, double cc,
+                           double d) {
+    if (n < 2 || n > 30) fail(RUMB_E_INVAL, "butterfly_noalloc: 2 <= n <= 30");
+    if (dtype != RUMB_F64 && dtype != RUMB_F32) fail(RUMB_E_INVAL, "butterfly_noalloc: dtype RUMB_F64 or RUMB_F32");
+    if (!in || !out) fail(RUMB_E_INVAL, "butterfly_noalloc: NULL buffer");
+    ll m2 = (ll)n << (n - 1);
+    size_t es = dtype == RUMB_F64 ? 8 : 4;
+    size_t bytes = (size_t)m2 * es;
+    if (bytes > NOALLOC_SLAB_BYTES)
+        fail(RUMB_E_INVAL, "butterfly_noalloc: the slab of n = " + std::to_string(n) + " needs " +
+                               std::to_string(bytes) + " bytes; the static staging array holds " +
+                               std::to_string(NOALLOC_SLAB_BYTES) + " (n <= 16)");
+    void *slab = noalloc_slab(c.device);
+    cudaStream_t st = c.own;
+    c.join_in();
+    RUMB_CUDA(cudaMemcpyAsync(slab, in, bytes, cudaMemcpyHostToDevice, st));
+    if (dtype == RUMB_F64)
+        xf_transform<double, double>(n, (const double *)slab, (double *)slab, Co<double>{a, b, cc, d}, st);
+    else
+        xf_transform<float, float>(n, (const float *)slab, (float *)slab,
+                                   Co<float>{(float)a, (float)b, (float)cc, (float)d}, st);
+    RUMB_CUDA(cudaMemcpyAsync(out, slab, bytes, cudaMemcpyDeviceToHost, st));
     RUMB_CUDA(cudaStreamSynchronize(st));
     c.join_out();
     return RUMB_OK;

@@ -8,6 +8,8 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
 int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, void *x2, void *s, void *y, void *z,
                int iters, int cold);
 int butterfly_host(Ctx &c, int n, int dtype, const void *in, void *out, double a, double b, double cc, double d);
+int butterfly_noalloc_host(Ctx &c, int n, int dtype, const void *in, void *out, double a, double b, double cc,
+                           double d);
 int prox_host(Ctx &c, int n, int dtype, const void *v, const void *xhat, const void *wmask, double beta2, void *out);
 int push_ub64_host(Ctx &c, int n, int dtype, const void *x, ll mp, const uint32_t *menu, const int32_t *alt,
                    const double *p, double *ub, double *p_fit);

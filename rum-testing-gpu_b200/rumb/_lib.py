@@ -82,6 +82,7 @@ _SIGS = {
     "rumb_mem_info": ([_vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
     "rumb_cancel": ([_vp], ctypes.c_int),
     "rumb_butterfly": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp] + [ctypes.c_double] * 4, ctypes.c_int),
+    "rumb_butterfly_noalloc": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp] + [ctypes.c_double] * 4, ctypes.c_int),
     "rumb_prox": ([_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_double, _vp], ctypes.c_int),
     "rumb_push_ub64": ([_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_longlong, _vp, _vp, _vp,
                         ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
@@ -188,6 +189,16 @@ class Context:
             raise ValueError("slab of n * 2^(n-1) values expected")
         out = np.empty_like(v)
         check(load().rumb_butterfly(self.h, n, dt, _p(v), _p(out), a, b, c, d))
+        return out
+
+    def butterfly_noalloc(self, n, v, a, b, c, d):
+        """butterfly() staged in the library's static device array: no device allocation, n <= 16."""
+        v = np.ascontiguousarray(v)
+        dt = {np.dtype(np.float64): F64, np.dtype(np.float32): F32}[v.dtype]
+        if v.size != n << (n - 1):
+            raise ValueError("slab of n * 2^(n-1) values expected")
+        out = np.empty_like(v)
+        check(load().rumb_butterfly_noalloc(self.h, n, dt, _p(v), _p(out), a, b, c, d))
         return out
 
     def prox(self, n, v, xhat, wmask, beta2):
