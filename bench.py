@@ -2,6 +2,8 @@
 """Benchmark: certified BM-ADMM solves per second at n = 18 (1 % menu density), abs gap 1e-5.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--dtype float64|mixed] [--impl rumb|reference]
+    python bench.py --profile-case ITERS [--dtype ...]   # one solve capped at ITERS iterations, for
+                                                          # profilers; prints no bench line
 
 Workload "n18_d1pct_k50": every menu of 18 alternatives with >= 2 members kept with probability
 0.01 (2,627 menus, 23,650 observed cells), p_hat from a Dirichlet(1) mixture of 50 random linear
@@ -11,8 +13,10 @@ solve from the cold start: float64 upper and lower bound every 50 iterations unt
 
 value   solves/s with the instance already in HBM (device pointers), all ranks summed
 e2e     the same through the C ABI from host buffers: rows uploaded and p_fit read back per solve
-roofline, for the kernel with the largest time share in an eager profile of 20 iterations:
-        algorithmic bytes per launch / its CUDA-event launch time, against MEASURED_PEAKS.json
+roofline, for the kernel with the largest time share in an eager profile of 20 iterations (after
+        2000 untimed ones): algorithmic bytes per launch / its CUDA-event launch time, against
+        MEASURED_PEAKS.json hbm_gbs
+gpu_launches   the library's own count of the kernels the timed solves launched
 cpu_baseline   the oracle (C restatement of the reference's iteration and certificate) on the host,
         a bounded sample of iterations scaled to solves/s by this run's iteration count
 
@@ -45,7 +49,9 @@ CHECK = 50
 # Iterations of the float64 certified solve of this seeded workload (the float64 library path
 # and the oracle follow the same trajectory; checked at n = 10 by tests/test_gpu_bm.py); the
 # reference arm, which runs only a sample, scales by it.
-CERT_ITERS_F64 = None
+CERT_ITERS_F64 = 43800
+# iterations run before the profiled ones: the roofline kernel is timed mid-solve
+PROFILE_WARMUP = 2000
 # DRAM bytes per launch of the dominant kernel, from the ncu capture summarised under profiles/
 NCU_TRAFFIC = {}
 
@@ -179,6 +185,8 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
+                    help="run one solve capped at ITERS iterations (for ncu) and print no bench line")
     args = ap.parse_args()
     rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
 
@@ -207,6 +215,13 @@ def main():
     prob_host = ctx.bm_problem(n, menu, alt, p)
     par = ctx.bm_params(beta, check=CHECK, abs_tol=ABS_TOL, rel_tol=None, dtype=args.dtype, max_iter=10 ** 7,
                         time_limit=600)
+    if args.profile_case > 0:
+        par.max_iter = args.profile_case
+        r, _, _ = ctx.bm_solve((prob_dev, None), par, want_fit=False)
+        torch.cuda.synchronize()
+        print("profile case: %d iterations, %d kernel launches, stop %s" % (r["iters"], r["launches"],
+                                                                           r["stop_reason"]))
+        return
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")       # > 126 MB of L2
 
     def solve(dev):
@@ -223,6 +238,7 @@ def main():
 
     def timed(dev, k):
         ms, res = [], None
+        timed.launches = 0
         for _ in range(k):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -232,6 +248,7 @@ def main():
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+            timed.launches += int(res["launches"])
         return ms, res
 
     for _ in range(args.warmup):
@@ -239,6 +256,7 @@ def main():
     barrier()
     with ClockSampler(local) as clk:
         ms_dev, res = timed(True, args.steps)
+        launches_dev = timed.launches
         barrier()
     clocks = clk.summary()
     barrier()
@@ -251,15 +269,14 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step_ms, e2e_ms = float(t[0]), float(t[1])
 
-    # roofline of the dominant kernel (eager profile, CUDA events per launch on the library's stream)
-    prof = ctx.bm_profile((prob_dev, None), par, iters=20)
-    launches = sum(k["launches"] for k in prof if k["name"].startswith(("bfly", "prox")))
+    # roofline of the dominant kernel: an eager profile (CUDA events around every launch on the
+    # library's stream) of 20 iterations and one check, after PROFILE_WARMUP iterations
+    prof = ctx.bm_profile((prob_dev, None), par, iters=20, warmup=PROFILE_WARMUP)
     top = max(prof, key=lambda k: k["total_ms"])
     tot = sum(k["total_ms"] for k in prof)
     per_launch_ms = top["total_ms"] / top["launches"]
     peak, peak_kind = load_peaks()
     achieved = top["bytes_per_launch"] / (per_launch_ms * 1e-3) / 1e9
-    iter_launches = launches / 20.0
 
     if world > 1:
         dist.barrier()
@@ -294,7 +311,7 @@ def main():
                      "us_per_launch": round(1e3 * k["total_ms"] / k["launches"], 2),
                      "gbs": round(k["bytes_per_launch"] / (k["total_ms"] / k["launches"] * 1e-3) / 1e9, 1)}
                     for k in sorted(prof, key=lambda k: -k["total_ms"])[:8]],
-        "gpu_launches": int(round(iter_launches * res["iters"] + 2 * n * res["n_push"] * 1.5)),
+        "gpu_launches": int(launches_dev),
         "cpu_baseline": cpu,
         "clocks": clocks,
     }

@@ -154,6 +154,7 @@ typedef struct {
     int n_push, n_lb;
     double setup_s, solve_s, push_s, per_iter_ms;
     double device_ms;    /* CUDA-event time of the solve on the context's stream */
+    long long launches;  /* kernels the call launched (graph replays count their kernels) */
 } rumb_bm_result;
 
 /* called once per check with (iterations, seconds since the call, phi, best ub, best lb) */
@@ -185,6 +186,7 @@ typedef struct {
     long long total_iters;/* slot-iterations run */
     double setup_s, solve_s, device_ms;
     int lo_bits;          /* transform split used */
+    long long launches;   /* kernels the call launched (graph replays count their kernels) */
 } rumb_batch_info;
 
 /* B draws of one menu structure (prob->menu, prob->alt; prob->p is the structure's reference
@@ -230,12 +232,13 @@ typedef struct {
     double bytes_per_launch;  /* algorithmic bytes one launch must move */
 } rumb_kernel_stat;
 
-/* Runs `iters` ADMM iterations from the cold start (plus one float64 check when
- * par->lb_every > 0) with an event pair around every kernel launch, and reports per kernel:
+/* Runs `warmup` untimed ADMM iterations from the cold start, then `iters` iterations (plus one
+ * float64 check when par->lb_every > 0) with an event pair around every kernel launch, and
+ * reports per kernel:
  * launches, total time and algorithmic bytes per launch. Fills at most cap entries. This is the
  * library's counterpart of the reference's per-phase timers (solver/flow_cg/solver.py:174-188). */
-RUMB_API int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int iters,
-                             rumb_kernel_stat *stats, int cap, int *count);
+RUMB_API int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int warmup,
+                             int iters, rumb_kernel_stat *stats, int cap, int *count);
 
 #ifdef __cplusplus
 }

@@ -209,12 +209,12 @@ int rumb_bm_solve_batch(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_b
     RUMB_API_END
 }
 
-int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int iters,
+int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int warmup, int iters,
                     rumb_kernel_stat *stats, int cap, int *count) {
     RUMB_API_BEGIN
     NEED_CTX(ctx);
     if (iters < 1) rumb::fail(RUMB_E_INVAL, "iters must be >= 1");
-    return rumb::bm_profile(ctx->c, prob, par, iters, stats, cap, count);
+    return rumb::bm_profile(ctx->c, prob, par, warmup, iters, stats, cap, count);
     RUMB_API_END
 }
 

@@ -910,6 +910,7 @@ static void promote_state(BmWork<float> &F, BmWork<double> &D, ll m2, cudaStream
 struct Graph {
     cudaGraph_t g = nullptr;
     cudaGraphExec_t e = nullptr;
+    long long kernels = 0;     // kernel launches captured (each replay launches them all)
     ~Graph() { reset(); }
     void reset() {
         if (e) cudaGraphExecDestroy(e);
@@ -921,18 +922,25 @@ struct Graph {
     void capture(cudaStream_t st, F &&fn) {
         reset();
         RUMB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const long long before = g_launches;
         try {
             fn();
         } catch (...) {
+            g_launches = before;
             cudaGraph_t tmp = nullptr;
             cudaStreamEndCapture(st, &tmp);
             if (tmp) cudaGraphDestroy(tmp);
             throw;
         }
+        kernels = g_launches - before;     // captured, not yet run
+        g_launches = before;
         RUMB_CUDA(cudaStreamEndCapture(st, &g));
         RUMB_CUDA(cudaGraphInstantiate(&e, g, 0));
     }
-    void launch(cudaStream_t st) { RUMB_CUDA(cudaGraphLaunch(e, st)); }
+    void launch(cudaStream_t st) {
+        RUMB_CUDA(cudaGraphLaunch(e, st));
+        g_launches += kernels;
+    }
 };
 
 static int graph_chunk(int check) {
@@ -1043,6 +1051,7 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
     check_params(par);
     if (!out) fail(RUMB_E_INVAL, "result is NULL");
     auto t0 = Clock::now();
+    const long long launches0 = g_launches;
     int n = pr->n;
     ll m2 = (ll)n << (n - 1);
     if (warm && (warm->n != n)) fail(RUMB_E_INVAL, "warm state was kept for another n");
@@ -1139,6 +1148,7 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
     out->push_s = L.push_s;
     out->per_iter_ms = L.it > 0 ? 1e3 * out->solve_s / (double)L.it : 0.0;
     out->device_ms = dms;
+    out->launches = g_launches - launches0;
     c.join_out();
     return RUMB_OK;
 }
@@ -1193,7 +1203,7 @@ thread_local Prof *g_prof = nullptr;
 
 // Runs `iters` iterations eagerly from the cold start with an event pair around every launch;
 // returns per-kernel-name launches, total milliseconds and algorithmic bytes per launch.
-int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int iters, rumb_kernel_stat *stats,
+int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int warmup, int iters, rumb_kernel_stat *stats,
                int cap, int *count) {
     check_problem(pr);
     check_params(par);
@@ -1219,7 +1229,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         enqueue_cold_start<T>(W, C, n, st);
         C.lo_bits = tune_lo_bits<T>(c, W, C, n, st);
         enqueue_cold_start<T>(W, C, n, st);
-        for (int i = 0; i < 3; ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
+        for (int i = 0; i < std::max(warmup, 3); ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
         RUMB_CUDA(cudaStreamSynchronize(st));
         g_prof = &prof;
         try {
@@ -1536,9 +1546,12 @@ int bm_solve_batch(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par,
     if (warm && warm->n != pr->n) fail(RUMB_E_INVAL, "warm state was kept for another n");
     c.cancel.store(0);
     c.join_in();
+    const long long launches0 = g_launches;
     int r;
     if (par->dtype == RUMB_F64) r = bm_solve_batch_t<double>(c, pr, par, bp, B, P, below, above, warm, out, info);
     else r = bm_solve_batch_t<float>(c, pr, par, bp, B, P, below, above, warm, out, info);
+    for (int b = 0; b < B; ++b) out[b].launches = 0;     // shared by the batch: counted in info
+    if (info) info->launches = g_launches - launches0;
     c.join_out();
     return r;
 }

@@ -15,7 +15,7 @@ int push_ub64_host(Ctx &c, int n, int dtype, const void *x, ll mp, const uint32_
                    const double *p, double *ub, double *p_fit);
 int fw_lb64_host(Ctx &c, int n, ll mp, const uint32_t *menu, const int32_t *alt, const double *y, const double *p,
                  double *lb);
-int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int iters, rumb_kernel_stat *stats,
+int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int warmup, int iters, rumb_kernel_stat *stats,
                int cap, int *count);
 int bm_solve_batch(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_batch_params *bp, int B,
                    const double *P, const double *below, const double *above, const rumb_bm_state *warm,

@@ -38,7 +38,10 @@ inline void cuda_check(cudaError_t e, const char *what) {
 }
 
 #define RUMB_CUDA(call) ::rumb::cuda_check((call), #call)
-#define RUMB_LAUNCH(what) ::rumb::cuda_check(cudaGetLastError(), what)
+// Kernels launched by the calling thread: RUMB_LAUNCH counts each launch, a CUDA graph replay adds
+// the kernels it captured; the C ABI reports the difference over a call.
+inline thread_local long long g_launches = 0;
+#define RUMB_LAUNCH(what) (++::rumb::g_launches, ::rumb::cuda_check(cudaGetLastError(), what))
 
 void set_last_error(const std::string &msg);
 

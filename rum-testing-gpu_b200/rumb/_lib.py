@@ -50,7 +50,7 @@ class BMResult(ctypes.Structure):
                 ("iters", ctypes.c_longlong), ("iters_f32", ctypes.c_longlong), ("stop", ctypes.c_int),
                 ("n_push", ctypes.c_int), ("n_lb", ctypes.c_int), ("setup_s", ctypes.c_double),
                 ("solve_s", ctypes.c_double), ("push_s", ctypes.c_double), ("per_iter_ms", ctypes.c_double),
-                ("device_ms", ctypes.c_double)]
+                ("device_ms", ctypes.c_double), ("launches", ctypes.c_longlong)]
 
 
 class BatchParams(ctypes.Structure):
@@ -60,7 +60,7 @@ class BatchParams(ctypes.Structure):
 class BatchInfo(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("bytes_per_slot", ctypes.c_double), ("total_iters", ctypes.c_longlong),
                 ("setup_s", ctypes.c_double), ("solve_s", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("lo_bits", ctypes.c_int)]
+                ("lo_bits", ctypes.c_int), ("launches", ctypes.c_longlong)]
 
 
 class KernelStat(ctypes.Structure):
@@ -94,7 +94,7 @@ _SIGS = {
     "rumb_bm_solve_batch": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), ctypes.POINTER(BatchParams),
                              ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.POINTER(BMResult), ctypes.POINTER(BatchInfo)],
                             ctypes.c_int),
-    "rumb_bm_profile": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), ctypes.c_int,
+    "rumb_bm_profile": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), ctypes.c_int, ctypes.c_int,
                          ctypes.POINTER(KernelStat), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "rumb_cg_pricer_create": ([_vp, ctypes.c_int, ctypes.c_longlong, _vp, _vp, ctypes.c_int, ctypes.c_int,
                                ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
@@ -304,13 +304,13 @@ class Context:
             out.append(d)
         return out, {f: getattr(info, f) for f, _ in BatchInfo._fields_}
 
-    def bm_profile(self, problem, params, iters=20):
+    def bm_profile(self, problem, params, iters=20, warmup=3):
         """[dict(name, launches, total_ms, bytes_per_launch)] over `iters` eager iterations."""
         pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
         cap = 64
         arr = (KernelStat * cap)()
         cnt = ctypes.c_int()
-        check(load().rumb_bm_profile(self.h, ctypes.byref(pr), ctypes.byref(params), int(iters), arr, cap,
+        check(load().rumb_bm_profile(self.h, ctypes.byref(pr), ctypes.byref(params), int(warmup), int(iters), arr, cap,
                                      ctypes.byref(cnt)))
         return [dict(name=arr[i].name.decode(), launches=arr[i].launches, total_ms=arr[i].total_ms,
                      bytes_per_launch=arr[i].bytes_per_launch) for i in range(cnt.value)]
