@@ -125,6 +125,45 @@ class PValue:
     draws_per_s: float
 
 
+def _dist(group):
+    """(rank, world, group) of the process group the draws are sharded over (1 rank without one)."""
+    try:
+        import torch.distributed as dist
+    except ImportError:
+        return 0, 1, None
+    if group is None and not (dist.is_available() and dist.is_initialized()):
+        return 0, 1, None
+    return dist.get_rank(group), dist.get_world_size(group), group
+
+
+def _device_for(group):
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def _broadcast_band(L0, U0, group):
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([L0, U0], dtype=torch.float64, device=_device_for(group))
+    dist.broadcast(t, src=dist.get_global_rank(group, 0) if group is not None else 0, group=group)
+    return float(t[0]), float(t[1])
+
+
+def _gather_record(L, U, solved, group):
+    """Every rank's (L, U, solved) combined: a draw's bounds are the tightest any rank found."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    t = torch.from_numpy(np.stack([L, U, solved.astype(np.float64)])).to(_device_for(group))
+    parts = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(parts, t, group=group)
+    allr = torch.stack(parts).cpu().numpy()
+    return allr[:, 0].max(axis=0), allr[:, 1].min(axis=0), allr[:, 2].max(axis=0) > 0
+
+
 class Bootstrap:
     def __init__(self, rum, n=None, panel=None, replies=None, B=None, weights=None, seed=None, r_n=None, eps_n=None,
                  method=None, method_args=None, abs_tol=None, rel_tol=None, max_time=None, draw_time=None,
@@ -221,18 +260,28 @@ class Bootstrap:
         self.solved[idx] = True
         self.time["solve"] += time.perf_counter() - t0
 
-    def p_value(self, alpha=0.05, max_draws=None):
+    def p_value(self, alpha=0.05, max_draws=None, group=None):
+        """The test's p-value. Under torch.distributed (group: a process group, or the default one
+        when it is initialized) every rank certifies p_hat on its own GPU, takes rank 0's band,
+        solves every world-th open draw starting at its rank, and one all_gather of (L, U, solved)
+        gives every rank the whole record; draws are independent, so nothing else is exchanged."""
         t0 = time.perf_counter()
+        rank, world, group = _dist(group)
         if self.L0 is None:
             self._certify()
+            if world > 1:
+                self.L0, self.U0 = _broadcast_band(self.L0, self.U0, group)
             self._screen()
         if self.U0 > ZERO:
             dec = decide(self.L, self.U, *self.tau)
             todo = np.flatnonzero((dec == UNDECIDED) & ~self.solved)
             if max_draws is not None:
                 todo = todo[:max_draws]
-            if todo.size:
-                self.solve_draws(todo)
+            mine = todo[rank::world] if world > 1 else todo
+            if mine.size:
+                self.solve_draws(mine)
+            if world > 1:
+                self.L, self.U, self.solved = _gather_record(self.L, self.U, self.solved, group)
         dec = decide(self.L, self.U, *self.tau)
         above = int((dec == ABOVE).sum())
         und = int((dec == UNDECIDED).sum())
