@@ -1,5 +1,7 @@
 """Flow-CG pricing on the GPU through the C ABI: bit-exact against the oracle (values, rankings,
 quantization steps) in every storage mode, and column-for-column equal CG trajectories."""
+import os
+
 import numpy as np
 import pytest
 
@@ -111,3 +113,32 @@ def test_cg_columns_on_config3_residuals(ctx):
 def test_pricer_rejects_bad_rows(ctx):
     with pytest.raises(_lib.RumbError):
         _lib.Pricer(ctx, 4, np.array([3, 4], dtype=np.uint64), np.array([0, 1, 2, 2, 2]), mode="u24")
+
+
+_REPLAY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "pricer_replay.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(_REPLAY), reason="reference kernel outputs not recorded")
+def test_pricer_matches_recorded_reference_kernels(ctx):
+    """Every stream mode and the mask sweep against the outputs the reference's own kernels gave
+    (tests/golden/make_replay_golden.py), bit for bit, n = 8 .. 18."""
+    import make_replay_golden as MR
+    g = np.load(_REPLAY)
+    for name, n, m, a, p in MR.cases():
+        menus, alts, p32, offsets, _ = O.cg_layout(n, m, a, p)
+        for mode in ("f32", "u16", "u24") + (("mask",) if n <= 16 else ()):
+            pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+            for trial in range(2):
+                key = "%s_t%d" % (name, trial)
+                s = g[key + "_scores"]
+                if mode == "mask":
+                    v, r, _ = pr.price(s)
+                    assert np.float32(v) == g[key + "_mask_vmax"]
+                    np.testing.assert_array_equal(r, g[key + "_mask_rank"])
+                    continue
+                v, r, mg, steps = pr.price(s, want_steps=True)
+                assert np.float32(v) == g["%s_%s_vmax" % (key, mode)], (key, mode)
+                np.testing.assert_array_equal(r, g["%s_%s_rank" % (key, mode)])
+                np.testing.assert_array_equal(np.asarray(steps, np.float32), g["%s_%s_steps" % (key, mode)])
+                assert abs(mg - float(g["%s_%s_margin" % (key, mode)])) <= 1e-6 * max(1.0, mg)
+            pr.close()

@@ -155,3 +155,32 @@ def test_oracle_cg_loop_closes_small_instance():
     r = O.cg_solve(8, cd[:, 0], cd[:, 1], cd[:, 2], mode="u24", max_iters=300, gap_abs_tol=1e-6)
     assert r["stop"] == "gap_abs"
     assert r["lb"] <= r["ub"] + 1e-12
+
+
+REPLAY = os.path.join(GOLD, "pricer_replay.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(REPLAY), reason="reference kernel outputs not recorded")
+def test_oracle_pricer_matches_recorded_reference_kernels():
+    """The oracle's stream pricers (fma decode) and mask sweep against the outputs the reference's
+    own kernels gave on a B200 (tests/golden/make_replay_golden.py), bit for bit; the n = 18 case is
+    left to the GPU test (minutes of oracle time)."""
+    import make_replay_golden as MR
+    g = np.load(REPLAY)
+    for name, n, m, a, p in MR.cases():
+        if n > 16:
+            continue
+        menus, alts, p32, offsets, _ = O.cg_layout(n, m, a, p)
+        for trial in range(2):
+            key = "%s_t%d" % (name, trial)
+            s = g[key + "_scores"]
+            np.testing.assert_array_equal(s, MR.scores_for(name, menus.size, trial))
+            for mode in ("f32", "u16", "u24"):
+                v, r, mg, steps = O.price_stream(n, menus, s, offsets, mode=mode)
+                assert np.float32(v) == g["%s_%s_vmax" % (key, mode)], (key, mode)
+                np.testing.assert_array_equal(r, g["%s_%s_rank" % (key, mode)])
+                np.testing.assert_array_equal(np.asarray(steps, np.float32), g["%s_%s_steps" % (key, mode)])
+                assert abs(mg - float(g["%s_%s_margin" % (key, mode)])) <= 1e-6 * max(1.0, mg)
+            v, r = O.price_mask(n, menus, s, offsets)
+            assert np.float32(v) == g[key + "_mask_vmax"]
+            np.testing.assert_array_equal(r, g[key + "_mask_rank"])
