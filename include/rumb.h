@@ -178,6 +178,10 @@ typedef struct {
     int slots;            /* draws resident at once; 0 = as many as fit mem_fraction of free memory */
     double mem_fraction;  /* share of free device memory the slots may take (0 = 0.8) */
     double draw_time;     /* seconds per draw (<= 0: none) */
+    const double *y0;     /* NULL, or B x mp predicted fits: each draw's bracket starts from the
+                             Frank-Wolfe lower bound at its y0 (certified for any y0) */
+    int y0_state;         /* with y0: also write y0 into the start state's observed entries */
+    double *p_fit;        /* NULL, or B x mp out: each draw's best upper-bound point on the rows */
 } rumb_batch_params;
 
 typedef struct {
@@ -239,6 +243,35 @@ typedef struct {
  * library's counterpart of the reference's per-phase timers (solver/flow_cg/solver.py:174-188). */
 RUMB_API int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int warmup,
                              int iters, rumb_kernel_stat *stats, int cap, int *count);
+
+/* ---------------------------------------------------------------- learned warm start
+ * No counterpart in the reference. A small multilayer perceptron (BF16 weights and activations,
+ * FP32 accumulation and master weights, GELU after every layer but the last, mean-squared-error
+ * loss, Adam) whose matrix products run on the tensor cores (tcgen05); the bootstrap trains it on
+ * solved draws to predict a new draw's fitted cells. */
+typedef struct rumb_mlp rumb_mlp;
+
+/* C[M x N] = A[M x K] . B[N x K]^T on the tensor cores: A and B bf16 (16-bit patterns), row-major;
+ * C float32; M and N multiples of 128, K a multiple of 64. Host buffers. */
+RUMB_API int rumb_gemm_bf16(rumb_ctx *ctx, int M, int N, int K, const uint16_t *A, const uint16_t *B, float *C);
+/* n_layers layers of widths dims[0] -> dims[1] -> ... -> dims[n_layers]; weights drawn
+ * uniform(+-1/sqrt(fan_in)) from seed. */
+RUMB_API int rumb_mlp_create(rumb_ctx *ctx, int n_layers, const int *dims, unsigned long long seed,
+                             rumb_mlp **out);
+RUMB_API int rumb_mlp_destroy(rumb_mlp *mlp);
+/* parameters in the layout of get/set_params: per layer W (dims[l+1] x dims[l], row-major), then b */
+RUMB_API int rumb_mlp_num_params(rumb_mlp *mlp, long long *count);
+RUMB_API int rumb_mlp_get_params(rumb_mlp *mlp, float *params);
+RUMB_API int rumb_mlp_set_params(rumb_mlp *mlp, const float *params);
+/* Y[rows x dims[L]] = the network at X[rows x dims[0]] (float32 host rows) */
+RUMB_API int rumb_mlp_forward(rumb_mlp *mlp, const float *X, long long rows, float *Y);
+/* loss = mean over rows x dims[L] of (net(X) - T)^2 and, if grad is not NULL, its gradient in the
+ * parameter layout (rows <= 16384) */
+RUMB_API int rumb_mlp_loss_grad(rumb_mlp *mlp, const float *X, const float *T, long long rows, double *loss,
+                                float *grad);
+/* epochs of Adam (lr) over shuffled mini-batches of `batch` rows; loss = the last epoch's mean */
+RUMB_API int rumb_mlp_train(rumb_mlp *mlp, const float *X, const float *T, long long rows, int epochs, int batch,
+                            double lr, unsigned long long seed, double *loss);
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,7 @@
 
 #include "bm.cuh"
 #include "ctx.cuh"
+#include "mlp.cuh"
 #include "pricer.cuh"
 
 namespace rumb {
@@ -258,6 +259,107 @@ int rumb_cg_pricer_destroy(rumb_cg_pricer *pr) {
         rumb::pricer_destroy(pr->p);
     }
     delete pr;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+// ---------------------------------------------------------------- tensor-core GEMM and MLP
+struct rumb_mlp {
+    rumb_ctx *ctx = nullptr;
+    rumb::Mlp *m = nullptr;
+};
+
+#define NEED_MLP(h)                                                    \
+    if (!(h) || !(h)->m) rumb::fail(RUMB_E_INVAL, "mlp is NULL");      \
+    rumb::DeviceGuard _dg((h)->ctx->c.device)
+
+int rumb_gemm_bf16(rumb_ctx *ctx, int M, int N, int K, const uint16_t *A, const uint16_t *B, float *C) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    return rumb::gemm_bf16_host(ctx->c, M, N, K, A, B, C);
+    RUMB_API_END
+}
+
+int rumb_mlp_create(rumb_ctx *ctx, int n_layers, const int *dims, unsigned long long seed, rumb_mlp **out) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    if (!out) rumb::fail(RUMB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    rumb_mlp *h = new rumb_mlp();
+    h->ctx = ctx;
+    try {
+        h->m = rumb::mlp_create(ctx->c, n_layers, dims, seed);
+    } catch (...) {
+        delete h;
+        throw;
+    }
+    *out = h;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_destroy(rumb_mlp *h) {
+    RUMB_API_BEGIN
+    if (!h) return RUMB_OK;
+    if (h->m) {
+        rumb::DeviceGuard dg(h->ctx->c.device);
+        rumb::mlp_destroy(h->m);
+    }
+    delete h;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_num_params(rumb_mlp *h, long long *count) {
+    RUMB_API_BEGIN
+    NEED_MLP(h);
+    if (!count) rumb::fail(RUMB_E_INVAL, "count is NULL");
+    *count = rumb::mlp_num_params(*h->m);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_get_params(rumb_mlp *h, float *params) {
+    RUMB_API_BEGIN
+    NEED_MLP(h);
+    if (!params) rumb::fail(RUMB_E_INVAL, "params is NULL");
+    rumb::mlp_get_params(*h->m, params, false);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_set_params(rumb_mlp *h, const float *params) {
+    RUMB_API_BEGIN
+    NEED_MLP(h);
+    if (!params) rumb::fail(RUMB_E_INVAL, "params is NULL");
+    rumb::mlp_set_params(*h->m, params);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_forward(rumb_mlp *h, const float *X, long long rows, float *Y) {
+    RUMB_API_BEGIN
+    NEED_MLP(h);
+    rumb::mlp_forward(*h->m, X, rows, Y);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_loss_grad(rumb_mlp *h, const float *X, const float *T, long long rows, double *loss, float *grad) {
+    RUMB_API_BEGIN
+    NEED_MLP(h);
+    double l = rumb::mlp_loss_grad(*h->m, X, T, rows, grad);
+    if (loss) *loss = l;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_mlp_train(rumb_mlp *h, const float *X, const float *T, long long rows, int epochs, int batch, double lr,
+                   unsigned long long seed, double *loss) {
+    RUMB_API_BEGIN
+    NEED_MLP(h);
+    double l = rumb::mlp_train(*h->m, X, T, rows, epochs, batch, lr, seed);
+    if (loss) *loss = l;
     return RUMB_OK;
     RUMB_API_END
 }

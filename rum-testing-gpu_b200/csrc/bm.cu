@@ -289,15 +289,16 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 }
 
 // Result slots of one check (device doubles)
-enum { R_PHI2 = 0, R_RY = 1, R_UB_NOW = 2, R_UB_BEST = 3, R_LB_NOW = 4, R_SLOTS = 8 };
+enum { R_PHI2 = 0, R_RY = 1, R_UB_NOW = 2, R_UB_BEST = 3, R_LB_NOW = 4, R_LB_SEED = 5, R_SLOTS = 8 };
 
 // phi^2 = sum (p - x2[obs])^2 and sum (p - y) y at the iterate; LB scatter g[obs] = r if g
 template <class T>
-__global__ void obs_stats_kernel(const T *x2, const ll *obs, const double *p, ll mp, double *g, double *res) {
+__global__ void obs_stats_kernel(const T *x2, const ll *obs, const double *p, ll mp, double *g, double *res,
+                                 const double *yv = nullptr) {
     __shared__ double sh[32];
     double f = 0.0, ry = 0.0;
     for (ll j = threadIdx.x; j < mp; j += blockDim.x) {
-        double y = (double)x2[obs[j]];
+        double y = yv ? yv[j] : (double)x2[obs[j]];     // yv: the observed values given directly
         double r = p[j] - y;
         f += r * r;
         ry += r * y;
@@ -443,10 +444,11 @@ static CertWork &cert_work(Ctx &c) {
 // UB part of a check: x2 (dtype T) -> q = Mobius -> push -> zeta -> ub_now, pfit; running best.
 template <class T>
 static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t st, const double *p_ovr = nullptr,
-                         double *res_ovr = nullptr) {
+                         double *res_ovr = nullptr, double *pfit_ovr = nullptr) {
     const double *pp = p_ovr ? p_ovr : W.p.as<double>();
     double *rr = res_ovr ? res_ovr : W.res.as<double>();
-    const bool commit = res_ovr == nullptr;            // batched draws keep no p_fit
+    // the best point's observed values: the workspace's own, a batched draw's own row, or none
+    double *pfit_best = res_ovr == nullptr ? W.pfit_best.as<double>() : pfit_ovr;
     ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
     const double eps = 1e-12;
     double *qa = W.qa.as<double>(), *qb = W.qb.as<double>();
@@ -470,9 +472,8 @@ static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t s
     xf_transform<double, double>(n, qb, qa, Co<double>{1.0, 1.0, 0.0, 1.0}, st);  // zeta -> x_ub in qa
     ub_eval_kernel<<<1, RED_THREADS, 0, st>>>(qa, W.obs.as<ll>(), pp, W.mp, W.pfit_cur.as<double>(), rr);
     RUMB_LAUNCH("ub_eval_kernel");
-    if (commit) {
-        ub_commit_kernel<<<grid_for(W.mp, 256), 256, 0, st>>>(W.pfit_cur.as<double>(), W.pfit_best.as<double>(), W.mp,
-                                                             rr);
+    if (pfit_best) {
+        ub_commit_kernel<<<grid_for(W.mp, 256), 256, 0, st>>>(W.pfit_cur.as<double>(), pfit_best, W.mp, rr);
         RUMB_LAUNCH("ub_commit_kernel");
     }
     ub_best_kernel<<<1, 32, 0, st>>>(rr);
@@ -482,13 +483,13 @@ static void enqueue_push(Ctx &c, CertWork &W, int n, const T *x2, cudaStream_t s
 // phi (and the LB's residual sums); with_lb also scatters g and runs the longest path.
 template <class T>
 static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_lb, cudaStream_t st,
-                             const double *p_ovr = nullptr, double *res_ovr = nullptr) {
+                             const double *p_ovr = nullptr, double *res_ovr = nullptr, const double *y_ovr = nullptr) {
     const double *pp = p_ovr ? p_ovr : W.p.as<double>();
     double *rr = res_ovr ? res_ovr : W.res.as<double>();
     ll Nloc = 1LL << (n - 1), m2 = (ll)n * Nloc, N = 1LL << n;
     double *g = W.qb.as<double>();
     if (with_lb) RUMB_CUDA(cudaMemsetAsync(g, 0, (size_t)m2 * 8, st));
-    obs_stats_kernel<T><<<1, RED_THREADS, 0, st>>>(x2, W.obs.as<ll>(), pp, W.mp, with_lb ? g : nullptr, rr);
+    obs_stats_kernel<T><<<1, RED_THREADS, 0, st>>>(x2, W.obs.as<ll>(), pp, W.mp, with_lb ? g : nullptr, rr, y_ovr);
     RUMB_LAUNCH("obs_stats_kernel");
     if (!with_lb) return;
     xf_transform<double, double>(n, g, g, Co<double>{1.0, 0.0, 1.0, 1.0}, st);    // subset sums
@@ -582,26 +583,6 @@ static BmCoef make_coef(int n, double beta, double alpha, double p) {
     return C;
 }
 
-template <class T>
-static void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots = 1) {
-    size_t smem = prox_tile_smem<T>(P.n);
-    dim3 grid((unsigned)(1LL << (P.n - PT_M)), (unsigned)slots);
-#define RUMB_PT_CASE(NN)                                                                                   \
-    if (P.n <= NN) {                                                                                       \
-        static bool attr = false;                                                                          \
-        if (!attr) {                                                                                       \
-            RUMB_CUDA(cudaFuncSetAttribute(prox_tile_kernel<T, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                           (int)prox_tile_smem<T>(NN)));                                   \
-            attr = true;                                                                                   \
-        }                                                                                                  \
-        prox_tile_kernel<T, NN><<<grid, PT_THREADS, smem, st>>>(P);                                        \
-        RUMB_LAUNCH("prox_tile_kernel");                                                                   \
-        return;                                                                                            \
-    }
-    RUMB_PT_CASE(30)
-#undef RUMB_PT_CASE
-    fail(RUMB_E_INVAL, "prox: n > 30");
-}
 
 // The reference's one_iter (solver/bm_admm/solver.py:240-254) for n <= 5: separate butterflies.
 template <class T>
@@ -831,8 +812,7 @@ static void setup_obs(Ctx &c, CertWork &CW, BmWork<T> *W, const rumb_bm_problem 
     RUMB_LAUNCH("obs_setup_kernel");
     RUMB_CUDA(cudaMemcpyAsync(CW.p.ptr, D.d_p, (size_t)pr.mp * 8, cudaMemcpyDeviceToDevice, st));
     if (W) {
-        menu_obs_kernel<<<grid_for(1LL << n, 256), 256, 0, st>>>(bits, n, Nloc, W->menu_obs.template as<uint32_t>());
-        RUMB_LAUNCH("menu_obs_kernel");
+        launch_menu_obs(bits, n, Nloc, W->menu_obs.template as<uint32_t>(), st);
     }
     int hbad = 0;
     RUMB_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, st));
@@ -1282,6 +1262,17 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
 // float64 check, and the host retires finished draws and refills their slots from the queue.
 // Slots are admitted by device memory: K = min(B, mem_fraction * free / bytes per slot).
 
+// x[obs[j]] = y[j]: a draw's predicted fit written into its state's observed entries
+template <class T>
+__global__ void scatter_vals_kernel(const ll *obs, const double *y, ll mp, T *x) {
+    ll j = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (j < mp) x[obs[j]] = (T)y[j];
+}
+
+__global__ void copy_double_kernel(double *dst, const double *src) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *src;
+}
+
 __global__ void scatter_rows_kernel(const ll *obs, const double *p, ll mp, double *p_dst, float *xf, double *xd) {
     ll j = blockIdx.x * (ll)blockDim.x + threadIdx.x;
     if (j >= mp) return;
@@ -1294,7 +1285,7 @@ __global__ void scatter_rows_kernel(const ll *obs, const double *p, ll mp, doubl
 template <class T>
 struct BatchWork : public BmWorkBase {
     DevBuf x2, s, y, z, x, Ax, t1, t2, xhat;   // K slabs each
-    DevBuf obsbits, menu_obs, diag, err, active, p, res;
+    DevBuf obsbits, menu_obs, diag, err, active, p, res, pfit;
     int K = 0, n = 0;
     ll mp = 0;
     void ensure(int n_, ll mp_, int K_) {
@@ -1308,6 +1299,7 @@ struct BatchWork : public BmWorkBase {
         err.ensure(16);
         active.ensure((size_t)K * 4);
         p.ensure((size_t)K * (size_t)mp * 8);
+        pfit.ensure((size_t)K * (size_t)mp * 8);
         res.ensure((size_t)K * R_SLOTS * 8);
     }
 };
@@ -1315,7 +1307,7 @@ struct BatchWork : public BmWorkBase {
 template <class T>
 static size_t batch_slot_bytes(int n, ll mp) {
     ll m2 = (ll)n << (n - 1);
-    return (size_t)9 * (size_t)m2 * sizeof(T) + (size_t)mp * 8 + R_SLOTS * 8;
+    return (size_t)9 * (size_t)m2 * sizeof(T) + (size_t)mp * 16 + R_SLOTS * 8;
 }
 
 template <class T>
@@ -1357,9 +1349,7 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
                                                                CW.obs.as<ll>(), W.xhat.template as<T>(),
                                                                W.obsbits.template as<uint32_t>(), bad.as<int>());
         RUMB_LAUNCH("obs_setup_kernel");
-        menu_obs_kernel<<<grid_for(1LL << n, 256), 256, 0, st>>>(W.obsbits.template as<uint32_t>(), n, 1LL << (n - 1),
-                                                               W.menu_obs.template as<uint32_t>());
-        RUMB_LAUNCH("menu_obs_kernel");
+        launch_menu_obs(W.obsbits.template as<uint32_t>(), n, 1LL << (n - 1), W.menu_obs.template as<uint32_t>(), st);
         int hbad = 0;
         RUMB_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaStreamSynchronize(st));
@@ -1385,6 +1375,13 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
     DevBuf pbuf;                                    // the draws' rows, uploaded once
     pbuf.ensure((size_t)B * (size_t)mp * 8);
     RUMB_CUDA(cudaMemcpyAsync(pbuf.ptr, P, (size_t)B * (size_t)mp * 8, cudaMemcpyHostToDevice, st));
+    const double *y0 = bp ? bp->y0 : nullptr;       // predicted fits: a lower-bound seed per draw
+    double *fit_out = bp ? bp->p_fit : nullptr;
+    DevBuf ybuf;
+    if (y0) {
+        ybuf.ensure((size_t)B * (size_t)mp * 8);
+        RUMB_CUDA(cudaMemcpyAsync(ybuf.ptr, y0, (size_t)B * (size_t)mp * 8, cudaMemcpyHostToDevice, st));
+    }
     std::vector<int> act(K, 0), draw_of(K, -1);
     std::vector<ll> it_of(K, 0);
     std::vector<double> ub_of(K, INFINITY), lb_of(K, 0.0), phi_of(K, NAN);
@@ -1430,6 +1427,19 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
             launch_prox_n<T, PROX_ONLY>(Pa, st);
             for (int i = 1; i < 4; ++i) RUMB_CUDA(cudaMemsetAsync(dst[i], 0, (size_t)m2 * sizeof(T), st));
         }
+        if (y0) {
+            // the Frank-Wolfe bound at the prediction is a certified lower bound for any y0: the
+            // draw's bracket starts from it (R_LB_SEED); y0_state also moves the state's observed
+            // entries to the prediction
+            const double *yb = ybuf.as<double>() + (size_t)b * mp;
+            if (bp->y0_state) {
+                scatter_vals_kernel<T><<<grid_for(mp, 256), 256, 0, st>>>(CW.obs.as<ll>(), yb, mp, dst[0]);
+                RUMB_LAUNCH("scatter_vals_kernel");
+            }
+            enqueue_stats_lb<T>(c, CW, n, dst[0], true, st, pk, rk, yb);
+            copy_double_kernel<<<1, 32, 0, st>>>(rk + R_LB_SEED, rk + R_LB_NOW);
+            RUMB_LAUNCH("copy_double_kernel");
+        }
     };
     for (int k = 0; k < K; ++k) admit(k);
     RUMB_CUDA(cudaMemcpyAsync(W.active.ptr, act.data(), (size_t)K * 4, cudaMemcpyHostToDevice, st));
@@ -1460,7 +1470,7 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
             double *rk = W.res.template as<double>() + (size_t)k * R_SLOTS;
             bool want_lb = (npush_of[k] % par->lb_every) == 0;
             enqueue_stats_lb<T>(c, CW, n, x2k, want_lb, st, pk, rk);
-            enqueue_push<T>(c, CW, n, x2k, st, pk, rk);
+            enqueue_push<T>(c, CW, n, x2k, st, pk, rk, fit_out ? W.pfit.template as<double>() + (size_t)k * mp : nullptr);
         }
         total_iters += (ll)nact * par->check;
         RUMB_CUDA(cudaMemcpyAsync(res.data(), W.res.ptr, res.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -1477,6 +1487,7 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
             phi_of[k] = std::sqrt(r[R_PHI2]);
             ub_of[k] = r[R_UB_BEST];
             if (want_lb) { nlb_of[k]++; if (r[R_LB_NOW] > lb_of[k]) lb_of[k] = r[R_LB_NOW]; }
+            if (r[R_LB_SEED] > lb_of[k]) lb_of[k] = r[R_LB_SEED];
             int b = draw_of[k];
             int stop = 0;
             double gap = ub_of[k] - lb_of[k];
@@ -1501,6 +1512,9 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
             o.iters_f32 = sizeof(T) == 4 ? it_of[k] : 0; o.stop = stop; o.n_push = npush_of[k]; o.n_lb = nlb_of[k];
             o.setup_s = 0.0; o.solve_s = secs(t_of[k], Clock::now()); o.push_s = 0.0;
             o.per_iter_ms = 0.0; o.device_ms = 0.0;
+            if (fit_out)
+                RUMB_CUDA(cudaMemcpyAsync(fit_out + (size_t)b * mp, W.pfit.template as<double>() + (size_t)k * mp,
+                                          (size_t)mp * 8, cudaMemcpyDeviceToHost, st));
             ++done;
             admit(k);
             changed = true;
@@ -1514,6 +1528,9 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
         o.lb = lb_of[k]; o.ub = ub_of[k]; o.phi = phi_of[k]; o.iters = it_of[k];
         o.iters_f32 = sizeof(T) == 4 ? it_of[k] : 0; o.stop = RUMB_STOP_TIME; o.n_push = npush_of[k];
         o.n_lb = nlb_of[k]; o.solve_s = secs(t_of[k], Clock::now());
+        if (fit_out)
+            RUMB_CUDA(cudaMemcpyAsync(fit_out + (size_t)draw_of[k] * mp, W.pfit.template as<double>() + (size_t)k * mp,
+                                      (size_t)mp * 8, cudaMemcpyDeviceToHost, st));
     }
     for (int b = next; b < B; ++b) {
         out[b] = rumb_bm_result{};

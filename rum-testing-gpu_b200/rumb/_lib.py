@@ -54,7 +54,8 @@ class BMResult(ctypes.Structure):
 
 
 class BatchParams(ctypes.Structure):
-    _fields_ = [("slots", ctypes.c_int), ("mem_fraction", ctypes.c_double), ("draw_time", ctypes.c_double)]
+    _fields_ = [("slots", ctypes.c_int), ("mem_fraction", ctypes.c_double), ("draw_time", ctypes.c_double),
+                ("y0", ctypes.c_void_p), ("y0_state", ctypes.c_int), ("p_fit", ctypes.c_void_p)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -74,6 +75,16 @@ TRACE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_d
 _vp = ctypes.c_void_p
 _SIGS = {
     "rumb_version": ([], ctypes.c_int),
+    "rumb_gemm_bf16": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
+    "rumb_mlp_create": ([_vp, ctypes.c_int, _vp, ctypes.c_ulonglong, ctypes.POINTER(_vp)], ctypes.c_int),
+    "rumb_mlp_destroy": ([_vp], ctypes.c_int),
+    "rumb_mlp_num_params": ([_vp, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "rumb_mlp_get_params": ([_vp, _vp], ctypes.c_int),
+    "rumb_mlp_set_params": ([_vp, _vp], ctypes.c_int),
+    "rumb_mlp_forward": ([_vp, _vp, ctypes.c_longlong, _vp], ctypes.c_int),
+    "rumb_mlp_loss_grad": ([_vp, _vp, _vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
+    "rumb_mlp_train": ([_vp, _vp, _vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                        ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "rumb_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
     "rumb_ctx_create": ([ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
     "rumb_ctx_destroy": ([_vp], ctypes.c_int),
@@ -282,8 +293,10 @@ class Context:
         return out, fit, (BMState(kept) if keep and kept.value else None)
 
     def bm_solve_batch(self, problem, params, P, below=None, above=None, warm=None, slots=0, mem_fraction=0.8,
-                       draw_time=0.0):
-        """Solves the rows of P (B x mp) together; (list of result dicts, info dict)."""
+                       draw_time=0.0, y0=None, y0_state=False, want_fit=False):
+        """Solves the rows of P (B x mp) together; (list of result dicts, info dict). y0 (B x mp):
+        predicted fits, whose Frank-Wolfe lower bounds seed the brackets (y0_state: and the start
+        states); want_fit: each result dict gets its draw's "p_fit" row."""
         pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
         P = np.ascontiguousarray(P, dtype=np.float64)
         if P.ndim != 2 or P.shape[1] != pr.mp:
@@ -293,14 +306,21 @@ class Context:
         hi = None if above is None else np.ascontiguousarray(np.broadcast_to(above, (B,)), dtype=np.float64)
         res = (BMResult * B)()
         info = BatchInfo()
-        bp = BatchParams(int(slots), float(mem_fraction), float(draw_time))
+        yy = None if y0 is None else np.ascontiguousarray(y0, dtype=np.float64)
+        if yy is not None and yy.shape != P.shape:
+            raise ValueError("y0 must have P's shape")
+        fits = np.zeros(P.shape, dtype=np.float64) if want_fit else None
+        bp = BatchParams(int(slots), float(mem_fraction), float(draw_time), _p(yy) if yy is not None else None,
+                         int(bool(y0_state)), _p(fits) if fits is not None else None)
         check(load().rumb_bm_solve_batch(self.h, ctypes.byref(pr), ctypes.byref(params), ctypes.byref(bp), B, _p(P),
                                          _p(lo) if lo is not None else None, _p(hi) if hi is not None else None,
                                          warm.h if warm else None, res, ctypes.byref(info)))
         out = []
-        for r in res:
+        for b, r in enumerate(res):
             d = {f: getattr(r, f) for f, _ in BMResult._fields_}
             d["stop_reason"] = STOP.get(r.stop, "unknown")
+            if fits is not None:
+                d["p_fit"] = fits[b]
             out.append(d)
         return out, {f: getattr(info, f) for f, _ in BatchInfo._fields_}
 
@@ -328,6 +348,83 @@ class Context:
 
 
 PRICE_MODES = {"mask": 0, "f32": 1, "u16": 2, "u24": 3}
+
+
+def to_bf16_bits(x):
+    """float32 -> bfloat16 bit patterns (uint16), round to nearest even."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return (((u + 0x7FFF + ((u >> 16) & 1)) >> 16) & 0xFFFF).astype(np.uint16)
+
+
+def gemm_bf16(ctx, A_bits, B_bits):
+    """C = A . B^T on the tensor cores (A [M x K], B [N x K] bfloat16 bit patterns): float32 C."""
+    A = np.ascontiguousarray(A_bits, dtype=np.uint16)
+    B = np.ascontiguousarray(B_bits, dtype=np.uint16)
+    (M, K), (N, K2) = A.shape, B.shape
+    if K != K2:
+        raise ValueError("A and B must share K")
+    C = np.empty((M, N), dtype=np.float32)
+    check(load().rumb_gemm_bf16(ctx.h, M, N, K, _p(A), _p(B), _p(C)))
+    return C
+
+
+class MLP:
+    """The tensor-core MLP (rumb_mlp_*): widths dims[0] -> ... -> dims[-1], GELU between layers."""
+
+    def __init__(self, ctx, dims, seed=0):
+        self.ctx, self.dims = ctx, [int(d) for d in dims]
+        d = np.asarray(self.dims, dtype=np.int32)
+        h = ctypes.c_void_p()
+        check(load().rumb_mlp_create(ctx.h, len(self.dims) - 1, _p(d), int(seed), ctypes.byref(h)))
+        self.h = h
+        n = ctypes.c_longlong()
+        check(load().rumb_mlp_num_params(self.h, ctypes.byref(n)))
+        self.num_params = int(n.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rumb_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        out = np.empty(self.num_params, dtype=np.float32)
+        check(load().rumb_mlp_get_params(self.h, _p(out)))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.num_params:
+            raise ValueError("expected %d parameters" % self.num_params)
+        check(load().rumb_mlp_set_params(self.h, _p(p)))
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.empty((X.shape[0], self.dims[-1]), dtype=np.float32)
+        check(load().rumb_mlp_forward(self.h, _p(X), X.shape[0], _p(Y)))
+        return Y
+
+    def loss_grad(self, X, T, want_grad=True):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        loss = ctypes.c_double()
+        g = np.empty(self.num_params, dtype=np.float32) if want_grad else None
+        check(load().rumb_mlp_loss_grad(self.h, _p(X), _p(T), X.shape[0], ctypes.byref(loss),
+                                        _p(g) if g is not None else None))
+        return loss.value, g
+
+    def train(self, X, T, epochs=20, batch=256, lr=1e-3, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        loss = ctypes.c_double()
+        check(load().rumb_mlp_train(self.h, _p(X), _p(T), X.shape[0], int(epochs), int(batch), float(lr), int(seed),
+                                    ctypes.byref(loss)))
+        return loss.value
 
 
 class Pricer:

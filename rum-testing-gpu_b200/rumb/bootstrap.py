@@ -18,6 +18,11 @@ solver/inference/draws.py:161-290), with its formulas and decisions:
               flow_cg one at a time through the Session, as the reference does. A float32 or mixed
               session solves the batch in float32; draws whose bracket stalls undecided are solved
               again in float64
+    learned   (learned=True, bm_admm) the first train_draws solved draws train a small BF16 network
+              on the tensor cores (rumb_mlp_*) to map a draw's cells to its fitted cells; every
+              later draw starts from the prediction: its bracket from the Frank-Wolfe lower bound
+              at the prediction (certified whatever the prediction) and its start state's fitted
+              cells moved there. A poor prediction costs iterations, never correctness
     p-value   p = (#above + #undecided) / B
 
 Respondent weights: "multinomial" (R picks with replacement per draw) and "multinomial_reject"
@@ -167,7 +172,8 @@ def _gather_record(L, U, solved, group):
 class Bootstrap:
     def __init__(self, rum, n=None, panel=None, replies=None, B=None, weights=None, seed=None, r_n=None, eps_n=None,
                  method=None, method_args=None, abs_tol=None, rel_tol=None, max_time=None, draw_time=None,
-                 batch_slots=0, verbose=False):
+                 batch_slots=0, verbose=False, learned=False, train_draws=512, mlp_hidden=(1024, 1024, 1024),
+                 mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=True, seed_net=0):
         d = defaults.BOOTSTRAP
         if panel is None or replies is not None:
             raise ValueError("this bootstrap takes a respondent panel (panel=)")
@@ -186,6 +192,13 @@ class Bootstrap:
         self.L, self.U = np.zeros(self.B), np.full(self.B, np.inf)
         self.solved = np.zeros(self.B, dtype=bool)
         self.n_refined = 0          # float32 draws that stalled undecided and finished in float64
+        self.iters = np.zeros(self.B, dtype=np.int64)
+        self.slot_iters = 0         # iterations the batched solves ran, summed over draws
+        # learned warm start: a network trained on solved draws predicts a draw's fitted cells
+        self.learned, self.train_draws = bool(learned), int(train_draws)
+        self.mlp_hidden, self.mlp_epochs, self.mlp_batch = tuple(mlp_hidden), int(mlp_epochs), int(mlp_batch)
+        self.mlp_lr, self.y0_state, self.seed_net = float(mlp_lr), bool(y0_state), int(seed_net)
+        self.net, self.learned_info = None, None
         self.L0 = self.U0 = None
         self.verbose = verbose
         self.time = dict(certificate=0.0, screen=0.0, solve=0.0)
@@ -212,8 +225,62 @@ class Bootstrap:
         self.n_screened = int((self.U < self.tau[0]).sum())
         self.time["screen"] += time.perf_counter() - t0
 
+    def _batch(self, ctx, prob, par, P, below, above, y0=None, want_fit=False):
+        """One batched solve of the rows P; a float32 batch's draws whose bracket stalls undecided
+        are solved again in float64. The result dicts, in P's order."""
+        s = self.session
+        res, info = ctx.bm_solve_batch(prob, par, P, below=below, above=above, warm=s._kept, slots=self.batch_slots,
+                                       draw_time=self.draw_time, y0=y0, y0_state=self.y0_state and y0 is not None,
+                                       want_fit=want_fit)
+        self.last_batch = info
+        self.slot_iters += int(info["total_iters"])
+        if par.dtype == 1:
+            lo = -np.inf if below is None else below
+            hi = np.inf if above is None else above
+            L = np.array([r["lb"] for r in res])
+            U = np.array([r["ub"] for r in res])
+            dec = decide(L, U, lo, hi)
+            redo = [j for j in range(len(res)) if res[j]["stop_reason"] == "stall" and
+                    (below is None or dec[j] == UNDECIDED)]
+            if redo:
+                par.dtype = 0
+                res2, info2 = ctx.bm_solve_batch(prob, par, P[redo], below=below, above=above, warm=s._kept,
+                                                 slots=self.batch_slots, draw_time=self.draw_time,
+                                                 y0=None if y0 is None else y0[redo],
+                                                 y0_state=self.y0_state and y0 is not None, want_fit=want_fit)
+                par.dtype = 1
+                self.slot_iters += int(info2["total_iters"])
+                for j, r in zip(redo, res2):
+                    r["lb"], r["ub"] = max(r["lb"], res[j]["lb"]), min(r["ub"], res[j]["ub"])
+                    res[j] = r
+                self.n_refined += len(redo)
+                self.last_batch_f64 = info2
+        return res
+
+    def _train_net(self, P, fits):
+        """Fits the network on solved draws: (P_b - p_hat) -> (p_fit_b - p_fit(p_hat)), scaled."""
+        from . import _lib
+        from .rum_solver import context
+        X = P - self.p_hat
+        Y = fits - self.session.fit
+        self.x_scale = float(np.std(X)) or 1.0
+        self.y_scale = float(np.std(Y)) or 1.0
+        mp = P.shape[1]
+        if mp > 16384:
+            raise ValueError("the learned warm start takes at most 16384 observed cells; got %d" % mp)
+        self.net = _lib.MLP(context(), [mp] + list(self.mlp_hidden) + [mp], seed=self.seed_net)
+        loss = self.net.train(X / self.x_scale, Y / self.y_scale, epochs=self.mlp_epochs, batch=self.mlp_batch,
+                              lr=self.mlp_lr, seed=self.seed_net)
+        self.learned_info = dict(n_train=int(P.shape[0]), train_loss=loss)
+
+    def predict_fit(self, P):
+        """The network's predicted fitted cells for the draws' rows P."""
+        return self.session.fit + self.y_scale * self.net.forward((P - self.p_hat) / self.x_scale)
+
     def solve_draws(self, idx, stops=True):
-        """Solve the draws idx: bm_admm all together (batched), flow_cg one at a time."""
+        """Solve the draws idx: bm_admm all together (batched), flow_cg one at a time. With learned=True
+        the first train_draws draws solved train the network, and every later draw starts from its
+        prediction (a certified lower-bound seed and, with y0_state, the start state's fitted cells)."""
         t0 = time.perf_counter()
         idx = np.asarray(idx, dtype=np.int64)
         if idx.size == 0:
@@ -232,31 +299,29 @@ class Bootstrap:
                                 lb_every=a["lb_every"], max_iter=a["max_iter"], abs_tol=self.abs_tol,
                                 rel_tol=self.rel_tol if self.rel_tol > 0 else None, dtype=dt)
             below, above = (tau_lo, tau_hi) if stops else (None, None)
-            res, info = ctx.bm_solve_batch(prob, par, P, below=below, above=above, warm=s._kept,
-                                           slots=self.batch_slots, draw_time=self.draw_time)
+            res = [None] * idx.size
+            todo = np.arange(idx.size)
+            if self.learned and self.net is None:
+                ntr = min(self.train_draws, idx.size)
+                part = self._batch(ctx, prob, par, P[:ntr], below, above, want_fit=True)
+                res[:ntr] = part
+                self._train_net(P[:ntr], np.stack([r["p_fit"] for r in part]))
+                todo = todo[ntr:]
+            if todo.size:
+                y0 = self.predict_fit(P[todo]) if self.net is not None else None
+                part = self._batch(ctx, prob, par, P[todo], below, above, y0=y0)
+                for j, r in zip(todo, part):
+                    res[j] = r
             for j, b in enumerate(idx):
                 self.L[b] = max(self.L[b], res[j]["lb"])
                 self.U[b] = min(self.U[b], res[j]["ub"])
-            self.last_batch = info
-            if dt == "float32":
-                # draws whose float32 bracket stalled before a decision finish in float64
-                dec = decide(self.L[idx], self.U[idx], tau_lo, tau_hi)
-                redo = [j for j in range(idx.size) if res[j]["stop_reason"] == "stall" and
-                        (not stops or dec[j] == UNDECIDED)]
-                if redo:
-                    par.dtype = 0
-                    res2, info2 = ctx.bm_solve_batch(prob, par, P[redo], below=below, above=above, warm=s._kept,
-                                                     slots=self.batch_slots, draw_time=self.draw_time)
-                    for j, r in zip(redo, res2):
-                        b = idx[j]
-                        self.L[b], self.U[b] = max(self.L[b], r["lb"]), min(self.U[b], r["ub"])
-                    self.n_refined += len(redo)
-                    self.last_batch_f64 = info2
+                self.iters[b] = res[j]["iters"]
         else:
             for j, b in enumerate(idx):
                 r = s.solve(P[j], abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_time=self.draw_time, warm=True,
                             below=tau_lo if stops else None, above=tau_hi if stops else None)
                 self.L[b], self.U[b] = max(self.L[b], r.lb), min(self.U[b], r.ub)
+                self.iters[b] = r.iterations
         self.solved[idx] = True
         self.time["solve"] += time.perf_counter() - t0
 
