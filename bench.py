@@ -52,8 +52,9 @@ CHECK = 50
 CERT_ITERS_F64 = 43800
 # iterations run before the profiled ones: the roofline kernel is timed mid-solve
 PROFILE_WARMUP = 2000
-# DRAM bytes per launch of the dominant kernel, from the ncu capture summarised under profiles/
-NCU_TRAFFIC = {}
+# DRAM bytes (read + write) per launch of the dominant kernel, from the ncu capture summarised in
+# profiles/iteration_kernels_n18_f64.md (same workload, float64 state)
+NCU_TRAFFIC = {"prox_tile<f64>": 60.5e6 + 0.516e6}
 
 
 def _env_int(k, d):
@@ -176,6 +177,35 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def pricing_sweeps(ctx, stream, sweeps=20):
+    """Flow-CG pricing at n = 18, 0.5 % menus (workload n18_d05pct_k50): the uint24 and uint16
+    stream sweeps (one full Bellman-Ford pass over the lattice plus the backtrace, read back each
+    sweep), timed with CUDA events on the bench stream; seeded float32 scores resident on the GPU."""
+    import torch
+    from rumb import _lib, flow_cg
+    from rumb.instances import config_instance
+    n, menu, alt, p = config_instance("n18_d05pct_k50", seed=0)
+    menus, alts, p32, offsets, _ = flow_cg.prepare_choice_data(menu, alt, p, n)
+    scores = torch.from_numpy(np.random.default_rng(0).standard_normal(menus.size).astype(np.float32)).cuda()
+    out = {"workload": "n18_d05pct_k50", "rows": int(menus.size), "subset_tests_per_sweep": int(menus.size) << (n - 1)}
+    for mode in ("u24", "u16"):
+        pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+        for _ in range(3):
+            pr.price_device(scores.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(sweeps):
+            pr.price_device(scores.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / sweeps
+        out[mode] = {"ms_per_sweep": ms, "sweeps_per_s": 1e3 / ms,
+                     "subset_tests_per_s": out["subset_tests_per_sweep"] / (ms * 1e-3)}
+        pr.close()
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -283,6 +313,8 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    with torch.cuda.stream(stream):
+        pricing = pricing_sweeps(ctx, stream)
     cpu = None
     if not args.no_cpu:
         v, desc, used = cpu_sample(n, menu, alt, p, 1, int(res["iters"]), int(res["n_push"]), sample_iters=40)
@@ -313,6 +345,7 @@ def main():
                     for k in sorted(prof, key=lambda k: -k["total_ms"])[:8]],
         "gpu_launches": int(launches_dev),
         "cpu_baseline": cpu,
+        "flow_cg_pricing": pricing,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
