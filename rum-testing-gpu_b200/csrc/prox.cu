@@ -1,11 +1,13 @@
 // The per-menu prox tile kernel (formulas and the tile layout in prox.cuh) and its launchers.
 //
-// One thread per menu S; the member loops walk the set bits of S in increasing alternative order
-// (the order of every sum), with the alternatives' run offsets in a shared table. Measured at
-// n = 18 and 20 against two other forms of the same loop (all n alternatives unrolled with a
-// predicate; the five lowest bits and the warp-uniform higher bits walked separately) and against
-// loading x, x2, z straight from the slab into registers: equal in float64, 15-35 % faster in
-// float32.
+// A CTA stages its tile's runs of x, x2 and z in shared memory with 16-byte cp.async copies
+// spread over all its threads (the runs are 64 or 128 values long: many small copies, which this
+// moves faster than one TMA bulk copy per run did: 47 against 50 us at n = 18 float64, 32 against
+// 35 us float32, 104 against 114 us at n = 20 float32), then one thread per menu S walks the
+// members by set bits in increasing alternative order (the order of every sum), and x2 and z
+// leave as 16-byte stores. The member loop by set bits measured equal or faster than two other
+// forms (all alternatives unrolled with a predicate; the five lowest bits and the warp-uniform
+// higher bits walked apart), and staging beat loading x, x2, z straight into registers by a third.
 #include "prox.cuh"
 
 namespace rumb {
@@ -24,7 +26,6 @@ __device__ __forceinline__ uint32_t cb32(uint32_t mask, int x) {
 template <class T, int N>
 __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T> P) {
     extern __shared__ __align__(128) unsigned char pt_smem[];
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(pt_smem);
     if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
     {
         const ll boff = (ll)blockIdx.y * P.bstride;
@@ -33,7 +34,7 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
         P.z += boff;
         P.xhat += boff;
     }
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x;
     const ll Nloc = P.Nloc;
     constexpr int E_max = (int)prox_tile_elems(N);
     T *sx = reinterpret_cast<T *>(pt_smem + 256);
@@ -41,39 +42,34 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
     T *sz = sx2 + E_max;
     const uint32_t base = (uint32_t)blockIdx.x << PT_M;
     int *roff = reinterpret_cast<int *>(pt_smem + 16);
-    if (tid == 0) {
-        mbar_init(mbar, 1);
-        fence_mbar_init();
+    __shared__ long long rg[32];     // global start of each alternative's run
+    __shared__ int hi_alt[32];       // the j-th present high run's alternative
+    if (tid < N) {
+        roff[tid] = pt_roff(base, tid);
+        rg[tid] = pt_rstart(base, tid, Nloc);
+        if (tid >= PT_M && ((base >> tid) & 1u)) hi_alt[__popc(base & ((1u << tid) - 1u) & ~((1u << PT_M) - 1u))] = tid;
     }
-    if (tid < N) roff[tid] = pt_roff(base, tid);
     __syncthreads();
-    if (tid < 32) {
-        // lane i issues alternative i's three copies; lane 0 first announces the byte count
-        if (lane == 0) {
-            unsigned elems = (unsigned)(PT_M * (1 << (PT_M - 1)) + __popc(base >> PT_M) * (1 << PT_M));
-            mbar_expect_tx(mbar, (unsigned)(3u * elems * sizeof(T)));
-        }
-        __syncwarp();
-        if (lane < N) {
-            int len = pt_rlen(base, lane);
-            if (len) {
-                int off = pt_roff(base, lane);
-                ll g = pt_rstart(base, lane, Nloc);
-                unsigned b = (unsigned)(len * sizeof(T));
-                tma_load_1d(sx + off, P.x + g, b, mbar);
-                tma_load_1d(sx2 + off, P.x2 + g, b, mbar);
-                tma_load_1d(sz + off, P.z + g, b, mbar);
-            }
-        }
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int Et = PT_M * (1 << (PT_M - 1)) + __popc(base >> PT_M) * (1 << PT_M);
+    // the run holding tile element e: the first PT_M runs are 2^(PT_M-1) long, the rest 2^PT_M
+    auto run_of = [&](int e) -> int {
+        return e < PT_M * (1 << (PT_M - 1)) ? (e >> (PT_M - 1)) : hi_alt[(e - PT_M * (1 << (PT_M - 1))) >> PT_M];
+    };
+    for (int c = tid; c < Et / VEC; c += PT_THREADS) {
+        const int e = c * VEC;
+        const int i = run_of(e);
+        const ll g = rg[i] + (e - roff[i]);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sx + e)), "l"(P.x + g) : "memory");
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sx2 + e)), "l"(P.x2 + g) : "memory");
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sz + e)), "l"(P.z + g) : "memory");
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
     const uint32_t low = (uint32_t)tid;
     const uint32_t S = base | low;
     const uint32_t wb = P.menu_obs[S];                 // observed members of S (one coalesced load)
-    if (!mbar_wait_bounded(mbar, 0)) {
-        if (tid == 0) atomicOr(P.err, 1u);
-        mbar_wait_bounded(mbar, 0);                    // a second bounded chance for in-flight copies
-        return;
-    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
     const int k = __popc(S);
     const T one = (T)1, two = (T)2;
     const bool mixed = wb != 0 && wb != S;
@@ -173,19 +169,13 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
         sx2[e] = u;
         sz[e] = sz[e] + P.b2 * u;
     }
-    fence_async_smem();
     __syncthreads();
-    if (tid < 32 && lane < N) {
-        int len = pt_rlen(base, lane);
-        if (len) {
-            int off = pt_roff(base, lane);
-            ll g = pt_rstart(base, lane, Nloc);
-            unsigned b = (unsigned)(len * sizeof(T));
-            tma_store_1d(P.x2 + g, sx2 + off, b);
-            tma_store_1d(P.z + g, sz + off, b);
-            tma_commit();
-            tma_wait_read();
-        }
+    for (int c = tid; c < Et / VEC; c += PT_THREADS) {
+        const int e = c * VEC;
+        const int i = run_of(e);
+        const ll g = rg[i] + (e - roff[i]);
+        *reinterpret_cast<uint4 *>(P.x2 + g) = *reinterpret_cast<const uint4 *>(sx2 + e);
+        *reinterpret_cast<uint4 *>(P.z + g) = *reinterpret_cast<const uint4 *>(sz + e);
     }
 }
 

@@ -4,9 +4,9 @@
 // slab entries of those menus form one contiguous, aligned run per alternative i:
 //   i <  m: the 2^(m-1) rests base/2 + compress(low, i) over the lows that contain i
 //   i >= m: the 2^m rests compress(base, i) + low, present only when base contains i
-// so the tile's x, x2 and z values arrive as a handful of 1-D TMA bulk copies
-// (cp.async.bulk, completion counted on one mbarrier) into shared memory, the projection runs
-// out of shared memory with a small register footprint, and x2 and z leave as bulk stores.
+// so the tile's x, x2 and z values are staged in shared memory as a few contiguous runs, the
+// projection runs out of shared memory with a small register footprint, and x2 and z go back the
+// same way (csrc/prox.cu).
 //
 // Per menu (the reference's fuse_xk, prox_all and fuse_z, solver/bm_admm/solver.py:37-46,66-139):
 //   xo = alpha x + (1 - alpha) x2,  v = xo - z / b2
@@ -15,8 +15,8 @@
 // The threshold comes from Michelot's active-set iteration (the active set only shrinks, at
 // most |S| rounds), which gives the reference's sort-based threshold without a sort.
 //
-// Bounded waits: the mbarrier wait gives up after ~2^32 cycles, records an error word and skips
-// the tile (the host turns the word into RUMB_E_TIMEOUT at the next check).
+// The mbarrier / bulk-copy helpers below serve the tensor-core GEMM (csrc/mlp.cu); their waits
+// are bounded (~2^32 cycles) and report failure instead of spinning on.
 #pragma once
 #include "common.cuh"
 

@@ -21,8 +21,9 @@ solver/inference/draws.py:161-290), with its formulas and decisions:
     learned   (learned=True, bm_admm) the first train_draws solved draws train a small BF16 network
               on the tensor cores (rumb_mlp_*) to map a draw's cells to its fitted cells; every
               later draw starts from the prediction: its bracket from the Frank-Wolfe lower bound
-              at the prediction (certified whatever the prediction) and its start state's fitted
-              cells moved there. A poor prediction costs iterations, never correctness
+              at the prediction (certified whatever the prediction); y0_state=True also moves the
+              start state's fitted cells there. A poor prediction costs iterations, never
+              correctness
     p-value   p = (#above + #undecided) / B
 
 Respondent weights: "multinomial" (R picks with replacement per draw) and "multinomial_reject"
@@ -173,7 +174,7 @@ class Bootstrap:
     def __init__(self, rum, n=None, panel=None, replies=None, B=None, weights=None, seed=None, r_n=None, eps_n=None,
                  method=None, method_args=None, abs_tol=None, rel_tol=None, max_time=None, draw_time=None,
                  batch_slots=0, verbose=False, learned=False, train_draws=512, mlp_hidden=(1024, 1024, 1024),
-                 mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=True, seed_net=0):
+                 mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=False, seed_net=0):
         d = defaults.BOOTSTRAP
         if panel is None or replies is not None:
             raise ValueError("this bootstrap takes a respondent panel (panel=)")
