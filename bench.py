@@ -53,8 +53,8 @@ CERT_ITERS_F64 = 43800
 # iterations run before the profiled ones: the roofline kernel is timed mid-solve
 PROFILE_WARMUP = 2000
 # DRAM bytes (read + write) per launch of the dominant kernel, from the ncu capture summarised in
-# profiles/iteration_kernels_n18_f64.md (same workload, float64 state)
-NCU_TRAFFIC = {"prox_tile<f64>": 60.5e6 + 0.516e6}
+# profiles/prox_tile_n18_f64.md (same workload, float64 state)
+NCU_TRAFFIC = {"prox_tile<f64>": 60.49e6 + 0.446e6}
 
 
 def _env_int(k, d):
