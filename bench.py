@@ -4,6 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--dtype float64|mixed] [--impl rumb|reference]
     python bench.py --profile-case ITERS [--dtype ...]   # one solve capped at ITERS iterations, for
                                                           # profilers; prints no bench line
+    python bench.py --workload bootstrap_n20             # batched bootstrap draws vs one at a time
 
 Workload "n18_d1pct_k50": every menu of 18 alternatives with >= 2 members kept with probability
 0.01 (2,627 menus, 23,650 observed cells), p_hat from a Dirichlet(1) mixture of 50 random linear
@@ -206,6 +207,49 @@ def pricing_sweeps(ctx, stream, sweeps=20):
     return out
 
 
+def run_bootstrap(args, rank, batch_draws=24, single_draws=4):
+    """Workload bootstrap_n20 (n = 20, 1 % menus, a 520-respondent panel of 30
+    menus each, K = 30): certify p_hat, then solve open draws to abs 5e-4 from p_hat's state,
+    batched (rumb_bm_solve_batch, all draws resident) against one at a time (Session.solve), both
+    float64. Wall time around each phase with the device synchronized on both sides; the one-at-a-
+    time draws are the batch's first draws, so the per-draw iterations compare directly."""
+    if rank != 0:
+        return
+    import torch
+    from rumb import RUM
+    from rumb import bootstrap as BS
+    from rumb.instances import config_instance
+    n, m, a, p, panel = config_instance("n20_d1pct_panel520")
+    rum = RUM(m, a, p, num_alternatives=n)
+    boot = rum.bootstrap(panel=panel, B=batch_draws, weights="multinomial", seed=0, method="bm_admm",
+                         method_args={"dtype": "float64"})
+    boot._certify()
+    idx = np.arange(batch_draws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    boot.solve_draws(idx, stops=False)
+    torch.cuda.synchronize()
+    tb = time.perf_counter() - t0
+    P = BS.perturb(boot.p_hat, boot.draws.rows(np.arange(single_draws)), boot.r_n, boot.eps_n)
+    its = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for j in range(single_draws):
+        r = boot.session.solve(P[j], abs_tol=boot.abs_tol, rel_tol=0.0, warm=True, max_time=600.0)
+        its.append(int(r.iterations))
+    torch.cuda.synchronize()
+    ts = time.perf_counter() - t0
+    line = {"metric": "n=20 bootstrap draws/s at abs gap 5e-4 (batched vs one at a time)",
+            "value": batch_draws / tb, "unit": "draws/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "n20_d1pct_panel520", "batch_draws": batch_draws, "abs_tol": boot.abs_tol,
+                       "slots": boot.last_batch["slots"], "iters_batched": boot.iters[idx].tolist()},
+            "one_at_a_time": {"value": single_draws / ts, "unit": "draws/s", "draws": single_draws,
+                              "iters": its},
+            "ratio_batched_over_one_at_a_time": (batch_draws / tb) / (single_draws / ts)}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -215,6 +259,8 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20"],
+                    help="bootstrap_n20: the batched-draw comparison (prints its own line)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
                     help="run one solve capped at ITERS iterations (for ncu) and print no bench line")
     args = ap.parse_args()
@@ -222,6 +268,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "bootstrap_n20":
+        run_bootstrap(args, rank)
         return
 
     import torch

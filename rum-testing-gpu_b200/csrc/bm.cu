@@ -636,6 +636,7 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
         Co<T> kQt{(T)C.Qt[0], (T)C.Qt[1], (T)C.Qt[2], (T)C.Qt[3]};
         Co<T> kQ{(T)C.Q[0], (T)C.Q[1], (T)C.Q[2], (T)C.Q[3]};
         Co<T> kAQ{(T)C.AQ[0], (T)C.AQ[1], (T)C.AQ[2], (T)C.AQ[3]};      // A Q, A = [[1,-1],[0,p]]
+        Co<T> kAr{(T)1, (T)-1, (T)0, p};                                   // A itself
         std::vector<XfShape> plan = xf_plan(n - 1, C.lo_bits);
         XfArgs<T, T> base{};
         base.Nloc = 1LL << (n - 1);
@@ -664,6 +665,7 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
                 xf_launch<T, T, K_PLAIN>(A, plan[i], n, st, K);
             }
             { XfArgs<T, T> A = at(plan[0]); A.in = t2; A.out = x; A.out2 = Ax; A.k1 = kQt; A.k2 = kQ; A.k3 = kAQ;
+              A.k4 = kAr;
               xf_launch<T, T, K_P3>(A, plan[0], n, st, K); }
             for (size_t i = 1; i < m; ++i) {
                 XfArgs<T, T> A = at(plan[i]); A.in = x; A.in2 = Ax; A.out = x; A.out2 = Ax; A.k1 = kQ; A.k3 = kAQ;

@@ -18,8 +18,8 @@
 // (solver/bm_admm/solver.py:240-254) into the transforms:
 //   K_P1   (low bits)  w = y - b1 s;  A' forward                              -> T1
 //   K_P2   (high bits) A' forward;  rhs = (z + b2 x2 - v) / b1;  Q^T backward -> T2
-//   K_P3   (low bits)  Q^T forward;  v *= 1/(gamma + lambda(rest));  fork:
-//                      Q backward -> T3,  (A Q) backward -> T4
+//   K_P3   (low bits)  Q^T forward;  v *= 1/(gamma + lambda(rest));  Q backward -> T3, and
+//                      A backward on a copy of T3 -> T4 (= (A Q) on the low window)
 //   K_P4   (high bits) Q forward on T3 -> x;  (A Q) forward on T4 -> A x, then the s/y update
 //                      a = -alpha Ax - (1-alpha) s; s' = max(y/b1 - a, 0); y -= b1 (a + s')
 //   K_FULL (all bits, n <= 13) P1..P4 in one pass
@@ -36,11 +36,19 @@ struct Co {
     T a, b, c, d;
 };
 
-// AP: the coefficients are A' = (1, 0, -1, p): lo' = lo, hi' = p hi - lo (one operation per pair)
-template <class T, bool AP>
+// Pair forms (MODE): 0 general (a, b, c, d); 1 A' = (1, 0, -1, p): lo' = lo, hi' = p hi - lo
+// (one operation per pair); 2 A = (1, -1, 0, p): lo' = lo - hi, hi' = p hi (two operations)
+constexpr int XF_GEN = 0, XF_APRIME = 1, XF_A = 2;
+
+template <class T, int MODE>
 __device__ __forceinline__ void xf_pair(T &X, T &Y, const Co<T> &k) {
-    if (AP) {
+    if (MODE == XF_APRIME) {
         Y = k.d * Y - X;
+        return;
+    }
+    if (MODE == XF_A) {
+        X = X - Y;
+        Y = k.d * Y;
         return;
     }
     T lo = k.a * X + k.b * Y;
@@ -50,7 +58,7 @@ __device__ __forceinline__ void xf_pair(T &X, T &Y, const Co<T> &k) {
 }
 
 // stages on register-index bits [B0, B0+NB), ascending
-template <class T, int R, int B0, int NB, bool AP>
+template <class T, int R, int B0, int NB, int AP>
 __device__ __forceinline__ void xf_regs(T (&v)[R], const Co<T> &k) {
 #pragma unroll
     for (int j = B0; j < B0 + NB; ++j) {
@@ -62,7 +70,7 @@ __device__ __forceinline__ void xf_regs(T (&v)[R], const Co<T> &k) {
 
 // the 5 lane-bit stages on every register value; the per-lane coefficients are picked once per
 // stage (lo lane: a, b; hi lane: d, c), so each value costs one multiply and one fma
-template <class T, int R, bool AP>
+template <class T, int R, int AP>
 __device__ __forceinline__ void xf_lanes(T (&v)[R], int lane, const Co<T> &k) {
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
@@ -71,8 +79,10 @@ __device__ __forceinline__ void xf_lanes(T (&v)[R], int lane, const Co<T> &k) {
 #pragma unroll
         for (int i = 0; i < R; ++i) {
             T o = __shfl_xor_sync(0xffffffffu, v[i], 1 << j);
-            if (AP) {
+            if (AP == XF_APRIME) {
                 if (hi) v[i] = k.d * v[i] - o;
+            } else if (AP == XF_A) {
+                v[i] = hi ? k.d * v[i] : v[i] - o;
             } else {
                 v[i] = c0 * v[i] + c1 * o;
             }
@@ -112,7 +122,7 @@ __device__ __forceinline__ void xf_B_to_A(T (&v)[1 << RB], T *sm, int w, int lan
 }
 
 // forward: (lanes) -> A regs -> transpose -> B regs;   starts in A, ends in B
-template <class T, int L, int RB, int WB, bool AP = false>
+template <class T, int L, int RB, int WB, int AP = XF_GEN>
 __device__ __forceinline__ void xf_forward(T (&v)[1 << RB], T *sm, int w, int lane, const Co<T> &k) {
     if (L) xf_lanes<T, 1 << RB, AP>(v, lane, k);
     xf_regs<T, 1 << RB, 0, RB, AP>(v, k);
@@ -123,14 +133,14 @@ __device__ __forceinline__ void xf_forward(T (&v)[1 << RB], T *sm, int w, int la
 }
 
 // backward: B regs -> transpose -> A regs -> (lanes);   starts in B, ends in A
-template <class T, int L, int RB, int WB>
+template <class T, int L, int RB, int WB, int AP = XF_GEN>
 __device__ __forceinline__ void xf_backward(T (&v)[1 << RB], T *sm, int w, int lane, const Co<T> &k) {
     if (WB) {
-        xf_regs<T, 1 << RB, RB - WB, WB, false>(v, k);
+        xf_regs<T, 1 << RB, RB - WB, WB, AP>(v, k);
         xf_B_to_A<T, RB, WB>(v, sm, w, lane);
     }
-    xf_regs<T, 1 << RB, 0, RB, false>(v, k);
-    if (L) xf_lanes<T, 1 << RB, false>(v, lane, k);
+    xf_regs<T, 1 << RB, 0, RB, AP>(v, k);
+    if (L) xf_lanes<T, 1 << RB, AP>(v, lane, k);
 }
 
 enum XfKind { K_PLAIN = 0, K_P1 = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_FULL = 5, K_DUAL = 6 };
@@ -234,8 +244,8 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
             xx[j] = A.x2[g];
         }
     }
-    if (KIND == K_P1 || KIND == K_P2 || KIND == K_FULL) xf_forward<T, L, RB, WB, true>(v, sm, w, lane, A.k1);
-    else xf_forward<T, L, RB, WB, false>(v, sm, w, lane, A.k1);
+    if (KIND == K_P1 || KIND == K_P2 || KIND == K_FULL) xf_forward<T, L, RB, WB, XF_APRIME>(v, sm, w, lane, A.k1);
+    else xf_forward<T, L, RB, WB, XF_GEN>(v, sm, w, lane, A.k1);
     // now in layout B (layout A when WB == 0)
     if (KIND == K_PLAIN || KIND == K_P1) {
 #pragma unroll
@@ -281,21 +291,28 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
         return;
     }
     if (KIND == K_P3) {
+        // (A Q) on the low window is A applied after Q: the fork copies Q's result (layout A) and
+        // runs the two-operation A form (k4 = (1, -1, 0, p)) forward from layout A to layout B
+        // instead of a second general transform; the factors of A commute, so the stage order
+        // does not matter
         T u[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
             ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
             v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
-            u[j] = v[j];
         }
         xf_backward<T, L, RB, WB>(v, sm, w, lane, A.k2);
-        xf_backward<T, L, RB, WB>(u, sm, w, lane, A.k3);
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
-            A.out[g] = v[j];
-            A.out2[g] = u[j];
+            u[j] = v[j];
+            A.out[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane)] = v[j];
+        }
+        xf_forward<T, L, RB, WB, XF_A>(u, sm, w, lane, A.k4);
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+            A.out2[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane)] = u[j];
         }
     }
 }

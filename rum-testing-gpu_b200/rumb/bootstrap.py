@@ -15,9 +15,9 @@ solver/inference/draws.py:161-290), with its formulas and decisions:
     solve     the draws still open, warm from p_hat's state, each stopping once it clears the band
               (ub < tau_lo: below; lb >= tau_hi: above). bm_admm solves them together with
               rumb_bm_solve_batch (slots admitted by device memory, retired as they finish);
-              flow_cg one at a time through the Session, as the reference does. A float32 or mixed
-              session solves the batch in float32; draws whose bracket stalls undecided are solved
-              again in float64
+              flow_cg one at a time through the Session, as the reference does. A float32 session
+              solves the batch in float32; draws whose bracket stalls undecided are solved again in
+              float64 (a mixed session batches in float64)
     learned   (learned=True, bm_admm) the first train_draws solved draws train a small BF16 network
               on the tensor cores (rumb_mlp_*) to map a draw's cells to its fitted cells; every
               later draw starts from the prediction: its bracket from the Frank-Wolfe lower bound
@@ -30,7 +30,10 @@ Respondent weights: "multinomial" (R picks with replacement per draw) and "multi
 (redraw a weight row that leaves a menu unseen), drawn from numpy.random.default_rng(seed) in the
 reference's order.
 """
+import hashlib
+import json
 import math
+import os
 import time
 from dataclasses import dataclass
 
@@ -42,6 +45,24 @@ from . import defaults
 BELOW, ABOVE, UNDECIDED = 0, 1, 2
 ZERO = 1e-9
 REDRAW_ROUNDS = 10000
+VERSION = 1                      # the record format's version (solver/inference/bootstrap.py:48)
+NEVER = 127                      # exit_flag of a draw that was never solved
+# a batched draw's stop reason as the Session's exit flag (1 tol, 5 threshold, 0 time, -1 iters,
+# -2 stalled)
+_STOP_FLAG = {"gap_abs": 1, "gap_rel": 2, "ub_target": 5, "lb_target": 5, "time_limit": 0, "max_iter": -1,
+              "stall": -2, "cancel": -4}
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def _plain(x):
+    if isinstance(x, np.generic):
+        return x.item()
+    if isinstance(x, np.ndarray):
+        return x.tolist()
+    raise TypeError("not JSON serializable: %r" % type(x))
 
 
 def scaling(n, r_n=None, eps_n=None):
@@ -74,6 +95,8 @@ class Draws:
         pm = np.asarray(panel["menu"], dtype=np.int64)
         pc = np.asarray(panel["chosen"], dtype=np.int64)
         _, codes = np.unique(resp, return_inverse=True)
+        codes = codes.astype(np.int64)
+        self.input_fingerprint = hashlib.sha256(codes.tobytes() + pm.tobytes() + pc.tobytes()).hexdigest()[:16]
         R = int(codes.max()) + 1
         menu, alternative = np.asarray(menu, dtype=np.int64), np.asarray(alternative, dtype=np.int64)
         M = menu.size
@@ -85,6 +108,7 @@ class Draws:
         key = m * 64 + pc
         pos = np.minimum(np.searchsorted(row_key[order], key), M - 1)
         hit = used & (row_key[order][pos] == key)
+        self.rows_unused = int((~used).sum())       # panel rows on menus that have no rum row
         self.offered = sp.csr_array((np.ones(int(used.sum())), (codes[used], m[used])), shape=(R, rum_menus.size))
         self.chose = sp.csr_array((np.ones(int(hit.sum())), (codes[hit], order[pos[hit]])), shape=(R, M))
         self.row_menu = row_menu
@@ -101,6 +125,11 @@ class Draws:
                 self.n_redraws += int(bad.sum())
                 W[bad] = rng.multinomial(R, np.ones(R) / R, size=int(bad.sum())).astype(np.float64)
         self.W = W
+
+    def summary(self):
+        """The record's account of the panel and its draws."""
+        return dict(respondents=self.R, rows_unused=self.rows_unused, redraws=self.n_redraws,
+                    emptied_menu_draws=None)
 
     def rows(self, idx):
         """The draws idx as a (len(idx), M) array: weighted shares, p_hat where a menu went unseen."""
@@ -174,7 +203,7 @@ class Bootstrap:
     def __init__(self, rum, n=None, panel=None, replies=None, B=None, weights=None, seed=None, r_n=None, eps_n=None,
                  method=None, method_args=None, abs_tol=None, rel_tol=None, max_time=None, draw_time=None,
                  batch_slots=0, verbose=False, learned=False, train_draws=512, mlp_hidden=(1024, 1024, 1024),
-                 mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=False, seed_net=0):
+                 mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=False, seed_net=0, checkpoint=None):
         d = defaults.BOOTSTRAP
         if panel is None or replies is not None:
             raise ValueError("this bootstrap takes a respondent panel (panel=)")
@@ -200,9 +229,29 @@ class Bootstrap:
         self.mlp_hidden, self.mlp_epochs, self.mlp_batch = tuple(mlp_hidden), int(mlp_epochs), int(mlp_batch)
         self.mlp_lr, self.y0_state, self.seed_net = float(mlp_lr), bool(y0_state), int(seed_net)
         self.net, self.learned_info = None, None
+        # the record (solver/inference/bootstrap.py:159-180,356-400): settings, fingerprints and
+        # per draw the bracket, the tightest tolerances asked and the last exit flag
+        self.method, self.method_args = method, method_args
+        self.settings = dict(n=self.n, input="panel", B=self.B, weights=self.draws.weights, seed=self.draws.seed,
+                             r_n=self.r_n, eps_n=self.eps_n, method=method, method_args=method_args,
+                             abs_tol=self.abs_tol, rel_tol=self.rel_tol, refine=d["refine"], max_time=self.max_time,
+                             draw_time=self.draw_time, weighted=False)
+        self.fingerprints = {"data": _sha(np.column_stack([np.asarray(rum.menu, dtype=np.float64),
+                                                           np.asarray(rum.alternative, dtype=np.float64),
+                                                           self.p_hat])),
+                             "panel": self.draws.input_fingerprint, "draws": None}
+        self.tol_stop = np.full(self.B, np.inf)
+        self.tol_full = np.full(self.B, np.inf)
+        self.flag = np.full(self.B, NEVER, dtype=np.int8)
+        self.results = {"p_value": {}, "confidence_interval": {}, "distance_interval": {}}
+        self.screened = False
+        self.n_screened = 0
+        self.checkpoint = checkpoint
         self.L0 = self.U0 = None
         self.verbose = verbose
         self.time = dict(certificate=0.0, screen=0.0, solve=0.0)
+        if checkpoint and os.path.exists(checkpoint):
+            self._resume(checkpoint)
 
     @property
     def tau(self):
@@ -224,6 +273,7 @@ class Bootstrap:
             P = perturb(self.p_hat, self.draws.rows(idx), self.r_n, self.eps_n)
             self.U[idx] = np.minimum(self.U[idx], np.sqrt(np.einsum("ij,ij->i", P - fit, P - fit)))
         self.n_screened = int((self.U < self.tau[0]).sum())
+        self.screened = True
         self.time["screen"] += time.perf_counter() - t0
 
     def _batch(self, ctx, prob, par, P, below, above, y0=None, want_fit=False):
@@ -291,11 +341,16 @@ class Bootstrap:
         rum, s = self.rum, self.session
         if s.method == "bm_admm" and rum.n >= 8 and rum._single.size == 0:
             from .rum_solver import context
+            if s._kept is None:                    # a resumed run: p_hat's state again, for the warm starts
+                s.solve(self.p_hat, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_time=self.max_time, keep=True)
             ctx = context()
             a = s._args
             g = rum._geom
             prob = ctx.bm_problem(rum.n, g.menu.astype(np.uint32), g.alternative.astype(np.int32), self.p_hat)
-            dt = "float32" if a["dtype"] in ("float32", "mixed") else "float64"
+            # a float32 batch only for a float32 session: a mixed session's draws would mostly stall
+            # above the tolerance in float32 (the bootstrap's abs 5e-4 is far below the float32
+            # floor at the distances of its panels) and be solved again from the start
+            dt = "float32" if a["dtype"] == "float32" else "float64"
             par = ctx.bm_params(a["beta"], alpha=a["alpha"], precond_p=a["precond_p"], check=a["check"],
                                 lb_every=a["lb_every"], max_iter=a["max_iter"], abs_tol=self.abs_tol,
                                 rel_tol=self.rel_tol if self.rel_tol > 0 else None, dtype=dt)
@@ -317,14 +372,66 @@ class Bootstrap:
                 self.L[b] = max(self.L[b], res[j]["lb"])
                 self.U[b] = min(self.U[b], res[j]["ub"])
                 self.iters[b] = res[j]["iters"]
+                self.flag[b] = _STOP_FLAG.get(res[j]["stop_reason"], -5)
         else:
             for j, b in enumerate(idx):
                 r = s.solve(P[j], abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_time=self.draw_time, warm=True,
                             below=tau_lo if stops else None, above=tau_hi if stops else None)
                 self.L[b], self.U[b] = max(self.L[b], r.lb), min(self.U[b], r.ub)
                 self.iters[b] = r.iterations
+                self.flag[b] = r.exit_flag
+        self.tol_stop[idx] = np.minimum(self.tol_stop[idx], self.abs_tol)
+        if not stops:
+            self.tol_full[idx] = np.minimum(self.tol_full[idx], self.abs_tol)
         self.solved[idx] = True
+        self._save_checkpoint()
         self.time["solve"] += time.perf_counter() - t0
+
+    # ------------------------------------------------------------------ record, checkpoint
+    def record(self):
+        """Everything needed to report or resume the run, as plain Python values, in the reference's
+        record layout (solver/inference/bootstrap.py:356-370)."""
+        s = self.session
+        return dict(version=VERSION, settings=self.settings, fingerprints=self.fingerprints,
+                    plan=dict(method=s.method, method_args=s.method_args, auto_reason=s.auto_reason),
+                    p_hat=dict(lb=self.L0, ub=self.U0, certificates=[]),
+                    tau=None if self.L0 is None else list(self.tau),
+                    scaling=dict(r_n=self.r_n, eps_n=self.eps_n, s=self.s),
+                    screen=dict(done=self.screened, n_below=self.n_screened),
+                    panel=self.draws.summary(),
+                    draws=dict(lb=self.L.tolist(), ub=self.U.tolist(), tol_stop=self.tol_stop.tolist(),
+                               tol_full=self.tol_full.tolist(), exit_flag=self.flag.tolist()),
+                    results=self.results, time=self.time, when=time.strftime("%Y-%m-%d %H:%M:%S"))
+
+    def save(self, path):
+        """record() as JSON (infinite bounds as Infinity), written atomically."""
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(self.record(), f, indent=1, default=_plain)
+        os.replace(tmp, path)
+
+    def _save_checkpoint(self):
+        if self.checkpoint:
+            self.save(self.checkpoint)
+
+    def _resume(self, path):
+        rec = json.load(open(path))
+        same = dict(version=rec.get("version") == VERSION,
+                    settings=json.loads(json.dumps(self.settings, default=_plain)) == rec.get("settings"),
+                    data=rec.get("fingerprints", {}).get("data") == self.fingerprints["data"],
+                    panel=rec.get("fingerprints", {}).get("panel") == self.fingerprints["panel"])
+        if not all(same.values()):
+            raise ValueError("checkpoint %s belongs to another run (differs in: %s); delete it or pass another path"
+                             % (path, ", ".join(k for k, v in same.items() if not v)))
+        dr = rec["draws"]
+        self.L, self.U = np.array(dr["lb"], dtype=np.float64), np.array(dr["ub"], dtype=np.float64)
+        self.tol_stop = np.array(dr["tol_stop"], dtype=np.float64)
+        self.tol_full = np.array(dr["tol_full"], dtype=np.float64)
+        self.flag = np.array(dr["exit_flag"], dtype=np.int8)
+        self.solved = self.flag != NEVER
+        self.L0, self.U0 = rec["p_hat"]["lb"], rec["p_hat"]["ub"]
+        self.screened, self.n_screened = rec["screen"]["done"], rec["screen"]["n_below"]
+        self.results, self.time = rec["results"], rec["time"]
 
     def p_value(self, alpha=0.05, max_draws=None, group=None):
         """The test's p-value. Under torch.distributed (group: a process group, or the default one
@@ -337,6 +444,9 @@ class Bootstrap:
             self._certify()
             if world > 1:
                 self.L0, self.U0 = _broadcast_band(self.L0, self.U0, group)
+        if not self.screened:
+            if self.session.fit is None:          # resumed before the screen: certify again
+                self._certify()
             self._screen()
         if self.U0 > ZERO:
             dec = decide(self.L, self.U, *self.tau)

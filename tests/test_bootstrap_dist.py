@@ -3,6 +3,7 @@ rank solves its share of the open draws, and the gathered record and p-value equ
 process's. The solver is a stand-in (no GPU); what is tested is the host-side sharding."""
 import os
 import socket
+import types
 
 import numpy as np
 import pytest
@@ -19,6 +20,8 @@ def _fake(rank_u0=None):
     b.L, b.U = np.zeros(B), np.full(B, np.inf)
     b.solved = np.zeros(B, dtype=bool)
     b.L0 = b.U0 = None
+    b.screened = False
+    b.session = types.SimpleNamespace(fit=np.zeros(1))
     b.time = dict(certificate=0.0, screen=0.0, solve=0.0)
     b.seen = []
 
@@ -29,6 +32,7 @@ def _fake(rank_u0=None):
         k = np.arange(B)
         b.U = np.minimum(b.U, np.where(k % 3 == 0, 0.5, 10.0))       # every third draw screened below
         b.n_screened = int((b.U < b.tau[0]).sum())
+        b.screened = True
 
     def solve(idx, stops=True):
         idx = np.asarray(idx)

@@ -95,9 +95,19 @@ def test_push_and_lower_bound_match_oracle(ctx, n):
     assert abs(ub32 - ub32_ref) <= 1e-11 * max(1.0, ub32_ref)
 
 
+def _instance(case):
+    if case == "n10_all_k20":
+        return config_instance(case)
+    n = int(case[1:3])                        # "n14_mix", "n16_mix": split passes P1..P4 (n >= 14)
+    from rumb.instances import mixture_instance
+    m, a, p = mixture_instance(n, 0.05 if n <= 14 else 0.02, K=20, N=300, seed=n)
+    return n, m, a, p
+
+
+@pytest.mark.parametrize("case", ["n10_all_k20", "n14_mix", "n16_mix"])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
-def test_iterates_track_oracle(ctx, dtype):
-    n, menu, alt, p = config_instance("n10_all_k20")
+def test_iterates_track_oracle(ctx, case, dtype):
+    n, menu, alt, p = _instance(case)
     beta = O.beta_default(p.size)
     dt = np.float64 if dtype == "float64" else np.float32
     bm = O.BMOracle(n, menu, alt, p, dtype=dt)
@@ -106,7 +116,15 @@ def test_iterates_track_oracle(ctx, dtype):
     st = ctx.bm_iterate(prob, par, None, 0, cold_start=True)
     np.testing.assert_allclose(st["x2"], bm.x2, atol=1e-12 if dt == np.float64 else 1e-6)
     total = 0
-    tol = {1: 1e-11, 10: 1e-10, 100: 1e-9} if dt == np.float64 else {1: 1e-5, 10: 1e-4, 100: 5e-4}
+    # float32: the GPU contracts and orders the 4 (n - 1) butterfly stages of an iteration
+    # differently from the oracle; at n >= 14 (the split passes) their rounding reaches ~5e-5 of the
+    # largest value after one iteration. float64 pins the arithmetic itself (1e-11 .. 1e-9).
+    if dt == np.float64:
+        tol = {1: 1e-11, 10: 1e-10, 100: 1e-9}
+    elif n < 14:
+        tol = {1: 1e-5, 10: 1e-4, 100: 5e-4}
+    else:
+        tol = {1: 2e-4, 10: 1e-3, 100: 4e-3}
     for k in (1, 9, 90):
         st = ctx.bm_iterate(prob, par, st, k)
         bm.iterate(k)

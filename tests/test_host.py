@@ -159,3 +159,31 @@ def test_bootstrap_draws_and_formulas():
     assert r_n == pytest.approx(math.sqrt(520)) and eps_n == pytest.approx(520 ** (-1 / 3))
     dec = BS.decide([0.0, 3.0, 1.0], [0.5, 4.0, 2.5], 1.0, 2.0)
     assert list(dec) == [BS.BELOW, BS.ABOVE, BS.UNDECIDED]
+
+
+def test_bootstrap_record_checkpoint_and_resume(fake_gpu, tmp_path):
+    """The record's layout (the reference's, solver/inference/bootstrap.py:356-400), an atomic
+    checkpoint, a resume that restores every draw, and a refusal to resume another run's file."""
+    from rumb import bootstrap as BS
+    from rumb.rum_solver import RUM
+    panel, (m, a, p) = panel_instance(10, 0.2, 60, 6, 4, seed=3)
+    rum = RUM(m, a, p, num_alternatives=10)
+    path = str(tmp_path / "boot.json")
+    b = rum.bootstrap(panel=panel, B=12, weights="multinomial", seed=0, method="bm_admm", checkpoint=path)
+    b.L0, b.U0 = 0.5, 0.6
+    b.L[:4], b.U[:4] = [0.1, 0.2, 0.3, 0.4], [0.15, 0.25, 0.35, 0.45]
+    b.flag[:4] = [1, 1, 5, -2]
+    b.tol_stop[:4] = 5e-4
+    b.screened, b.n_screened = True, 3
+    b.save(path)
+    rec = json.load(open(path))
+    assert set(rec) >= {"version", "settings", "fingerprints", "plan", "p_hat", "tau", "scaling", "screen", "panel",
+                        "draws", "results", "time", "when"}
+    assert rec["draws"]["exit_flag"][:5] == [1, 1, 5, -2, BS.NEVER] and rec["draws"]["ub"][5] == float("inf")
+    r = rum.bootstrap(panel=panel, B=12, weights="multinomial", seed=0, method="bm_admm", checkpoint=path)
+    np.testing.assert_array_equal(r.L, b.L)
+    np.testing.assert_array_equal(r.U, b.U)
+    np.testing.assert_array_equal(r.flag, b.flag)
+    assert (r.L0, r.U0) == (0.5, 0.6) and r.screened and r.solved.sum() == 4
+    with pytest.raises(ValueError, match="belongs to another run"):
+        rum.bootstrap(panel=panel, B=12, weights="multinomial", seed=1, method="bm_admm", checkpoint=path)
