@@ -207,7 +207,7 @@ def pricing_sweeps(ctx, stream, sweeps=20):
     return out
 
 
-def run_bootstrap(args, rank, batch_draws=24, single_draws=4):
+def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
     """Workload bootstrap_n20 (n = 20, 1 % menus, a 520-respondent panel of 30
     menus each, K = 30): certify p_hat, then solve open draws to abs 5e-4 from p_hat's state,
     batched (rumb_bm_solve_batch, all draws resident) against one at a time (Session.solve), both

@@ -143,6 +143,10 @@ typedef struct {
     double stall_rtol;   /* float32 state: once the gap shrank by less than this fraction over the
                             last stall_checks checks, RUMB_MIXED hands over to float64 and
                             RUMB_F32 stops with RUMB_STOP_STALL */
+    int overlap_check;   /* 1 (with use_graph): each check runs on a second stream on a snapshot
+                            of the state while the next interval's iterations run; a stop takes
+                            effect one interval later (iters counts the work done), the bracket is
+                            the check's. 0: checks in line (the reference's sequence) */
 } rumb_bm_params;
 
 typedef struct {
@@ -177,7 +181,8 @@ RUMB_API int rumb_bm_iterate(rumb_ctx *ctx, const rumb_bm_problem *prob, const r
 typedef struct {
     int slots;            /* draws resident at once; 0 = as many as fit mem_fraction of free memory */
     double mem_fraction;  /* share of free device memory the slots may take (0 = 0.8) */
-    double draw_time;     /* seconds per draw (<= 0: none) */
+    double draw_time;     /* seconds per draw (<= 0: none), of the GPU's time: the K resident draws
+                             share it, so a draw stops after draw_time x K seconds of wall time */
     const double *y0;     /* NULL, or B x mp predicted fits: each draw's bracket starts from the
                              Frank-Wolfe lower bound at its y0 (certified for any y0) */
     int y0_state;         /* with y0: also write y0 into the start state's observed entries */

@@ -91,6 +91,13 @@ int rumb_ctx_destroy(rumb_ctx *ctx) {
         ctx->c.cert.reset();
         ctx->c.scratch.reset();
         ctx->c.layers.clear();
+        if (ctx->c.aux) {
+            cudaStreamSynchronize(ctx->c.aux);
+            cudaStreamDestroy(ctx->c.aux);
+        }
+        if (ctx->c.ev_snap) cudaEventDestroy(ctx->c.ev_snap);
+        if (ctx->c.ev_done) cudaEventDestroy(ctx->c.ev_done);
+        if (ctx->c.res_host) cudaFreeHost(ctx->c.res_host);
         if (ctx->c.ev_a) cudaEventDestroy(ctx->c.ev_a);
         if (ctx->c.ev_b) cudaEventDestroy(ctx->c.ev_b);
         if (ctx->c.own) cudaStreamDestroy(ctx->c.own);

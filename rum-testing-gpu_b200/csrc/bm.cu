@@ -512,6 +512,7 @@ static void enqueue_stats_lb(Ctx &c, CertWork &W, int n, const T *x2, bool with_
 template <class T>
 struct BmWork : public BmWorkBase {
     DevBuf x2, s, y, z, x, Ax, t1, t2, xhat, obsbits, diag, err, menu_obs;
+    DevBuf snap;                 // overlapped checks: the snapshot of x2 a check reads
     int n = 0;
     void ensure(int n_) {
         n = n_;
@@ -948,6 +949,104 @@ struct LoopState {
     std::vector<double> gaps;   // mixed mode: the bracket's gap at every check
 };
 
+// The check loop with every check overlapped with the next interval's iterations: the iterations
+// run on the context's stream, a snapshot of x2 is copied there, and the check (phi, push, lower
+// bound) runs on the second stream on the snapshot while the following interval iterates. The host
+// reads check k after enqueueing interval k + 1, so a stop lands one interval after its check.
+template <class T>
+static bool run_leg_overlap(Ctx &c, CertWork &CW, BmWork<T> &W, const rumb_bm_problem &pr,
+                            const rumb_bm_params &par, LoopState &L, Clock::time_point t0, bool stall_exit,
+                            Graph &g_iter, int chunk, rumb_trace_fn trace, void *user) {
+    const int n = pr.n;
+    const ll m2 = (ll)n << (n - 1);
+    cudaStream_t st = c.own;
+    c.ensure_aux();
+    cudaStream_t cs = c.aux;
+    W.snap.ensure((size_t)m2 * sizeof(T));
+    T *x2s = W.snap.template as<T>();
+    Graph h_ub, h_ublb;
+    h_ub.capture(cs, [&] {
+        enqueue_stats_lb<T>(c, CW, n, x2s, false, cs);
+        enqueue_push<T>(c, CW, n, x2s, cs);
+    });
+    h_ublb.capture(cs, [&] {
+        enqueue_stats_lb<T>(c, CW, n, x2s, true, cs);
+        enqueue_push<T>(c, CW, n, x2s, cs);
+    });
+    struct AuxSync {   // no check may outlive the loop (its graphs and the snapshot)
+        cudaStream_t s;
+        ~AuxSync() { cudaStreamSynchronize(s); }
+    } aux_sync{cs};
+    RUMB_CUDA(cudaEventRecord(c.ev_snap, st));        // the set-up on st comes before any check
+    RUMB_CUDA(cudaStreamWaitEvent(cs, c.ev_snap, 0));
+    RUMB_CUDA(cudaEventRecord(c.ev_done, cs));
+    double *res = c.res_host;
+    bool pending = false, pend_lb = false;
+    ll pend_it = 0;
+    // 0 go on, 1 stop, 2 float32 stall (hand over)
+    auto process = [&]() -> int {
+        RUMB_CUDA(cudaEventSynchronize(c.ev_done));
+        pending = false;
+        L.checks++;
+        L.phi = std::sqrt(res[R_PHI2]);
+        L.ub = res[R_UB_BEST];
+        if (pend_lb) {
+            L.n_lb++;
+            if (res[R_LB_NOW] > L.lb) L.lb = res[R_LB_NOW];
+        }
+        if (trace) trace(user, pend_it, secs(t0, Clock::now()), L.phi, L.ub, L.lb);
+        if (std::isfinite(par.ub_target) && L.ub <= par.ub_target) { L.stop = RUMB_STOP_UB_TARGET; return 1; }
+        if (std::isfinite(par.lb_target) && L.lb >= par.lb_target) { L.stop = RUMB_STOP_LB_TARGET; return 1; }
+        double gap = L.ub - L.lb;
+        if (par.abs_tol >= 0 && gap <= par.abs_tol) { L.stop = RUMB_STOP_GAP_ABS; return 1; }
+        if (par.rel_tol >= 0 && L.lb > 0 && gap / L.lb <= par.rel_tol) { L.stop = RUMB_STOP_GAP_REL; return 1; }
+        if (stall_exit) {
+            L.gaps.push_back(gap);
+            size_t Wn = (size_t)(par.stall_checks > 0 ? par.stall_checks : 1);
+            if (L.gaps.size() > Wn && gap > (1.0 - par.stall_rtol) * L.gaps[L.gaps.size() - 1 - Wn]) return 2;
+        }
+        return 0;
+    };
+    auto finish = [&](int r) -> bool {
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        RUMB_CUDA(cudaStreamSynchronize(cs));
+        return r != 2;
+    };
+    while (L.it < par.max_iter) {
+        for (int i = 0; i < par.check / chunk; ++i) g_iter.launch(st);
+        L.it += par.check;
+        if (sizeof(T) == 4) L.it32 += par.check;
+        RUMB_CUDA(cudaStreamWaitEvent(st, c.ev_done, 0));   // the last check no longer reads the snapshot
+        RUMB_CUDA(cudaMemcpyAsync(x2s, W.x2.ptr, (size_t)m2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        RUMB_CUDA(cudaEventRecord(c.ev_snap, st));
+        if (pending) {
+            auto tp = Clock::now();
+            int r = process();
+            L.push_s += secs(tp, Clock::now());
+            if (r) return finish(r);
+        }
+        double el = secs(t0, Clock::now());
+        if ((par.time_limit > 0 && el > par.time_limit) || c.cancel.load()) {
+            L.stop = c.cancel.load() ? RUMB_STOP_CANCEL : RUMB_STOP_TIME;
+            return finish(1);
+        }
+        const bool want_lb = (L.checks % par.lb_every) == 0;
+        RUMB_CUDA(cudaStreamWaitEvent(cs, c.ev_snap, 0));
+        (want_lb ? h_ublb : h_ub).launch(cs);
+        RUMB_CUDA(cudaMemcpyAsync(res, CW.res.ptr, R_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, cs));
+        RUMB_CUDA(cudaEventRecord(c.ev_done, cs));
+        pending = true;
+        pend_lb = want_lb;
+        pend_it = L.it;
+    }
+    if (pending) {
+        int r = process();
+        if (r) return finish(r);
+    }
+    L.stop = RUMB_STOP_MAX_ITER;
+    return finish(1);
+}
+
 template <class T>
 static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const rumb_bm_problem &pr,
                     const rumb_bm_params &par, LoopState &L, Clock::time_point t0, bool stall_exit,
@@ -968,6 +1067,8 @@ static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const r
             enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
         });
     }
+    if (graphs && par.overlap_check) return run_leg_overlap<T>(c, CW, W, pr, par, L, t0, stall_exit, g_iter, chunk,
+                                                              trace, user);
     double res[R_SLOTS];
     while (L.it < par.max_iter) {
         if (graphs) {
@@ -1499,7 +1600,8 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
             else if (par->abs_tol >= 0 && gap <= par->abs_tol) stop = RUMB_STOP_GAP_ABS;
             else if (par->rel_tol >= 0 && lb_of[k] > 0 && gap / lb_of[k] <= par->rel_tol) stop = RUMB_STOP_GAP_REL;
             else if (it_of[k] >= par->max_iter) stop = RUMB_STOP_MAX_ITER;
-            else if (bp && bp->draw_time > 0 && secs(t_of[k], Clock::now()) > bp->draw_time) stop = RUMB_STOP_TIME;
+            // the K resident draws share the GPU: a draw's budget is draw_time of its share
+            else if (bp && bp->draw_time > 0 && secs(t_of[k], Clock::now()) > bp->draw_time * K) stop = RUMB_STOP_TIME;
             else if (par->stall_checks > 0) {
                 // a float32 state's bracket stops closing at its rounding floor
                 gaps_of[k].push_back(gap);

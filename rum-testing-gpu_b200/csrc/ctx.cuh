@@ -29,6 +29,17 @@ struct Ctx {
     std::unique_ptr<BmWorkBase> cert;           // float64 certificate workspace
     std::unique_ptr<BmWorkBase> scratch;        // primitive calls' scratch
     std::map<std::pair<int, int>, int> lo_bits; // tuned low-window size per (n, state bytes)
+    // overlapped checks: a second stream, its two events and pinned result words (made on first use)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_done = nullptr;
+    double *res_host = nullptr;
+    void ensure_aux() {
+        if (aux) return;
+        RUMB_CUDA(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+        RUMB_CUDA(cudaEventCreateWithFlags(&ev_snap, cudaEventDisableTiming));
+        RUMB_CUDA(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+        RUMB_CUDA(cudaMallocHost(&res_host, 64 * sizeof(double)));
+    }
 
     // Make the context's stream wait for the caller's stream (call start) ...
     void join_in() {

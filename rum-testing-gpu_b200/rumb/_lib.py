@@ -42,7 +42,8 @@ class BMParams(ctypes.Structure):
                 ("check", ctypes.c_int), ("lb_every", ctypes.c_int), ("max_iter", ctypes.c_longlong),
                 ("abs_tol", ctypes.c_double), ("rel_tol", ctypes.c_double), ("time_limit", ctypes.c_double),
                 ("ub_target", ctypes.c_double), ("lb_target", ctypes.c_double), ("dtype", ctypes.c_int),
-                ("use_graph", ctypes.c_int), ("stall_checks", ctypes.c_int), ("stall_rtol", ctypes.c_double)]
+                ("use_graph", ctypes.c_int), ("stall_checks", ctypes.c_int), ("stall_rtol", ctypes.c_double),
+                ("overlap_check", ctypes.c_int)]
 
 
 class BMResult(ctypes.Structure):
@@ -246,7 +247,7 @@ class Context:
     @staticmethod
     def bm_params(beta, alpha=1.95, precond_p=math.sqrt(2.0), check=50, lb_every=1, max_iter=10 ** 7,
                   abs_tol=1e-5, rel_tol=1e-4, time_limit=0.0, ub_target=None, lb_target=None, dtype="float64",
-                  use_graph=True, stall_checks=20, stall_rtol=0.05):
+                  use_graph=True, stall_checks=20, stall_rtol=0.05, overlap_check=False):
         P = BMParams()
         P.beta, P.alpha, P.precond_p = float(beta), float(alpha), float(precond_p)
         P.check, P.lb_every, P.max_iter = int(check), int(lb_every), int(max_iter)
@@ -258,6 +259,7 @@ class Context:
         P.dtype = DTYPES[dtype] if isinstance(dtype, str) else int(dtype)
         P.use_graph = int(bool(use_graph))
         P.stall_checks, P.stall_rtol = int(stall_checks), float(stall_rtol)
+        P.overlap_check = int(bool(overlap_check))
         return P
 
     @staticmethod

@@ -205,3 +205,24 @@ def test_invalid_input_is_an_error_not_a_fault(ctx):
     n, menu, alt, p = config_instance("n10_all_k20")
     r, _, _ = ctx.bm_solve(ctx.bm_problem(n, menu, alt, p), ctx.bm_params(2.5, max_iter=50))
     assert r["iters"] == 50
+
+
+@pytest.mark.parametrize("dtype", ["float64", "mixed"])
+def test_overlapped_checks_certify_the_same_bracket(ctx, dtype):
+    """Checks on a second stream beside the next interval: the same checks of the same states, so
+    the same bracket, found one interval later (the stop takes effect after the running interval)."""
+    n, menu, alt, p = _instance("n14_mix")
+    beta = O.beta_default(p.size)
+    prob = ctx.bm_problem(n, menu, alt, p)
+    base, fit0, _ = ctx.bm_solve(prob, ctx.bm_params(beta, abs_tol=1e-6, rel_tol=None, dtype=dtype))
+    ov, fit1, _ = ctx.bm_solve(prob, ctx.bm_params(beta, abs_tol=1e-6, rel_tol=None, dtype=dtype,
+                                                   overlap_check=True))
+    assert ov["stop_reason"] == base["stop_reason"] == "gap_abs"
+    assert ov["ub"] - ov["lb"] <= 1e-6
+    assert ov["lb"] <= base["ub"] + 1e-12 and base["lb"] <= ov["ub"] + 1e-12
+    if dtype == "float64":
+        # mixed hands over to float64 one interval later, so only float64 repeats the trajectory
+        assert ov["n_push"] == base["n_push"]
+        assert ov["iters"] == base["iters"] + 50
+        assert ov["ub"] == base["ub"] and ov["lb"] == base["lb"]
+        np.testing.assert_array_equal(fit1, fit0)
