@@ -292,8 +292,10 @@ def main():
     d_p = torch.from_numpy(p).cuda()
     prob_dev = _lib.BMProblem(n, mp, d_menu.data_ptr(), d_alt.data_ptr(), d_p.data_ptr(), 1)
     prob_host = ctx.bm_problem(n, menu, alt, p)
+    # checks overlapped with the next interval (rumb_bm_params.overlap_check): the same certified
+    # bracket, reached one interval (50 iterations) later, with the float64 check off the critical path
     par = ctx.bm_params(beta, check=CHECK, abs_tol=ABS_TOL, rel_tol=None, dtype=args.dtype, max_iter=10 ** 7,
-                        time_limit=600)
+                        time_limit=600, overlap_check=True)
     if args.profile_case > 0:
         par.max_iter = args.profile_case
         r, _, _ = ctx.bm_solve((prob_dev, None), par, want_fit=False)
@@ -380,6 +382,7 @@ def main():
                    "checks_per_solve": int(res["n_push"]),
                    "ub": res["ub"], "lb": res["lb"], "state_dtype": args.dtype,
                    "l2": "flushed (256 MB write) before every timed solve; state slabs exceed L2",
+                   "check_overlap": True,
                    "parallelism": "replicas x%d" % world},
         "e2e": {"value": world * 1e3 / e2e_ms, "unit": "solves/s", "h2d_bytes_per_step": int(mp * 16),
                 "d2h_bytes_per_step": int(mp * 8 + 64 * res_e2e["n_push"] + 104)},

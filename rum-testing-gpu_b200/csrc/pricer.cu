@@ -15,6 +15,7 @@
 //     lanes read the same row at the same time (a broadcast), with the lane's own predicate.
 //   * quantization blocks are 1024 consecutive ranks: one CTA of 1024 threads per block, block
 //     min / max (exact, order-free), step = (max - min) / levels and q = rintf((v - min) / step)
+//     (the values themselves come from a separate launch over 256-rank tiles, see below)
 //     with IEEE division; the previous layer is decoded as fma(q, step, min) (fma_decode = 1,
 //     the contraction the reference's JIT compiler applies to m + q * e) or as a rounded multiply
 //     then add (fma_decode = 0).
@@ -62,10 +63,27 @@ __device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
     return __fadd_rn(m, __fmul_rn(qf, e));
 }
 
-__global__ void __launch_bounds__(PB) stream_layer_kernel(PricerArgs A) {
-    __shared__ float smin[PB / 32], smax[PB / 32];
+// One popcount layer of the stream sweep, in two launches.
+//
+// stream_eval_kernel: a CTA of 1024 threads covers PE_R = 256 consecutive ranks with PE_G = 4
+// groups of alternatives (warp w: ranks 32 (w mod 8) .., group w / 8 = the x with x mod 4 equal to
+// it), so a layer of C ranks spreads over C / 256 CTAs instead of C / 1024. Each thread walks its
+// group's x from high to low (the rows of x in order, one float32 add at a time, a warp-uniform row
+// loop), keeps the candidate with `>=` (ties -> lowest x); the four group winners of a rank are
+// merged the same way (the larger value, on a tie the lower x), which is the sequential descending
+// loop's winner. Output: the float32 value (and the predecessor byte) per rank.
+// stream_quant_kernel: one CTA per quantization block of 1024 ranks, as the number format asks:
+// block min / max, step, rintf quantization of every value (u16 / u24 modes).
+constexpr int PE_R = 256, PE_G = 4;
+
+__global__ void __launch_bounds__(1024) stream_eval_kernel(PricerArgs A, float *vals) {
+    __shared__ float pbest[PE_G][PE_R];
+    __shared__ signed char pbx[PE_G][PE_R];
     const int n = A.n, k = A.k;
-    const ull r = (ull)blockIdx.x * PB + threadIdx.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rg = w & 7, xg = w >> 3;
+    const int loc = rg * 32 + lane;
+    const ull r = (ull)blockIdx.x * PE_R + loc;
     const bool valid = r < A.count;
     // colex unranking of r into D (elements ascending)
     ull D = 0;
@@ -80,38 +98,57 @@ __global__ void __launch_bounds__(PB) stream_layer_kernel(PricerArgs A) {
         }
     }
     float best = 0.0f;
-    int bestx = 0;
-    bool seen = false;
-    ull suf = 0, remain = r;
-    int t = k;                                      // elements of D at or above x still to visit
+    int bestx = -1;
     for (int x = n - 1; x >= 0; --x) {
-        bool in = valid && ((D >> x) & 1ULL);
-        // sequential float32 sum of x's rows with menu subset of D (warp-uniform row loop)
-        float w = 0.0f;
+        if ((x & (PE_G - 1)) != xg) continue;            // uniform per warp
+        const bool in = valid && ((D >> x) & 1ULL);
+        float wsum = 0.0f;
         const ll lo = A.offsets[x], hi = A.offsets[x + 1];
         if (__any_sync(0xffffffffu, in)) {
             for (ll i = lo; i < hi; ++i) {
                 ull Dp = __ldg(A.menus + i);
                 float sc = __ldg(A.scores + i);
-                if (in && (Dp & D) == Dp) w = __fadd_rn(w, sc);
+                if (in && (Dp & D) == Dp) wsum = __fadd_rn(wsum, sc);
             }
         }
         if (in) {
-            --t;                                    // x is element t of D (0-based, ascending)
-            remain -= A.binom[x * (n + 1) + (t + 1)];
-            ull rp = remain + suf;
-            suf += A.binom[x * (n + 1) + t];
-            float vp = decode_prev(A, rp);
-            float cand = __fadd_rn(vp, w);
-            if (!seen || cand >= best) { best = cand; seen = true; bestx = x; }
+            // colex rank of D \ {x}: with D's elements d_0 < ... and x = d_j,
+            // sum_{i<j} C(d_i, i+1) + sum_{i>j} C(d_i, i) = r - sum_{i>=j} C(d_i, i+1) + sum_{i>j} C(d_i, i)
+            int i = __popcll(D & ((1ULL << x) - 1ULL));
+            const int j = i;
+            ull sub = 0, add = 0;
+            for (ull E = D & ~((1ULL << x) - 1ULL); E; E &= E - 1ULL, ++i) {
+                const int d = __ffsll((long long)E) - 1;
+                sub += A.binom[d * (n + 1) + (i + 1)];
+                if (i > j) add += A.binom[d * (n + 1) + i];
+            }
+            const ull rp = r - sub + add;
+            const float cand = __fadd_rn(decode_prev(A, rp), wsum);
+            if (bestx < 0 || cand >= best) { best = cand; bestx = x; }
         }
     }
-    if (valid && A.pred) A.pred[r] = (uint8_t)bestx;
-    if (A.mode == 1) {
-        if (valid) A.vcur_f[r] = best;
-        return;
+    pbest[xg][loc] = best;
+    pbx[xg][loc] = (signed char)bestx;
+    __syncthreads();
+    if (xg != 0 || !valid) return;
+    float b = pbest[0][loc];
+    int bx = pbx[0][loc];
+    for (int g = 1; g < PE_G; ++g) {
+        const float c = pbest[g][loc];
+        const int cx = pbx[g][loc];
+        if (cx < 0) continue;
+        if (bx < 0 || c > b || (c == b && cx < bx)) { b = c; bx = cx; }
     }
-    // block min / max over the valid ranks
+    if (A.pred) A.pred[r] = (uint8_t)bx;
+    if (A.mode == 1) A.vcur_f[r] = b;
+    else vals[r] = b;
+}
+
+__global__ void __launch_bounds__(PB) stream_quant_kernel(PricerArgs A, const float *vals) {
+    __shared__ float smin[PB / 32], smax[PB / 32];
+    const ull r = (ull)blockIdx.x * PB + threadIdx.x;
+    const bool valid = r < A.count;
+    const float best = valid ? vals[r] : 0.0f;
     float tmin = valid ? best : 3.0e38f, tmax = valid ? best : -3.0e38f;
     for (int o = 16; o > 0; o >>= 1) {
         tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
@@ -291,6 +328,7 @@ struct Pricer {
     DevBuf pred_ptrs;                       // device array of pred pointers (n+1)
     DevBuf layer_step;                      // n+1 uints (float bits)
     DevBuf Vs, Ps;                          // sub-lattice / mask scratch
+    DevBuf vals;                            // a layer's float32 values before quantization
     DevBuf out;                             // PriceOut
     std::vector<ll> host_offsets;
 };
@@ -349,6 +387,7 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
         ull cap = 0;
         for (ull v : P->counts) cap = v > cap ? v : cap;
         ull nblk = (cap + PB - 1) / PB;
+        P->vals.ensure((size_t)cap * 4);
         for (int i = 0; i < 2; ++i) {
             P->v[i].ensure((size_t)cap * (mode == 1 ? 4 : 2));
             if (mode == 3) P->l[i].ensure((size_t)cap);
@@ -431,9 +470,12 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
             A.ecur = P->e[cur].as<float>();
             A.pred = k >= P->k_pred ? P->pred[k]->as<uint8_t>() : nullptr;
             A.layer_step = P->layer_step.as<unsigned int>() + k;
-            unsigned grid = (unsigned)((A.count + PB - 1) / PB);
-            stream_layer_kernel<<<grid, PB, 0, st>>>(A);
-            RUMB_LAUNCH("stream_layer_kernel");
+            stream_eval_kernel<<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, P->vals.as<float>());
+            RUMB_LAUNCH("stream_eval_kernel");
+            if (A.mode != 1) {
+                stream_quant_kernel<<<(unsigned)((A.count + PB - 1) / PB), PB, 0, st>>>(A, P->vals.as<float>());
+                RUMB_LAUNCH("stream_quant_kernel");
+            }
             std::swap(cur, prev);
         }
         backtrace_kernel<<<1, 1024, 0, st>>>(n, P->k_pred, P->binom.as<ull>(), P->pred_ptrs.as<uint8_t *>(), menus,
