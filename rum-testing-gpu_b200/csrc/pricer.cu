@@ -65,23 +65,24 @@ __device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
 
 // One popcount layer of the stream sweep, in two launches.
 //
-// stream_eval_kernel: a CTA of 1024 threads covers PE_R = 256 consecutive ranks with PE_G = 4
-// groups of alternatives (warp w: ranks 32 (w mod 8) .., group w / 8 = the x with x mod 4 equal to
-// it), so a layer of C ranks spreads over C / 256 CTAs instead of C / 1024. Each thread walks its
+// stream_eval_kernel: a CTA of 1024 threads covers PE_R = 128 consecutive ranks with PE_G = 8
+// groups of alternatives (warp w: ranks 32 (w mod 4) .., group w / 4 = the x with x mod 8 equal to
+// it), so a layer of C ranks spreads over C / 128 CTAs instead of C / 1024. Each thread walks its
 // group's x from high to low (the rows of x in order, one float32 add at a time, a warp-uniform row
 // loop), keeps the candidate with `>=` (ties -> lowest x); the four group winners of a rank are
 // merged the same way (the larger value, on a tie the lower x), which is the sequential descending
 // loop's winner. Output: the float32 value (and the predecessor byte) per rank.
 // stream_quant_kernel: one CTA per quantization block of 1024 ranks, as the number format asks:
 // block min / max, step, rintf quantization of every value (u16 / u24 modes).
-constexpr int PE_R = 256, PE_G = 4;
+constexpr int PE_R = 128, PE_G = 8;
+static_assert((PE_R / 32) * PE_G == 32 && (PE_G & (PE_G - 1)) == 0, "32 warps; PE_G a power of two");
 
 __global__ void __launch_bounds__(1024) stream_eval_kernel(PricerArgs A, float *vals) {
     __shared__ float pbest[PE_G][PE_R];
     __shared__ signed char pbx[PE_G][PE_R];
     const int n = A.n, k = A.k;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rg = w & 7, xg = w >> 3;
+    const int rg = w % (PE_R / 32), xg = w / (PE_R / 32);
     const int loc = rg * 32 + lane;
     const ull r = (ull)blockIdx.x * PE_R + loc;
     const bool valid = r < A.count;
