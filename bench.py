@@ -5,6 +5,7 @@
     python bench.py --profile-case ITERS [--dtype ...]   # one solve capped at ITERS iterations, for
                                                           # profilers; prints no bench line
     python bench.py --workload bootstrap_n20             # batched bootstrap draws vs one at a time
+    python bench.py --workload paper                     # paper instances beside the reference's times
 
 Workload "n18_d1pct_k50": every menu of 18 alternatives with >= 2 members kept with probability
 0.01 (2,627 menus, 23,650 observed cells), p_hat from a Dirichlet(1) mixture of 50 random linear
@@ -250,6 +251,44 @@ def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
     print(json.dumps(line), flush=True)
 
 
+# published RTX 5090 figures for the paper instances (the reference's records)
+PAPER = {
+    "bm_admm_n20_d1pct": {"seconds": 45.09, "iterations": 7800, "bracket": [18.603539524, 18.621794959],
+                          "record": "replication/feasibility_in_density/results/cert_bm_admm_n20_d1pct.json"},
+    "flow_cg_n18_d1pct": {"seconds": 15.86, "columns": 848, "record": "data/opt_refs.json (key n18_d1pct)"},
+}
+
+
+def run_paper(args, rank):
+    """Workload paper: the reference's certified runs on two of its paper instances, regenerated
+    from its generator (sha256 fingerprints checked): BM-ADMM on n20_d1pct (104,885 cells) in
+    float64, rel 1e-3, bounds every 200 iterations; Flow-CG on n18_d1pct (23,568 cells), rel 1e-3.
+    Prints the library's times beside the reference's published RTX 5090 times (its records)."""
+    if rank != 0:
+        return
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import paper_instances as PI
+    from rumb import RUM
+    out = {}
+    for key, n, cat, method, margs in (("bm_admm_n20_d1pct", 20, "d1pct", "bm_admm", {"dtype": "float64", "check": 200}),
+                                      ("flow_cg_n18_d1pct", 18, "d1pct", "flow_cg", None)):
+        cd, mp = PI.get_instance(n, cat)
+        rum = RUM(cd[:, 0].astype(np.int64), cd[:, 1].astype(np.int64), cd[:, 2], num_alternatives=n)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = rum.calculate_distance(method=method, method_args=margs, abs_tol=0.0, rel_tol=1e-3, max_time=600)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        out[key] = {"seconds": sec, "lb": r.lb, "ub": r.ub, "iterations": r.iterations, "unit": r.iteration_unit,
+                    "status": r.status, "cells": int(mp), "fingerprint": PI.fingerprint(cd),
+                    "reference_rtx5090": PAPER[key], "speedup_vs_published": PAPER[key]["seconds"] / sec}
+    line = {"metric": "paper instances: certified solve seconds (rel 1e-3)", "value": out["bm_admm_n20_d1pct"]["seconds"],
+            "unit": "s", "higher_is_better": False, "n_gpus": 1, "data": "the reference's paper instances (regenerated)",
+            "runs": out}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -259,8 +298,9 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20"],
-                    help="bootstrap_n20: the batched-draw comparison (prints its own line)")
+    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper"],
+                    help="bootstrap_n20: the batched-draw comparison; paper: the reference's certified runs on "
+                         "its paper instances beside its published times (each prints its own line)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
                     help="run one solve capped at ITERS iterations (for ncu) and print no bench line")
     args = ap.parse_args()
@@ -271,6 +311,9 @@ def main():
         return
     if args.workload == "bootstrap_n20":
         run_bootstrap(args, rank)
+        return
+    if args.workload == "paper":
+        run_paper(args, rank)
         return
 
     import torch
