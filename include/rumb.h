@@ -216,6 +216,11 @@ RUMB_API int rumb_bm_solve_batch(rumb_ctx *ctx, const rumb_bm_problem *prob, con
 #define RUMB_PRICE_F32 1  /* rank-indexed, two live layers, float32 */
 #define RUMB_PRICE_U16 2  /* rank-indexed, 16-bit mantissa per rank + float32 (offset, step) per 1024 ranks */
 #define RUMB_PRICE_U24 3  /* rank-indexed, 24-bit mantissa per rank + float32 (offset, step) per 1024 ranks */
+/* OR-ed into mode: evaluate w(x, D) by scanning x's rows in every sweep. Without it the pricer
+ * builds, once, for every pair (D, x in D) the list of x's rows whose menu is a subset of D, in
+ * row order (when n <= 26, the lists have < 2^32 entries and fit a quarter of the free device
+ * memory), and a sweep adds exactly those rows' scores: the same float32 sums, far fewer tests. */
+#define RUMB_PRICE_SCAN 16
 
 /* A pricer over the rows (menu bitmask, alternative) in x-major order: offsets[x]..offsets[x+1]
  * are alternative x's rows (offsets has n+1 entries, offsets[n] = mp). k_pred: predecessors are
@@ -232,6 +237,10 @@ RUMB_API int rumb_cg_pricer_create(rumb_ctx *ctx, int n, long long mp, const uin
 RUMB_API int rumb_cg_price(rumb_cg_pricer *pricer, const float *scores, int on_device, double *vmax,
                            int32_t *rank_pos, double *margin, float *layer_step);
 RUMB_API int rumb_cg_pricer_destroy(rumb_cg_pricer *pricer);
+/* list_entries = the number of cover-list entries (-1 when the pricer scans rows), list_bytes =
+ * their device bytes with the offsets. Either pointer may be NULL. (No counterpart in the
+ * reference, which always scans.) */
+RUMB_API int rumb_cg_pricer_info(const rumb_cg_pricer *pricer, long long *list_entries, long long *list_bytes);
 
 /* ---------------------------------------------------------------- profiling */
 typedef struct {

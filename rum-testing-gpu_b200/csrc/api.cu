@@ -258,6 +258,14 @@ int rumb_cg_price(rumb_cg_pricer *pr, const float *scores, int on_device, double
     RUMB_API_END
 }
 
+int rumb_cg_pricer_info(const rumb_cg_pricer *pr, long long *list_entries, long long *list_bytes) {
+    RUMB_API_BEGIN
+    if (!pr || !pr->p) rumb::fail(RUMB_E_INVAL, "pricer is NULL");
+    rumb::pricer_info(pr->p, list_entries, list_bytes);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
 int rumb_cg_pricer_destroy(rumb_cg_pricer *pr) {
     RUMB_API_BEGIN
     if (!pr) return RUMB_OK;

@@ -21,6 +21,10 @@
 //     then add (fma_decode = 0).
 //   * the sub-lattice DP after the descent uses the original menus and row order restricted to
 //     the node reached, which is what the reference's relabelled sub-problem adds up.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "ctx.cuh"
@@ -52,7 +56,27 @@ struct PricerArgs {
     float *mcur, *ecur;
     uint8_t *pred;             // nullptr when this layer keeps no predecessors
     unsigned int *layer_step;  // float bits, atomicMax (steps are >= 0)
+    // mask mode: the layer's nodes, values and predecessors indexed by the mask
+    const int *nodes;
+    float *vmask;
+    uint8_t *pmask;
+    // w(x, D): row scan or cover lists (W_SCAN / W_LIST16 / W_LIST32)
+    int wmode;
+    const unsigned *loffs;
+    const void *lent;
+    ull lbase;                 // this layer's first pair index
 };
+
+__device__ ull colex_rank_dev(ull mask, const ull *binom, int n) {
+    ull r = 0;
+    int t = 0;
+    for (int b = 0; b < n; ++b)
+        if ((mask >> b) & 1ULL) {
+            ++t;
+            r += binom[b * (n + 1) + t];
+        }
+    return r;
+}
 
 __device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
     if (A.mode == 1) return A.vprev_f[rp];
@@ -63,21 +87,70 @@ __device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
     return __fadd_rn(m, __fmul_rn(qf, e));
 }
 
-// One popcount layer of the stream sweep, in two launches.
+// Cover lists. Only a small share of the (D, x, row) tests of a sweep succeed (a row of menu m
+// qualifies for 2^(n - |m|) of the 2^(n-1) subsets D containing its alternative), and the menus do
+// not change between sweeps of one pricer. So the pricer builds, once, for every pair (D, x in D)
+// the list of x's rows whose menu is a subset of D, in row order, as indices local to x's rows;
+// a sweep then adds exactly those rows' scores in that order, which is the same float32 sum as the
+// row scan. Pair (D, x) of layer k = |D|, colex rank r of D and position j of x among D's elements
+// (ascending) has index layer_base[k] + r k + j, with layer_base[k] = sum_{i<k} C(n, i) i, so a
+// layer's lists are contiguous. offs[p]..offs[p+1] delimit pair p's entries (uint32 offsets);
+// entries are uint16 when every alternative has <= 65536 rows, else uint32.
+enum { W_SCAN = 0, W_LIST16 = 1, W_LIST32 = 2 };
+
+// w(x, D) by scanning x's rows: a warp-uniform row loop (broadcast loads) with the lane's own
+// subset test; every lane of the warp must call it.
+__device__ __forceinline__ float w_scan(const ull *menus, const float *scores, ll lo, ll hi, ull D, bool in) {
+    float w = 0.0f;
+    if (__any_sync(0xffffffffu, in)) {
+        for (ll i = lo; i < hi; ++i) {
+            ull Dp = __ldg(menus + i);
+            float sc = __ldg(scores + i);
+            if (in && (Dp & D) == Dp) w = __fadd_rn(w, sc);
+        }
+    }
+    return w;
+}
+
+// w(x, D) from pair p's cover list (sx = x's first score).
+template <class IT>
+__device__ __forceinline__ float w_list(const unsigned *offs, const IT *ent, ull p, const float *sx) {
+    const unsigned b = __ldg(offs + p), e = __ldg(offs + p + 1);
+    float w = 0.0f;
+#pragma unroll 4
+    for (unsigned i = b; i < e; ++i) w = __fadd_rn(w, __ldg(sx + __ldg(ent + i)));
+    return w;
+}
+
+__device__ __forceinline__ float w_of(const PricerArgs &A, int x, ull D, bool in, ull p) {
+    const ll lo = A.offsets[x];
+    if (A.wmode == W_SCAN) return w_scan(A.menus, A.scores, lo, A.offsets[x + 1], D, in);
+    if (!in) return 0.0f;
+    if (A.wmode == W_LIST16) return w_list(A.loffs, (const uint16_t *)A.lent, p, A.scores + lo);
+    return w_list(A.loffs, (const uint32_t *)A.lent, p, A.scores + lo);
+}
+
+// One popcount layer k of the sweep.
 //
-// stream_eval_kernel: a CTA of 1024 threads covers PE_R = 128 consecutive ranks with PE_G = 8
+// layer_eval_kernel: a CTA of 1024 threads covers PE_R = 128 consecutive ranks with PE_G = 8
 // groups of alternatives (warp w: ranks 32 (w mod 4) .., group w / 4 = the x with x mod 8 equal to
-// it), so a layer of C ranks spreads over C / 128 CTAs instead of C / 1024. Each thread walks its
-// group's x from high to low (the rows of x in order, one float32 add at a time, a warp-uniform row
-// loop), keeps the candidate with `>=` (ties -> lowest x); the four group winners of a rank are
-// merged the same way (the larger value, on a tie the lower x), which is the sequential descending
-// loop's winner. Output: the float32 value (and the predecessor byte) per rank.
+// it), so a layer of C ranks spreads over C / 128 CTAs. Each thread walks its group's x from high
+// to low, keeps the candidate with `>=` (ties -> lowest x); the eight group winners of a rank are
+// merged the same way (the larger value, on a tie the lower x). That is the winner of the
+// reference's loops in both modes: x descending with `>=` (stream) and x ascending with `>`
+// (mask) both keep the lowest x among equal values.
+//   MASK: the subset of rank r is the layer table's node r (ascending masks of popcount k, i.e.
+//         colex order), values and predecessors are indexed by the mask and updated in place.
+//   stream: D is the colex unranking of r; the value of D \ {x} is read from the previous layer's
+//         storage at its colex rank; output: the float32 value (f32 mode, and the predecessor
+//         byte) or the value for stream_quant_kernel to quantize (u16 / u24).
 // stream_quant_kernel: one CTA per quantization block of 1024 ranks, as the number format asks:
 // block min / max, step, rintf quantization of every value (u16 / u24 modes).
 constexpr int PE_R = 128, PE_G = 8;
 static_assert((PE_R / 32) * PE_G == 32 && (PE_G & (PE_G - 1)) == 0, "32 warps; PE_G a power of two");
 
-__global__ void __launch_bounds__(1024) stream_eval_kernel(PricerArgs A, float *vals) {
+template <bool MASK>
+__global__ void __launch_bounds__(1024) layer_eval_kernel(PricerArgs A, float *vals) {
     __shared__ float pbest[PE_G][PE_R];
     __shared__ signed char pbx[PE_G][PE_R];
     const int n = A.n, k = A.k;
@@ -86,45 +159,47 @@ __global__ void __launch_bounds__(1024) stream_eval_kernel(PricerArgs A, float *
     const int loc = rg * 32 + lane;
     const ull r = (ull)blockIdx.x * PE_R + loc;
     const bool valid = r < A.count;
-    // colex unranking of r into D (elements ascending)
     ull D = 0;
     if (valid) {
-        ull rr = r;
-        int b = n - 1;
-        for (int t = k; t >= 1; --t) {
-            while (A.binom[b * (n + 1) + t] > rr) --b;
-            D |= 1ULL << b;
-            rr -= A.binom[b * (n + 1) + t];
-            --b;
+        if (MASK) {
+            D = (ull)(unsigned)A.nodes[r];
+        } else {
+            // colex unranking of r into D (elements ascending)
+            ull rr = r;
+            int b = n - 1;
+            for (int t = k; t >= 1; --t) {
+                while (A.binom[b * (n + 1) + t] > rr) --b;
+                D |= 1ULL << b;
+                rr -= A.binom[b * (n + 1) + t];
+                --b;
+            }
         }
     }
+    const ull pbase = A.lbase + r * (ull)k;
     float best = 0.0f;
     int bestx = -1;
     for (int x = n - 1; x >= 0; --x) {
         if ((x & (PE_G - 1)) != xg) continue;            // uniform per warp
         const bool in = valid && ((D >> x) & 1ULL);
-        float wsum = 0.0f;
-        const ll lo = A.offsets[x], hi = A.offsets[x + 1];
-        if (__any_sync(0xffffffffu, in)) {
-            for (ll i = lo; i < hi; ++i) {
-                ull Dp = __ldg(A.menus + i);
-                float sc = __ldg(A.scores + i);
-                if (in && (Dp & D) == Dp) wsum = __fadd_rn(wsum, sc);
-            }
-        }
+        const int j = __popcll(D & ((1ULL << x) - 1ULL));
+        const float wsum = w_of(A, x, D, in, pbase + j);
         if (in) {
-            // colex rank of D \ {x}: with D's elements d_0 < ... and x = d_j,
-            // sum_{i<j} C(d_i, i+1) + sum_{i>j} C(d_i, i) = r - sum_{i>=j} C(d_i, i+1) + sum_{i>j} C(d_i, i)
-            int i = __popcll(D & ((1ULL << x) - 1ULL));
-            const int j = i;
-            ull sub = 0, add = 0;
-            for (ull E = D & ~((1ULL << x) - 1ULL); E; E &= E - 1ULL, ++i) {
-                const int d = __ffsll((long long)E) - 1;
-                sub += A.binom[d * (n + 1) + (i + 1)];
-                if (i > j) add += A.binom[d * (n + 1) + i];
+            float prev;
+            if (MASK) {
+                prev = A.vmask[D ^ (1ULL << x)];
+            } else {
+                // colex rank of D \ {x}: with D's elements d_0 < ... and x = d_j,
+                // sum_{i<j} C(d_i, i+1) + sum_{i>j} C(d_i, i) = r - sum_{i>=j} C(d_i, i+1) + sum_{i>j} C(d_i, i)
+                int i = j;
+                ull sub = 0, add = 0;
+                for (ull E = D & ~((1ULL << x) - 1ULL); E; E &= E - 1ULL, ++i) {
+                    const int d = __ffsll((long long)E) - 1;
+                    sub += A.binom[d * (n + 1) + (i + 1)];
+                    if (i > j) add += A.binom[d * (n + 1) + i];
+                }
+                prev = decode_prev(A, r - sub + add);
             }
-            const ull rp = r - sub + add;
-            const float cand = __fadd_rn(decode_prev(A, rp), wsum);
+            const float cand = __fadd_rn(prev, wsum);
             if (bestx < 0 || cand >= best) { best = cand; bestx = x; }
         }
     }
@@ -140,9 +215,47 @@ __global__ void __launch_bounds__(1024) stream_eval_kernel(PricerArgs A, float *
         if (cx < 0) continue;
         if (bx < 0 || c > b || (c == b && cx < bx)) { b = c; bx = cx; }
     }
+    if (MASK) {
+        A.vmask[D] = b;
+        A.pmask[D] = (uint8_t)bx;
+        return;
+    }
     if (A.pred) A.pred[r] = (uint8_t)bx;
     if (A.mode == 1) A.vcur_f[r] = b;
     else vals[r] = b;
+}
+
+// Cover-list construction, once per pricer: thread per subset D (mask order, all layers in one
+// launch); the warp walks the alternatives in order and scans x's rows for its lanes with x in D
+// (broadcast loads). COUNT: offs[pair] = the number of rows; else the rows' local indices are
+// written from offs[pair] on (offs then holds the exclusive prefix sums).
+template <bool COUNT, class IT>
+__global__ void cover_build_kernel(int n, ull nD, const ull *binom, const ull *layer_base, const ull *menus,
+                                   const ll *offsets, unsigned *offs, IT *ent) {
+    const ull D = blockIdx.x * (ull)blockDim.x + threadIdx.x;
+    const bool valid = D < nD && D != 0;
+    ull p = 0;
+    if (valid) {
+        const int k = __popcll(D);
+        p = layer_base[k] + colex_rank_dev(D, binom, n) * (ull)k;
+    }
+    for (int x = 0; x < n; ++x) {
+        const bool in = valid && ((D >> x) & 1ULL);
+        if (__any_sync(0xffffffffu, in)) {
+            const ll lo = offsets[x], hi = offsets[x + 1];
+            unsigned c = 0;
+            const unsigned o = (!COUNT && in) ? offs[p] : 0u;
+            for (ll i = lo; i < hi; ++i) {
+                const ull Dp = __ldg(menus + i);
+                if (in && (Dp & D) == Dp) {
+                    if (!COUNT) ent[o + c] = (IT)(i - lo);
+                    ++c;
+                }
+            }
+            if (COUNT && in) offs[p] = c;
+        }
+        if (in) ++p;
+    }
 }
 
 __global__ void __launch_bounds__(PB) stream_quant_kernel(PricerArgs A, const float *vals) {
@@ -178,47 +291,6 @@ __global__ void __launch_bounds__(PB) stream_quant_kernel(PricerArgs A, const fl
     }
 }
 
-// Mask-indexed layer: thread per node of layer c (node ids from the popcount-ordered table).
-__global__ void mask_layer_kernel(const int *nodes, ll ns, const ull *menus, const float *scores, const ll *offsets,
-                                  int n, float *V, uint8_t *pred) {
-    ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
-    bool valid = i < ns;
-    ull D = valid ? (ull)(unsigned)nodes[i] : 0ULL;
-    float best = 0.0f;
-    bool seen = false;
-    int bx = 0;
-    for (int x = 0; x < n; ++x) {
-        bool in = valid && ((D >> x) & 1ULL);
-        float w = 0.0f;
-        if (__any_sync(0xffffffffu, in)) {
-            for (ll j = offsets[x]; j < offsets[x + 1]; ++j) {
-                ull Dp = __ldg(menus + j);
-                float sc = __ldg(scores + j);
-                if (in && (Dp & D) == Dp) w = __fadd_rn(w, sc);
-            }
-        }
-        if (in) {
-            float cand = __fadd_rn(V[D ^ (1ULL << x)], w);
-            if (!seen || cand > best) { best = cand; seen = true; bx = x; }
-        }
-    }
-    if (valid) {
-        V[D] = best;
-        pred[D] = (uint8_t)bx;
-    }
-}
-
-__device__ ull colex_rank_dev(ull mask, const ull *binom, int n) {
-    ull r = 0;
-    int t = 0;
-    for (int b = 0; b < n; ++b)
-        if ((mask >> b) & 1ULL) {
-            ++t;
-            r += binom[b * (n + 1) + t];
-        }
-    return r;
-}
-
 // Result block written by the device backtrace (one small D2H copy per price call).
 struct PriceOut {
     float vtop;            // f32 value at the full set (f32 / mask modes)
@@ -233,7 +305,8 @@ struct PriceOut {
 __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *const *preds, const ull *menus,
                                  const float *scores, const ll *offsets, float *Vs, uint8_t *Ps, PriceOut *out,
                                  const float *vtop_f, const uint16_t *vtop_h, const uint8_t *ltop, const float *mtop,
-                                 const float *etop, int mode) {
+                                 const float *etop, int mode, int wmode, const unsigned *loffs, const void *lent,
+                                 const ull *layer_base) {
     __shared__ ull sD;
     __shared__ int elems[MAXN_PR];
     __shared__ int spos;
@@ -275,13 +348,20 @@ __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *c
             float best = 0.0f;
             bool seen = false;
             int bj = 0;
+            const ull pbase = wmode == W_SCAN ? 0 : layer_base[c] + colex_rank_dev(Dorig, binom, n) * (ull)c;
             for (int j = 0; j < K; ++j) {
                 if (!((s >> j) & 1ULL)) continue;
                 int x = elems[j];
                 float w = 0.0f;
-                for (ll i = offsets[x]; i < offsets[x + 1]; ++i) {
-                    ull Dp = menus[i];
-                    if ((Dp & Dorig) == Dp) w = __fadd_rn(w, scores[i]);
+                if (wmode == W_SCAN) {
+                    for (ll i = offsets[x]; i < offsets[x + 1]; ++i) {
+                        ull Dp = menus[i];
+                        if ((Dp & Dorig) == Dp) w = __fadd_rn(w, scores[i]);
+                    }
+                } else {
+                    const ull p = pbase + __popcll(Dorig & ((1ULL << x) - 1ULL));
+                    w = wmode == W_LIST16 ? w_list(loffs, (const uint16_t *)lent, p, scores + offsets[x])
+                                          : w_list(loffs, (const uint32_t *)lent, p, scores + offsets[x]);
                 }
                 float cand = __fadd_rn(Vs[s ^ (1ULL << j)], w);
                 if (!seen || cand > best) { best = cand; seen = true; bj = j; }
@@ -332,6 +412,12 @@ struct Pricer {
     DevBuf vals;                            // a layer's float32 values before quantization
     DevBuf out;                             // PriceOut
     std::vector<ll> host_offsets;
+    // cover lists (wmode != W_SCAN)
+    int wmode = W_SCAN;
+    ull list_entries = 0;
+    size_t list_bytes = 0;
+    std::vector<ull> lbase;                 // first pair index per layer (n+2)
+    DevBuf lbase_dev, loffs, lent;
 };
 
 static std::vector<ull> binom_host(int n) {
@@ -344,8 +430,64 @@ static std::vector<ull> binom_host(int n) {
     return t;
 }
 
+// Builds the cover lists when they fit: n <= 26, fewer than 2^32 entries and at most a quarter of
+// the device's free memory; otherwise the sweeps scan x's rows.
+static void build_cover_lists(Pricer &P, const uint64_t *menus_host) {
+    const int n = P.n;
+    if (P.mp == 0 || n > 26) return;
+    const ull pairs = (ull)n << (n - 1);
+    // a row of menu m qualifies for the 2^(n - |m|) subsets containing m (exact in a double)
+    double entries = 0.0;
+    for (ll i = 0; i < P.mp; ++i) entries += std::ldexp(1.0, n - __builtin_popcountll(menus_host[i]));
+    ll maxrows = 0;
+    for (int x = 0; x < n; ++x) maxrows = std::max(maxrows, P.host_offsets[x + 1] - P.host_offsets[x]);
+    const bool idx16 = maxrows <= 65536;
+    const double bytes = (double)(pairs + 1) * 4.0 + entries * (idx16 ? 2.0 : 4.0);
+    size_t free_b = 0, total_b = 0;
+    RUMB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (entries >= 4294967295.0 || bytes > 0.25 * (double)free_b) return;
+    cudaStream_t st = P.c->own;
+    std::vector<ull> bt = binom_host(n);
+    P.lbase.assign(n + 2, 0);
+    for (int k = 0; k <= n; ++k) P.lbase[k + 1] = P.lbase[k] + bt[n * (n + 1) + k] * (ull)k;
+    P.lbase_dev.ensure((size_t)(n + 2) * 8);
+    RUMB_CUDA(cudaMemcpyAsync(P.lbase_dev.ptr, P.lbase.data(), (size_t)(n + 2) * 8, cudaMemcpyHostToDevice, st));
+    P.loffs.ensure((size_t)(pairs + 1) * 4);
+    RUMB_CUDA(cudaMemsetAsync(P.loffs.ptr, 0, (size_t)(pairs + 1) * 4, st));
+    const ull nD = 1ULL << n;
+    unsigned *offs = P.loffs.as<unsigned>();
+    cover_build_kernel<true, uint32_t><<<grid_for((ll)nD, 256), 256, 0, st>>>(
+        n, nD, P.binom.as<ull>(), P.lbase_dev.as<ull>(), P.menus.as<ull>(), P.offsets.as<ll>(), offs, nullptr);
+    RUMB_LAUNCH("cover_build_kernel<count>");
+    size_t tmp_bytes = 0;
+    RUMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, offs, offs, (ll)(pairs + 1), st));
+    DevBuf tmp;
+    tmp.ensure(std::max<size_t>(tmp_bytes, 16));
+    RUMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tmp_bytes, offs, offs, (ll)(pairs + 1), st));
+    unsigned total = 0;
+    RUMB_CUDA(cudaMemcpyAsync(&total, offs + pairs, 4, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    if ((double)total != entries) fail(RUMB_E_INTERNAL, "cover lists: entry count does not match the menus");
+    P.lent.ensure((size_t)total * (idx16 ? 2 : 4) + 16);
+    if (idx16)
+        cover_build_kernel<false, uint16_t><<<grid_for((ll)nD, 256), 256, 0, st>>>(
+            n, nD, P.binom.as<ull>(), P.lbase_dev.as<ull>(), P.menus.as<ull>(), P.offsets.as<ll>(), offs,
+            P.lent.as<uint16_t>());
+    else
+        cover_build_kernel<false, uint32_t><<<grid_for((ll)nD, 256), 256, 0, st>>>(
+            n, nD, P.binom.as<ull>(), P.lbase_dev.as<ull>(), P.menus.as<ull>(), P.offsets.as<ll>(), offs,
+            P.lent.as<uint32_t>());
+    RUMB_LAUNCH("cover_build_kernel<fill>");
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    P.wmode = idx16 ? W_LIST16 : W_LIST32;
+    P.list_entries = total;
+    P.list_bytes = (size_t)bytes;
+}
+
 Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t *offsets, int mode, int k_pred,
                       int fma_decode) {
+    const bool scan = (mode & RUMB_PRICE_SCAN) != 0;
+    mode &= ~RUMB_PRICE_SCAN;
     if (mode < 0 || mode > 3) fail(RUMB_E_INVAL, "pricer mode must be 0 (mask), 1 (f32), 2 (u16) or 3 (u24)");
     if (n < 1 || n > 39) fail(RUMB_E_INVAL, "pricing handles 1 <= n <= 39");
     if (mode == 0 && n > 30) fail(RUMB_E_INVAL, "mask pricing handles n <= 30");
@@ -410,7 +552,13 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
         P->Ps.ensure((size_t)Nsub);
     }
     RUMB_CUDA(cudaStreamSynchronize(st));
+    if (!scan) build_cover_lists(*P, menus);
     return P.release();
+}
+
+void pricer_info(const Pricer *P, long long *list_entries, long long *list_bytes) {
+    if (list_entries) *list_entries = P->wmode == W_SCAN ? -1 : (long long)P->list_entries;
+    if (list_bytes) *list_bytes = P->wmode == W_SCAN ? 0 : (long long)P->list_bytes;
 }
 
 void pricer_destroy(Pricer *P) { delete P; }
@@ -430,17 +578,40 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
     const ull *menus = P->menus.as<ull>();
     const ll *offs = P->offsets.as<ll>();
     RUMB_CUDA(cudaMemsetAsync(P->layer_step.ptr, 0, (size_t)(n + 1) * 4, st));
+    auto args = [&](int k) {
+        PricerArgs A{};
+        A.n = n;
+        A.k = k;
+        A.count = P->counts[k];
+        A.binom = P->binom.as<ull>();
+        A.menus = menus;
+        A.scores = scores;
+        A.offsets = offs;
+        A.mode = P->mode;
+        A.fma_decode = P->fma_decode;
+        A.wmode = P->wmode;
+        A.loffs = P->loffs.as<unsigned>();
+        A.lent = P->lent.ptr;
+        A.lbase = P->wmode == W_SCAN ? 0 : P->lbase[k];
+        return A;
+    };
+    const unsigned *loffs = P->loffs.as<unsigned>();
+    const ull *lbase = P->lbase_dev.as<ull>();
     if (P->mode == 0) {
         RUMB_CUDA(cudaMemsetAsync(P->Vs.ptr, 0, ((size_t)1 << n) * 4, st));
         RUMB_CUDA(cudaMemsetAsync(P->Ps.ptr, 0, (size_t)1 << n, st));
         std::vector<ll> bounds;
         const int *nodes = c.layer_table(n, bounds);
-        for (int cc = 1; cc <= n; ++cc) {
-            ll lo = bounds[cc], ns = bounds[cc + 1] - lo;
-            mask_layer_kernel<<<grid_for(ns, 256), 256, 0, st>>>(nodes + lo, ns, menus, scores, offs, n,
-                                                                  P->Vs.as<float>(), P->Ps.as<uint8_t>());
-            RUMB_LAUNCH("mask_layer_kernel");
+        for (int k = 1; k <= n; ++k) {
+            PricerArgs A = args(k);
+            A.nodes = nodes + bounds[k];
+            A.vmask = P->Vs.as<float>();
+            A.pmask = P->Ps.as<uint8_t>();
+            layer_eval_kernel<true><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, nullptr);
+            RUMB_LAUNCH("layer_eval_kernel<mask>");
         }
+        mask_readout_kernel<<<1, 32, 0, st>>>(n, P->Vs.as<float>(), P->Ps.as<uint8_t>(), P->out.as<PriceOut>());
+        RUMB_LAUNCH("mask_readout_kernel");
     } else {
         int cur = 0, prev = 1;
         // layer 0: V = 0 (offset 0, step 0, q 0)
@@ -449,16 +620,7 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
         RUMB_CUDA(cudaMemsetAsync(P->m[prev].ptr, 0, 4, st));
         RUMB_CUDA(cudaMemsetAsync(P->e[prev].ptr, 0, 4, st));
         for (int k = 1; k <= n; ++k) {
-            PricerArgs A{};
-            A.n = n;
-            A.k = k;
-            A.count = P->counts[k];
-            A.binom = P->binom.as<ull>();
-            A.menus = menus;
-            A.scores = scores;
-            A.offsets = offs;
-            A.mode = P->mode;
-            A.fma_decode = P->fma_decode;
+            PricerArgs A = args(k);
             A.vprev_f = P->v[prev].as<float>();
             A.vprev_h = P->v[prev].as<uint16_t>();
             A.lprev = P->l[prev].as<uint8_t>();
@@ -471,8 +633,8 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
             A.ecur = P->e[cur].as<float>();
             A.pred = k >= P->k_pred ? P->pred[k]->as<uint8_t>() : nullptr;
             A.layer_step = P->layer_step.as<unsigned int>() + k;
-            stream_eval_kernel<<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, P->vals.as<float>());
-            RUMB_LAUNCH("stream_eval_kernel");
+            layer_eval_kernel<false><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, P->vals.as<float>());
+            RUMB_LAUNCH("layer_eval_kernel<stream>");
             if (A.mode != 1) {
                 stream_quant_kernel<<<(unsigned)((A.count + PB - 1) / PB), PB, 0, st>>>(A, P->vals.as<float>());
                 RUMB_LAUNCH("stream_quant_kernel");
@@ -483,12 +645,8 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
                                              scores, offs, P->Vs.as<float>(), P->Ps.as<uint8_t>(),
                                              P->out.as<PriceOut>(), P->v[prev].as<float>(), P->v[prev].as<uint16_t>(),
                                              P->l[prev].as<uint8_t>(), P->m[prev].as<float>(), P->e[prev].as<float>(),
-                                             P->mode);
+                                             P->mode, P->wmode, loffs, P->lent.ptr, lbase);
         RUMB_LAUNCH("backtrace_kernel");
-    }
-    if (P->mode == 0) {
-        mask_readout_kernel<<<1, 32, 0, st>>>(n, P->Vs.as<float>(), P->Ps.as<uint8_t>(), P->out.as<PriceOut>());
-        RUMB_LAUNCH("mask_readout_kernel");
     }
     PriceOut h;
     std::vector<unsigned int> steps(n + 1);

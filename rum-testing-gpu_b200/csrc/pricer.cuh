@@ -10,6 +10,7 @@ void pricer_destroy(Pricer *P);
 void pricer_price(Pricer *P, const float *scores, int on_device, double *vmax, int32_t *rank_pos, double *margin,
                   float *layer_step_out);
 int pricer_device(const Pricer *P);
+void pricer_info(const Pricer *P, long long *list_entries, long long *list_bytes);
 }  // namespace rumb
 
 struct rumb_cg_pricer {

@@ -113,6 +113,7 @@ _SIGS = {
     "rumb_cg_price": ([_vp, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _vp,
                        ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
     "rumb_cg_pricer_destroy": ([_vp], ctypes.c_int),
+    "rumb_cg_pricer_info": ([_vp, _vp, _vp], ctypes.c_int),
     "rumb_bm_iterate": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, _vp, _vp, _vp,
                          ctypes.c_int, ctypes.c_int], ctypes.c_int),
 }
@@ -350,6 +351,7 @@ class Context:
 
 
 PRICE_MODES = {"mask": 0, "f32": 1, "u16": 2, "u24": 3}
+PRICE_SCAN = 16
 
 
 def to_bf16_bits(x):
@@ -432,14 +434,23 @@ class MLP:
 class Pricer:
     """Flow-CG pricer on one GPU (rows in x-major order; see rumb_cg_pricer_create)."""
 
-    def __init__(self, ctx, n, menus, offsets, mode="u24", k_pred=None, fma_decode=True):
+    def __init__(self, ctx, n, menus, offsets, mode="u24", k_pred=None, fma_decode=True, lists=True):
+        """lists=False: scan x's rows in every sweep instead of walking the cover lists."""
         menus = np.ascontiguousarray(menus, dtype=np.uint64)
         offsets = np.ascontiguousarray(offsets, dtype=np.int64)
         h = ctypes.c_void_p()
-        check(load().rumb_cg_pricer_create(ctx.h, int(n), menus.size, _p(menus), _p(offsets), PRICE_MODES[mode],
+        code = PRICE_MODES[mode] | (0 if lists else PRICE_SCAN)
+        check(load().rumb_cg_pricer_create(ctx.h, int(n), menus.size, _p(menus), _p(offsets), code,
                                            0 if k_pred is None else int(k_pred), int(bool(fma_decode)),
                                            ctypes.byref(h)))
         self.h, self.n, self.mp, self.mode, self.ctx = h, int(n), menus.size, mode, ctx
+
+    @property
+    def list_entries(self):
+        """Cover-list entries (-1 when the pricer scans rows)."""
+        e = ctypes.c_longlong()
+        check(load().rumb_cg_pricer_info(self.h, ctypes.byref(e), None))
+        return e.value
 
     def price(self, scores, want_steps=False):
         """(vmax, rank_pos int32[n], margin[, layer_step float32[n+1]]) for float32 scores."""

@@ -35,19 +35,20 @@ def prepare_choice_data(menu, alt, p, n):
 
 
 def ranking_column(menus, alts, rank_pos, n):
-    """0/1 column: row s is 1 when alts[s] is the best-ranked member of menus[s]."""
+    """0/1 column: row s is 1 when alts[s] is the best-ranked member of menus[s] (alternatives
+    visited best first; a row's winner is the first of them in its menu)."""
     rank_pos = np.asarray(rank_pos, dtype=np.int64)
-    memb = ((menus[:, None] >> np.arange(n, dtype=np.uint64)[None, :]) & np.uint64(1)).astype(bool)
-    ranks = np.where(memb, rank_pos[None, :], n + 1)
-    return (np.argmin(ranks, axis=1) == alts).astype(np.uint8)
+    left = np.ones(menus.size, dtype=bool)
+    col = np.zeros(menus.size, dtype=np.uint8)
+    for x in np.argsort(rank_pos, kind="stable"):
+        hit = left & ((menus & np.uint64(1 << int(x))) != 0)
+        col[hit & (alts == x)] = 1
+        left &= ~hit
+    return col
 
 
 def _popcount64(x):
-    x = x.astype(np.uint64)
-    x = x - ((x >> np.uint64(1)) & np.uint64(0x5555555555555555))
-    x = (x & np.uint64(0x3333333333333333)) + ((x >> np.uint64(2)) & np.uint64(0x3333333333333333))
-    x = (x + (x >> np.uint64(4))) & np.uint64(0x0F0F0F0F0F0F0F0F)
-    return (x * np.uint64(0x0101010101010101)) >> np.uint64(56)
+    return np.bitwise_count(np.asarray(x, dtype=np.uint64))
 
 
 def _pack(col):
@@ -76,7 +77,7 @@ class GramMaintainer:
         b = _pack(col)
         self.bits[k] = b
         if k > 0:
-            counts = _popcount64(self.bits[:k] & b).sum(axis=1).astype(np.float64)
+            counts = _popcount64(self.bits[:k] & b).sum(axis=1, dtype=np.int64).astype(np.float64)
             self.Q[k, :k] = counts
             self.Q[:k, k] = counts
         self.Q[k, k] = float(_popcount64(b).sum())
@@ -167,10 +168,26 @@ class CGProblem:
         self.pricer = _lib.Pricer(ctx, n, self.menus, self.offsets, mode=mode, k_pred=k_pred)
 
 
-def solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi_ub_target=None, gap_rel_tol=None,
-             gap_abs_tol=None, init_columns=None, init_lambda=None, early_ub_check=False, lb_stop=None,
-             record_columns=False):
+def _one_blas_thread():
+    """The master's matrices are at most a few hundred wide: a multithreaded BLAS spends more on
+    waking threads than on the factorizations, so the CG loop runs with one BLAS thread."""
+    try:
+        from threadpoolctl import threadpool_limits
+    except ImportError:
+        import contextlib
+        return contextlib.nullcontext()
+    return threadpool_limits(1, user_api="blas")
+
+
+def solve_cg(prob, p, **kw):
     """solve_cgbfqp_cholbitset on a CGProblem with row probabilities p (input row order)."""
+    with _one_blas_thread():
+        return _solve_cg(prob, p, **kw)
+
+
+def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi_ub_target=None, gap_rel_tol=None,
+              gap_abs_tol=None, init_columns=None, init_lambda=None, early_ub_check=False, lb_stop=None,
+              record_columns=False):
     n = prob.n
     t_setup = time.perf_counter()
     p_obs = np.asarray(p, dtype=np.float64)[prob.perm].astype(np.float32).astype(np.float64)

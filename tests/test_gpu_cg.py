@@ -51,6 +51,60 @@ def test_pricer_bit_exact_against_oracle(ctx, name, cd, n, mode):
     pr.close()
 
 
+def _cover_entries(menus, n):
+    pc = np.array([bin(int(v)).count("1") for v in menus])
+    return int(np.sum(np.ldexp(1.0, n - pc)))
+
+
+@pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
+def test_cover_lists_equal_row_scan(ctx, name, cd, n):
+    """The cover-list sweep and the row-scan sweep give the same bits in every storage mode (the
+    scan itself is pinned to the oracle above and by the recorded reference kernels)."""
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    rng = np.random.RandomState(11)
+    scores = [rng.randn(menus.size).astype(np.float32), (p32 - p32.mean()).astype(np.float32),
+              np.round(rng.randn(menus.size) * 4).astype(np.float32)]       # many exact ties
+    for mode in ("mask", "f32", "u16", "u24"):
+        a = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+        b = _lib.Pricer(ctx, n, menus, offsets, mode=mode, lists=False)
+        assert a.list_entries == _cover_entries(menus, n) and b.list_entries == -1
+        for s in scores:
+            va, ra, ma, sa = a.price(s, want_steps=True)
+            vb, rb, mb, sb = b.price(s, want_steps=True)
+            assert va == vb and ma == mb, (mode, va, vb)
+            np.testing.assert_array_equal(ra, rb)
+            np.testing.assert_array_equal(sa, sb)
+        a.close()
+        b.close()
+
+
+def test_cover_lists_wide_alternative(ctx):
+    """An alternative with more than 65536 rows (32-bit list entries): n = 18, alternative 0 observed
+    in every menu of 9 or more that holds it (89,846 rows), the others in a sparse random set."""
+    n = 18
+    rng = np.random.RandomState(5)
+    all_m = np.arange(1, 1 << n, dtype=np.int64)
+    pc = np.array([bin(int(v)).count("1") for v in all_m])
+    wide = all_m[((all_m & 1) == 1) & (pc >= 9)]
+    rest = all_m[(pc >= 2) & (rng.rand(all_m.size) < 0.01)]
+    rest_a = [[x for x in range(1, n) if (int(m) >> x) & 1] for m in rest]
+    rows_m = np.concatenate([wide, np.repeat(rest, [len(r) for r in rest_a])])
+    rows_a = np.concatenate([np.zeros(wide.size, dtype=np.int64), np.concatenate(rest_a).astype(np.int64)])
+    menus, alts, p32, offsets, _ = O.cg_layout(n, rows_m, rows_a, np.ones(rows_m.size))
+    assert offsets[1] - offsets[0] > 65536
+    s = (rng.randn(menus.size) * 0.01).astype(np.float32)
+    for mode in ("mask", "u24"):
+        a = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+        b = _lib.Pricer(ctx, n, menus, offsets, mode=mode, lists=False)
+        assert a.list_entries == _cover_entries(menus, n)
+        va, ra, ma = a.price(s)
+        vb, rb, mb = b.price(s)
+        assert va == vb and ma == mb
+        np.testing.assert_array_equal(ra, rb)
+        a.close()
+        b.close()
+
+
 def test_mask_and_f32_stream_identical(ctx):
     cd, mp = PI.gen_medium(14, mult=4)
     menus, alts, p32, offsets, _ = O.cg_layout(14, cd[:, 0], cd[:, 1], cd[:, 2])
