@@ -66,14 +66,22 @@ class GramMaintainer:
         self.M, self.W = int(M), (int(M) + 63) // 64
         self.phat = np.asarray(phat, dtype=np.float64)
         self.K, self.max_K = 0, int(max_K)
-        self.bits = np.zeros((self.max_K, self.W), dtype=np.uint64)
-        self.Q = np.zeros((self.max_K, self.max_K))
-        self.h = np.zeros(self.max_K)
+        self._grow(min(self.max_K, 256))
+
+    def _grow(self, cap):
+        """Storage for cap columns (doubled as columns arrive, so Q's rows stay close together)."""
+        bits, Q, h = np.zeros((cap, self.W), dtype=np.uint64), np.zeros((cap, cap)), np.zeros(cap)
+        if self.K:
+            k = self.K
+            bits[:k], Q[:k, :k], h[:k] = self.bits[:k], self.Q[:k, :k], self.h[:k]
+        self.bits, self.Q, self.h, self.cap = bits, Q, h, cap
 
     def add_column(self, col):
         k = self.K
         if k >= self.max_K:
             raise RuntimeError("max_K=%d exceeded" % self.max_K)
+        if k >= self.cap:
+            self._grow(min(self.max_K, 2 * self.cap))
         b = _pack(col)
         self.bits[k] = b
         if k > 0:
@@ -100,8 +108,10 @@ class PoutMaintainer:
         self.pos.append(np.where(col.astype(bool))[0].astype(np.int64))
 
     def apply_delta(self, delta):
+        # np.add.at adds in index order, one element at a time: the same float64 sums as the
+        # reference's fancy-index += (a column's positions are distinct), without its temporaries
         for a in np.where(np.abs(delta) > 1e-12)[0]:
-            self.p_out[self.pos[int(a)]] += float(delta[a])
+            np.add.at(self.p_out, self.pos[int(a)], float(delta[a]))
 
 
 def project_simplex(y):
@@ -124,7 +134,8 @@ def solve_qp_native(Q, h, A_init=None, max_outer=200, tol=1e-10, reg=1e-12):
         A_arr = np.asarray(A, dtype=np.int64)
         k = len(A)
         ones_A = np.ones(k)
-        Q_AA = Q[np.ix_(A_arr, A_arr)] + reg * np.eye(k)
+        Q_AA = Q[np.ix_(A_arr, A_arr)]
+        Q_AA[np.diag_indices(k)] += reg       # = Q_AA + reg * I bit for bit (the entries are >= 0)
         h_A = h[A_arr]
         try:
             cf = cho_factor(Q_AA, lower=True, check_finite=False)
