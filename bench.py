@@ -6,6 +6,7 @@
                                                           # profilers; prints no bench line
     python bench.py --workload bootstrap_n20             # batched bootstrap draws vs one at a time
     python bench.py --workload paper                     # paper instances beside the reference's times
+    python bench.py --workload pricing --steps 20        # Flow-CG pricing sweeps alone
 
 Workload "n18_d1pct_k50": every menu of 18 alternatives with >= 2 members kept with probability
 0.01 (2,627 menus, 23,650 observed cells), p_hat from a Dirichlet(1) mixture of 50 random linear
@@ -180,9 +181,10 @@ def run_reference(args, rank):
 
 
 def pricing_sweeps(ctx, stream, sweeps=20):
-    """Flow-CG pricing at n = 18, 0.5 % menus (workload n18_d05pct_k50): the uint24 and uint16
-    stream sweeps (one full Bellman-Ford pass over the lattice plus the backtrace, read back each
-    sweep), timed with CUDA events on the bench stream; seeded float32 scores resident on the GPU."""
+    """Flow-CG pricing at n = 18, 0.5 % menus (workload n18_d05pct_k50): the uint24, uint16 and mask
+    sweeps over the cover lists and the uint24 sweep scanning rows (one full Bellman-Ford pass over
+    the lattice plus the backtrace, read back each sweep), timed with CUDA events on the bench
+    stream; seeded float32 scores resident on the GPU."""
     import torch
     from rumb import _lib, flow_cg
     from rumb.instances import config_instance
@@ -190,8 +192,8 @@ def pricing_sweeps(ctx, stream, sweeps=20):
     menus, alts, p32, offsets, _ = flow_cg.prepare_choice_data(menu, alt, p, n)
     scores = torch.from_numpy(np.random.default_rng(0).standard_normal(menus.size).astype(np.float32)).cuda()
     out = {"workload": "n18_d05pct_k50", "rows": int(menus.size), "subset_tests_per_sweep": int(menus.size) << (n - 1)}
-    for mode in ("u24", "u16"):
-        pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+    for mode, lists in (("u24", True), ("u16", True), ("mask", True), ("u24", False)):
+        pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode, lists=lists)
         for _ in range(3):
             pr.price_device(scores.data_ptr())
         torch.cuda.synchronize()
@@ -202,10 +204,32 @@ def pricing_sweeps(ctx, stream, sweeps=20):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / sweeps
-        out[mode] = {"ms_per_sweep": ms, "sweeps_per_s": 1e3 / ms,
-                     "subset_tests_per_s": out["subset_tests_per_sweep"] / (ms * 1e-3)}
+        entries = pr.list_entries
+        if lists:
+            out["cover_list_entries"] = entries
+        # the cover lists read per sweep: n 2^(n-1) + 1 uint32 offsets and the uint16 entries
+        list_bytes = 4 * ((n << (n - 1)) + 1) + 2 * entries if entries >= 0 else 0
+        out[mode if lists else mode + "_row_scan"] = {
+            "ms_per_sweep": ms, "sweeps_per_s": 1e3 / ms,
+            "subset_tests_per_s": out["subset_tests_per_sweep"] / (ms * 1e-3),
+            "list_bytes_per_sweep": list_bytes, "list_gb_per_s": list_bytes / (ms * 1e-3) / 1e9}
         pr.close()
     return out
+
+
+def run_pricing(args, rank):
+    """Workload pricing: the Flow-CG pricing sweeps of n18_d05pct_k50 alone (cover lists in the
+    u24, u16 and mask storages, and the row scan for comparison), one JSON line."""
+    if rank != 0:
+        return
+    import torch
+    from rumb import _lib
+    ctx = _lib.Context(0)
+    stream = torch.cuda.current_stream()
+    res = pricing_sweeps(ctx, stream, sweeps=max(args.steps, 1))
+    print(json.dumps({"metric": "Flow-CG pricing sweeps/s (n = 18, 0.5 % menus)", "value": res["u24"]["sweeps_per_s"],
+                      "unit": "sweeps/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u24",
+                      "data": "synthetic", "config": {"workload": "n18_d05pct_k50"}, "pricing": res}), flush=True)
 
 
 def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
@@ -298,7 +322,7 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper"],
+    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing"],
                     help="bootstrap_n20: the batched-draw comparison; paper: the reference's certified runs on "
                          "its paper instances beside its published times (each prints its own line)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
@@ -314,6 +338,9 @@ def main():
         return
     if args.workload == "paper":
         run_paper(args, rank)
+        return
+    if args.workload == "pricing":
+        run_pricing(args, rank)
         return
 
     import torch
