@@ -78,6 +78,40 @@ __device__ ull colex_rank_dev(ull mask, const ull *binom, int n) {
     return r;
 }
 
+// The binomial table C(b, t) at b*(n+1)+t, staged into shared memory by the whole CTA (the
+// unranking and ranking below walk it with dependent lookups).
+constexpr int BIN_MAX = (MAXN_PR + 1) * (MAXN_PR + 1);
+__device__ __forceinline__ void stage_binom(ull *sbin, const ull *binom, int n) {
+    for (int i = threadIdx.x; i < (n + 1) * (n + 1); i += blockDim.x) sbin[i] = binom[i];
+}
+
+// Colex unranking of r into a k-subset of [0, n) (elements ascending).
+__device__ __forceinline__ ull colex_unrank(ull r, int k, int n, const ull *bin) {
+    ull D = 0;
+    int b = n - 1;
+    for (int t = k; t >= 1; --t) {
+        while (bin[b * (n + 1) + t] > r) --b;
+        D |= 1ULL << b;
+        r -= bin[b * (n + 1) + t];
+        --b;
+    }
+    return D;
+}
+
+// Colex rank of D \ {x} from r = rank of D: with D's elements d_0 < ... and x = d_j (j = the
+// number of elements below x), sum_{i<j} C(d_i, i+1) + sum_{i>j} C(d_i, i)
+// = r - sum_{i>=j} C(d_i, i+1) + sum_{i>j} C(d_i, i).
+__device__ __forceinline__ ull colex_rank_without(ull r, ull D, int x, int j, int n, const ull *bin) {
+    int i = j;
+    ull sub = 0, add = 0;
+    for (ull E = D & ~((1ULL << x) - 1ULL); E; E &= E - 1ULL, ++i) {
+        const int d = __ffsll((long long)E) - 1;
+        sub += bin[d * (n + 1) + (i + 1)];
+        if (i > j) add += bin[d * (n + 1) + i];
+    }
+    return r - sub + add;
+}
+
 __device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
     if (A.mode == 1) return A.vprev_f[rp];
     unsigned int q = A.vprev_h[rp];
@@ -153,28 +187,19 @@ template <bool MASK>
 __global__ void __launch_bounds__(1024) layer_eval_kernel(PricerArgs A, float *vals) {
     __shared__ float pbest[PE_G][PE_R];
     __shared__ signed char pbx[PE_G][PE_R];
+    __shared__ ull sbin[MASK ? 1 : BIN_MAX];
     const int n = A.n, k = A.k;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rg = w % (PE_R / 32), xg = w / (PE_R / 32);
     const int loc = rg * 32 + lane;
     const ull r = (ull)blockIdx.x * PE_R + loc;
     const bool valid = r < A.count;
-    ull D = 0;
-    if (valid) {
-        if (MASK) {
-            D = (ull)(unsigned)A.nodes[r];
-        } else {
-            // colex unranking of r into D (elements ascending)
-            ull rr = r;
-            int b = n - 1;
-            for (int t = k; t >= 1; --t) {
-                while (A.binom[b * (n + 1) + t] > rr) --b;
-                D |= 1ULL << b;
-                rr -= A.binom[b * (n + 1) + t];
-                --b;
-            }
-        }
+    if (!MASK) {
+        stage_binom(sbin, A.binom, n);
+        __syncthreads();
     }
+    ull D = 0;
+    if (valid) D = MASK ? (ull)(unsigned)A.nodes[r] : colex_unrank(r, k, n, sbin);
     const ull pbase = A.lbase + r * (ull)k;
     float best = 0.0f;
     int bestx = -1;
@@ -185,20 +210,8 @@ __global__ void __launch_bounds__(1024) layer_eval_kernel(PricerArgs A, float *v
         const float wsum = w_of(A, x, D, in, pbase + j);
         if (in) {
             float prev;
-            if (MASK) {
-                prev = A.vmask[D ^ (1ULL << x)];
-            } else {
-                // colex rank of D \ {x}: with D's elements d_0 < ... and x = d_j,
-                // sum_{i<j} C(d_i, i+1) + sum_{i>j} C(d_i, i) = r - sum_{i>=j} C(d_i, i+1) + sum_{i>j} C(d_i, i)
-                int i = j;
-                ull sub = 0, add = 0;
-                for (ull E = D & ~((1ULL << x) - 1ULL); E; E &= E - 1ULL, ++i) {
-                    const int d = __ffsll((long long)E) - 1;
-                    sub += A.binom[d * (n + 1) + (i + 1)];
-                    if (i > j) add += A.binom[d * (n + 1) + i];
-                }
-                prev = decode_prev(A, r - sub + add);
-            }
+            if (MASK) prev = A.vmask[D ^ (1ULL << x)];
+            else prev = decode_prev(A, colex_rank_without(r, D, x, j, n, sbin));
             const float cand = __fadd_rn(prev, wsum);
             if (bestx < 0 || cand >= best) { best = cand; bestx = x; }
         }
@@ -223,6 +236,65 @@ __global__ void __launch_bounds__(1024) layer_eval_kernel(PricerArgs A, float *v
     if (A.pred) A.pred[r] = (uint8_t)bx;
     if (A.mode == 1) A.vcur_f[r] = b;
     else vals[r] = b;
+}
+
+// The same layer for long lists (the top layers, where a subset's lists hold up to all of x's
+// rows): one CTA per rank, warp w takes the alternatives x = w, w + NW, ... in D. The warp walks
+// pair (D, x)'s list 32 entries at a time (coalesced index loads, 32 score gathers in flight, the
+// next chunk loaded while this one is added) and adds the chunk's scores in list order through
+// shuffles, so each sum is the same sequence of float32 additions as one thread's loop. The
+// candidates then merge in x order with `>` (ties -> lowest x).
+template <bool MASK, class IT>
+__global__ void __launch_bounds__(1024) layer_wide_kernel(PricerArgs A, float *vals) {
+    __shared__ ull sbin[MASK ? 1 : BIN_MAX];
+    __shared__ float cv[MAXN_PR];
+    __shared__ ull sD;
+    const int n = A.n, k = A.k;
+    const ull r = blockIdx.x;
+    const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (!MASK) stage_binom(sbin, A.binom, n);
+    __syncthreads();
+    if (threadIdx.x == 0) sD = MASK ? (ull)(unsigned)A.nodes[r] : colex_unrank(r, k, n, sbin);
+    __syncthreads();
+    const ull D = sD;
+    const ull pbase = A.lbase + r * (ull)k;
+    const IT *ent = (const IT *)A.lent;
+    for (int x = w; x < n; x += nw) {
+        if (!((D >> x) & 1ULL)) continue;                 // uniform per warp
+        const int j = __popcll(D & ((1ULL << x) - 1ULL));
+        const unsigned b = __ldg(A.loffs + pbase + j), e = __ldg(A.loffs + pbase + j + 1);
+        const float *sx = A.scores + A.offsets[x];
+        float wsum = 0.0f;
+        float v = (b + lane < e) ? __ldg(sx + __ldg(ent + b + lane)) : 0.0f;
+        for (unsigned c = b; c < e; c += 32) {
+            const unsigned nx = c + 32 + lane;
+            const float vn = nx < e ? __ldg(sx + __ldg(ent + nx)) : 0.0f;
+            const int m = (e - c) < 32u ? (int)(e - c) : 32;
+            for (int u = 0; u < m; ++u) wsum = __fadd_rn(wsum, __shfl_sync(0xffffffffu, v, u));
+            v = vn;
+        }
+        if (lane == 0) {
+            const float prev = MASK ? A.vmask[D ^ (1ULL << x)]
+                                    : decode_prev(A, colex_rank_without(r, D, x, j, n, sbin));
+            cv[x] = __fadd_rn(prev, wsum);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    float best = 0.0f;
+    int bx = -1;
+    for (int x = 0; x < n; ++x) {
+        if (!((D >> x) & 1ULL)) continue;
+        if (bx < 0 || cv[x] > best) { best = cv[x]; bx = x; }
+    }
+    if (MASK) {
+        A.vmask[D] = best;
+        A.pmask[D] = (uint8_t)bx;
+        return;
+    }
+    if (A.pred) A.pred[r] = (uint8_t)bx;
+    if (A.mode == 1) A.vcur_f[r] = best;
+    else vals[r] = best;
 }
 
 // Cover-list construction, once per pricer: thread per subset D (mask order, all layers in one
@@ -310,11 +382,14 @@ __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *c
     __shared__ ull sD;
     __shared__ int elems[MAXN_PR];
     __shared__ int spos;
+    __shared__ ull sbin[BIN_MAX];
+    stage_binom(sbin, binom, n);
+    __syncthreads();
     if (threadIdx.x == 0) {
         ull D = (n >= 64) ? ~0ULL : ((1ULL << n) - 1ULL);
         int pos = 0;
         for (int k = n; k > k_pred; --k) {
-            ull r = colex_rank_dev(D, binom, n);
+            ull r = colex_rank_dev(D, sbin, n);
             int x = preds[k][r];
             out->rank_pos[x] = pos++;
             D ^= 1ULL << x;
@@ -348,7 +423,7 @@ __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *c
             float best = 0.0f;
             bool seen = false;
             int bj = 0;
-            const ull pbase = wmode == W_SCAN ? 0 : layer_base[c] + colex_rank_dev(Dorig, binom, n) * (ull)c;
+            const ull pbase = wmode == W_SCAN ? 0 : layer_base[c] + colex_rank_dev(Dorig, sbin, n) * (ull)c;
             for (int j = 0; j < K; ++j) {
                 if (!((s >> j) & 1ULL)) continue;
                 int x = elems[j];
@@ -418,7 +493,10 @@ struct Pricer {
     size_t list_bytes = 0;
     std::vector<ull> lbase;                 // first pair index per layer (n+2)
     DevBuf lbase_dev, loffs, lent;
+    std::vector<char> wide;                 // per layer: layer_wide_kernel (1) or layer_eval_kernel (0)
 };
+
+static void run_sweep(Pricer *P, const float *scores, bool calibrate);
 
 static std::vector<ull> binom_host(int n) {
     std::vector<ull> t((size_t)(n + 1) * (n + 1), 0);
@@ -445,7 +523,7 @@ static void build_cover_lists(Pricer &P, const uint64_t *menus_host) {
     const double bytes = (double)(pairs + 1) * 4.0 + entries * (idx16 ? 2.0 : 4.0);
     size_t free_b = 0, total_b = 0;
     RUMB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    if (entries >= 4294967295.0 || bytes > 0.25 * (double)free_b) return;
+    if (entries >= 4294967295.0 - 64.0 || bytes > 0.25 * (double)free_b) return;
     cudaStream_t st = P.c->own;
     std::vector<ull> bt = binom_host(n);
     P.lbase.assign(n + 2, 0);
@@ -482,6 +560,10 @@ static void build_cover_lists(Pricer &P, const uint64_t *menus_host) {
     P.wmode = idx16 ? W_LIST16 : W_LIST32;
     P.list_entries = total;
     P.list_bytes = (size_t)bytes;
+    // pick each layer's kernel by timing one sweep (zero scores; both kernels give the same bits)
+    RUMB_CUDA(cudaMemsetAsync(P.scores.ptr, 0, (size_t)P.mp * 4, st));
+    run_sweep(&P, P.scores.as<float>(), true);
+    RUMB_CUDA(cudaStreamSynchronize(st));
 }
 
 Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t *offsets, int mode, int k_pred,
@@ -552,6 +634,7 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
         P->Ps.ensure((size_t)Nsub);
     }
     RUMB_CUDA(cudaStreamSynchronize(st));
+    P->wide.assign(n + 1, 0);
     if (!scan) build_cover_lists(*P, menus);
     return P.release();
 }
@@ -565,18 +648,51 @@ void pricer_destroy(Pricer *P) { delete P; }
 
 int pricer_device(const Pricer *P) { return P->c->device; }
 
-void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vmax, int32_t *rank_pos, double *margin,
-                  float *layer_step_out) {
+// One sweep over the lattice on the context's stream, ending with the backtrace (stream storage)
+// or the readout (mask storage) into P->out. calibrate: time each layer with both layer kernels
+// (they write the same values) and keep the faster one for the layer.
+static void run_sweep(Pricer *P, const float *scores, bool calibrate) {
     Ctx &c = *P->c;
     cudaStream_t st = c.own;
-    int n = P->n;
-    const float *scores = scores_host;
-    if (!on_device) {
-        if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->scores.ptr, scores_host, (size_t)P->mp * 4, cudaMemcpyHostToDevice, st));
-        scores = P->scores.as<float>();
-    }
+    const int n = P->n;
     const ull *menus = P->menus.as<ull>();
     const ll *offs = P->offsets.as<ll>();
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    if (calibrate)
+        for (auto &e : ev) RUMB_CUDA(cudaEventCreate(&e));
+    auto layer = [&](PricerArgs &A, bool mask, float *vals) {
+        auto thread_kernel = [&]() {
+            if (mask) layer_eval_kernel<true><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, vals);
+            else layer_eval_kernel<false><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, vals);
+            RUMB_LAUNCH("layer_eval_kernel");
+        };
+        auto wide_kernel = [&]() {
+            const unsigned threads = 32u * (unsigned)std::min(n, 32), grid = (unsigned)A.count;
+            if (mask && P->wmode == W_LIST16) layer_wide_kernel<true, uint16_t><<<grid, threads, 0, st>>>(A, vals);
+            else if (mask) layer_wide_kernel<true, uint32_t><<<grid, threads, 0, st>>>(A, vals);
+            else if (P->wmode == W_LIST16) layer_wide_kernel<false, uint16_t><<<grid, threads, 0, st>>>(A, vals);
+            else layer_wide_kernel<false, uint32_t><<<grid, threads, 0, st>>>(A, vals);
+            RUMB_LAUNCH("layer_wide_kernel");
+        };
+        if (P->wmode == W_SCAN) {
+            thread_kernel();
+        } else if (calibrate) {
+            float t_thread = 0.0f, t_wide = 0.0f;
+            RUMB_CUDA(cudaEventRecord(ev[0], st));
+            thread_kernel();
+            RUMB_CUDA(cudaEventRecord(ev[1], st));
+            wide_kernel();
+            RUMB_CUDA(cudaEventRecord(ev[2], st));
+            RUMB_CUDA(cudaEventSynchronize(ev[2]));
+            RUMB_CUDA(cudaEventElapsedTime(&t_thread, ev[0], ev[1]));
+            RUMB_CUDA(cudaEventElapsedTime(&t_wide, ev[1], ev[2]));
+            P->wide[A.k] = t_wide < t_thread ? 1 : 0;
+        } else if (P->wide[A.k]) {
+            wide_kernel();
+        } else {
+            thread_kernel();
+        }
+    };
     RUMB_CUDA(cudaMemsetAsync(P->layer_step.ptr, 0, (size_t)(n + 1) * 4, st));
     auto args = [&](int k) {
         PricerArgs A{};
@@ -607,8 +723,7 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
             A.nodes = nodes + bounds[k];
             A.vmask = P->Vs.as<float>();
             A.pmask = P->Ps.as<uint8_t>();
-            layer_eval_kernel<true><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, nullptr);
-            RUMB_LAUNCH("layer_eval_kernel<mask>");
+            layer(A, true, nullptr);
         }
         mask_readout_kernel<<<1, 32, 0, st>>>(n, P->Vs.as<float>(), P->Ps.as<uint8_t>(), P->out.as<PriceOut>());
         RUMB_LAUNCH("mask_readout_kernel");
@@ -633,8 +748,7 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
             A.ecur = P->e[cur].as<float>();
             A.pred = k >= P->k_pred ? P->pred[k]->as<uint8_t>() : nullptr;
             A.layer_step = P->layer_step.as<unsigned int>() + k;
-            layer_eval_kernel<false><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, P->vals.as<float>());
-            RUMB_LAUNCH("layer_eval_kernel<stream>");
+            layer(A, false, P->vals.as<float>());
             if (A.mode != 1) {
                 stream_quant_kernel<<<(unsigned)((A.count + PB - 1) / PB), PB, 0, st>>>(A, P->vals.as<float>());
                 RUMB_LAUNCH("stream_quant_kernel");
@@ -648,6 +762,21 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
                                              P->mode, P->wmode, loffs, P->lent.ptr, lbase);
         RUMB_LAUNCH("backtrace_kernel");
     }
+    if (calibrate)
+        for (auto &e : ev) cudaEventDestroy(e);
+}
+
+void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vmax, int32_t *rank_pos, double *margin,
+                  float *layer_step_out) {
+    Ctx &c = *P->c;
+    cudaStream_t st = c.own;
+    int n = P->n;
+    const float *scores = scores_host;
+    if (!on_device) {
+        if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->scores.ptr, scores_host, (size_t)P->mp * 4, cudaMemcpyHostToDevice, st));
+        scores = P->scores.as<float>();
+    }
+    run_sweep(P, scores, false);
     PriceOut h;
     std::vector<unsigned int> steps(n + 1);
     RUMB_CUDA(cudaMemcpyAsync(&h, P->out.ptr, sizeof(PriceOut), cudaMemcpyDeviceToHost, st));
