@@ -373,12 +373,13 @@ struct PriceOut {
 };
 
 // Descent through the stored predecessor layers (stream modes), then the mask DP on the
-// sub-lattice of the node reached; one CTA. V/pred scratch: 2^K entries (K = k_pred).
+// sub-lattice of the node reached; one CTA. V/pred scratch: 2^K entries (K = k_pred); Ws: the
+// 2^K K sub-lattice sums.
 __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *const *preds, const ull *menus,
                                  const float *scores, const ll *offsets, float *Vs, uint8_t *Ps, PriceOut *out,
                                  const float *vtop_f, const uint16_t *vtop_h, const uint8_t *ltop, const float *mtop,
                                  const float *etop, int mode, int wmode, const unsigned *loffs, const void *lent,
-                                 const ull *layer_base) {
+                                 const ull *layer_base, float *Ws) {
     __shared__ ull sD;
     __shared__ int elems[MAXN_PR];
     __shared__ int spos;
@@ -413,32 +414,41 @@ __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *c
     const int K = __popcll(D);
     const ull Nsub = 1ULL << K;
     for (ull s = threadIdx.x; s < Nsub; s += blockDim.x) { Vs[s] = 0.0f; Ps[s] = 0; }
+    // w(x_j, D(s)) for every sub-lattice node s and member j: independent of the DP, so all of them
+    // at once (Ws[s K + j]), then the layers only add and compare
+    for (ull t = threadIdx.x; t < Nsub * (ull)K; t += blockDim.x) {
+        const ull s = t / (ull)K;
+        const int j = (int)(t - s * (ull)K);
+        if (!((s >> j) & 1ULL)) continue;
+        ull Dorig = 0;
+        for (int i = 0; i < K; ++i)
+            if ((s >> i) & 1ULL) Dorig |= 1ULL << elems[i];
+        const int x = elems[j];
+        float w = 0.0f;
+        if (wmode == W_SCAN) {
+            for (ll i = offsets[x]; i < offsets[x + 1]; ++i) {
+                ull Dp = menus[i];
+                if ((Dp & Dorig) == Dp) w = __fadd_rn(w, scores[i]);
+            }
+        } else {
+            const int c = __popcll(s);
+            const ull p = layer_base[c] + colex_rank_dev(Dorig, sbin, n) * (ull)c +
+                          __popcll(Dorig & ((1ULL << x) - 1ULL));
+            w = wmode == W_LIST16 ? w_list(loffs, (const uint16_t *)lent, p, scores + offsets[x])
+                                  : w_list(loffs, (const uint32_t *)lent, p, scores + offsets[x]);
+        }
+        Ws[t] = w;
+    }
     __syncthreads();
     for (int c = 1; c <= K; ++c) {
         for (ull s = threadIdx.x; s < Nsub; s += blockDim.x) {
             if (__popcll(s) != c) continue;
-            ull Dorig = 0;
-            for (int j = 0; j < K; ++j)
-                if ((s >> j) & 1ULL) Dorig |= 1ULL << elems[j];
             float best = 0.0f;
             bool seen = false;
             int bj = 0;
-            const ull pbase = wmode == W_SCAN ? 0 : layer_base[c] + colex_rank_dev(Dorig, sbin, n) * (ull)c;
             for (int j = 0; j < K; ++j) {
                 if (!((s >> j) & 1ULL)) continue;
-                int x = elems[j];
-                float w = 0.0f;
-                if (wmode == W_SCAN) {
-                    for (ll i = offsets[x]; i < offsets[x + 1]; ++i) {
-                        ull Dp = menus[i];
-                        if ((Dp & Dorig) == Dp) w = __fadd_rn(w, scores[i]);
-                    }
-                } else {
-                    const ull p = pbase + __popcll(Dorig & ((1ULL << x) - 1ULL));
-                    w = wmode == W_LIST16 ? w_list(loffs, (const uint16_t *)lent, p, scores + offsets[x])
-                                          : w_list(loffs, (const uint32_t *)lent, p, scores + offsets[x]);
-                }
-                float cand = __fadd_rn(Vs[s ^ (1ULL << j)], w);
+                float cand = __fadd_rn(Vs[s ^ (1ULL << j)], Ws[s * (ull)K + j]);
                 if (!seen || cand > best) { best = cand; seen = true; bj = j; }
             }
             Vs[s] = best;
@@ -484,6 +494,7 @@ struct Pricer {
     DevBuf pred_ptrs;                       // device array of pred pointers (n+1)
     DevBuf layer_step;                      // n+1 uints (float bits)
     DevBuf Vs, Ps;                          // sub-lattice / mask scratch
+    DevBuf Ws;                              // sub-lattice sums w(x_j, D(s)): 2^k_pred * k_pred floats
     DevBuf vals;                            // a layer's float32 values before quantization
     DevBuf out;                             // PriceOut
     std::vector<ll> host_offsets;
@@ -496,7 +507,10 @@ struct Pricer {
     std::vector<char> wide;                 // per layer: layer_wide_kernel (1) or layer_eval_kernel (0)
 };
 
-static void run_sweep(Pricer *P, const float *scores, bool calibrate);
+// Mean cover-list length from which a layer runs layer_wide_kernel (measured at n = 18: a mean of
+// 82 entries takes 68 us with a thread per pair and 13 us with a warp per pair; 41 entries, 41 and
+// 49 us).
+constexpr double WIDE_MIN_LIST = 64.0;
 
 static std::vector<ull> binom_host(int n) {
     std::vector<ull> t((size_t)(n + 1) * (n + 1), 0);
@@ -560,10 +574,15 @@ static void build_cover_lists(Pricer &P, const uint64_t *menus_host) {
     P.wmode = idx16 ? W_LIST16 : W_LIST32;
     P.list_entries = total;
     P.list_bytes = (size_t)bytes;
-    // pick each layer's kernel by timing one sweep (zero scores; both kernels give the same bits)
-    RUMB_CUDA(cudaMemsetAsync(P.scores.ptr, 0, (size_t)P.mp * 4, st));
-    run_sweep(&P, P.scores.as<float>(), true);
-    RUMB_CUDA(cudaStreamSynchronize(st));
+    // each layer's kernel from its mean list length (both kernels give the same bits): one thread per
+    // pair while lists are short, a warp per pair from WIDE_MIN_LIST entries on
+    std::vector<unsigned> at(n + 2, 0);
+    for (int k = 1; k <= n + 1; ++k)
+        RUMB_CUDA(cudaMemcpy(&at[k], offs + P.lbase[k], 4, cudaMemcpyDeviceToHost));
+    for (int k = 1; k <= n; ++k) {
+        const double pairs_k = (double)(P.lbase[k + 1] - P.lbase[k]);
+        P.wide[k] = pairs_k > 0 && (double)(at[k + 1] - at[k]) >= WIDE_MIN_LIST * pairs_k ? 1 : 0;
+    }
 }
 
 Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t *offsets, int mode, int k_pred,
@@ -632,6 +651,7 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
         ull Nsub = 1ULL << P->k_pred;
         P->Vs.ensure((size_t)Nsub * 4);
         P->Ps.ensure((size_t)Nsub);
+        P->Ws.ensure((size_t)Nsub * P->k_pred * 4);
     }
     RUMB_CUDA(cudaStreamSynchronize(st));
     P->wide.assign(n + 1, 0);
@@ -649,17 +669,13 @@ void pricer_destroy(Pricer *P) { delete P; }
 int pricer_device(const Pricer *P) { return P->c->device; }
 
 // One sweep over the lattice on the context's stream, ending with the backtrace (stream storage)
-// or the readout (mask storage) into P->out. calibrate: time each layer with both layer kernels
-// (they write the same values) and keep the faster one for the layer.
-static void run_sweep(Pricer *P, const float *scores, bool calibrate) {
+// or the readout (mask storage) into P->out.
+static void run_sweep(Pricer *P, const float *scores) {
     Ctx &c = *P->c;
     cudaStream_t st = c.own;
     const int n = P->n;
     const ull *menus = P->menus.as<ull>();
     const ll *offs = P->offsets.as<ll>();
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    if (calibrate)
-        for (auto &e : ev) RUMB_CUDA(cudaEventCreate(&e));
     auto layer = [&](PricerArgs &A, bool mask, float *vals) {
         auto thread_kernel = [&]() {
             if (mask) layer_eval_kernel<true><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, vals);
@@ -674,24 +690,8 @@ static void run_sweep(Pricer *P, const float *scores, bool calibrate) {
             else layer_wide_kernel<false, uint32_t><<<grid, threads, 0, st>>>(A, vals);
             RUMB_LAUNCH("layer_wide_kernel");
         };
-        if (P->wmode == W_SCAN) {
-            thread_kernel();
-        } else if (calibrate) {
-            float t_thread = 0.0f, t_wide = 0.0f;
-            RUMB_CUDA(cudaEventRecord(ev[0], st));
-            thread_kernel();
-            RUMB_CUDA(cudaEventRecord(ev[1], st));
-            wide_kernel();
-            RUMB_CUDA(cudaEventRecord(ev[2], st));
-            RUMB_CUDA(cudaEventSynchronize(ev[2]));
-            RUMB_CUDA(cudaEventElapsedTime(&t_thread, ev[0], ev[1]));
-            RUMB_CUDA(cudaEventElapsedTime(&t_wide, ev[1], ev[2]));
-            P->wide[A.k] = t_wide < t_thread ? 1 : 0;
-        } else if (P->wide[A.k]) {
-            wide_kernel();
-        } else {
-            thread_kernel();
-        }
+        if (P->wmode != W_SCAN && P->wide[A.k]) wide_kernel();
+        else thread_kernel();
     };
     RUMB_CUDA(cudaMemsetAsync(P->layer_step.ptr, 0, (size_t)(n + 1) * 4, st));
     auto args = [&](int k) {
@@ -759,11 +759,9 @@ static void run_sweep(Pricer *P, const float *scores, bool calibrate) {
                                              scores, offs, P->Vs.as<float>(), P->Ps.as<uint8_t>(),
                                              P->out.as<PriceOut>(), P->v[prev].as<float>(), P->v[prev].as<uint16_t>(),
                                              P->l[prev].as<uint8_t>(), P->m[prev].as<float>(), P->e[prev].as<float>(),
-                                             P->mode, P->wmode, loffs, P->lent.ptr, lbase);
+                                             P->mode, P->wmode, loffs, P->lent.ptr, lbase, P->Ws.as<float>());
         RUMB_LAUNCH("backtrace_kernel");
     }
-    if (calibrate)
-        for (auto &e : ev) cudaEventDestroy(e);
 }
 
 void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vmax, int32_t *rank_pos, double *margin,
@@ -776,7 +774,7 @@ void pricer_price(Pricer *P, const float *scores_host, int on_device, double *vm
         if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->scores.ptr, scores_host, (size_t)P->mp * 4, cudaMemcpyHostToDevice, st));
         scores = P->scores.as<float>();
     }
-    run_sweep(P, scores, false);
+    run_sweep(P, scores);
     PriceOut h;
     std::vector<unsigned int> steps(n + 1);
     RUMB_CUDA(cudaMemcpyAsync(&h, P->out.ptr, sizeof(PriceOut), cudaMemcpyDeviceToHost, st));
