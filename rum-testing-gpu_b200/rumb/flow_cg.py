@@ -125,29 +125,40 @@ def project_simplex(y):
     return np.maximum(y - css[rho - 1] / rho, 0.0)
 
 
-def solve_qp_native(Q, h, A_init=None, max_outer=200, tol=1e-10, reg=1e-12):
-    """Active set + Cholesky for min 1/2 lam'Q lam - h'lam over the simplex; (lam, support)."""
+def solve_qp_native(Q, h, A_init=None, max_outer=200, tol=1e-10, reg=1e-12, memo=None):
+    """Active set + Cholesky for min 1/2 lam'Q lam - h'lam over the simplex; (lam, support).
+
+    memo: a dict kept across the calls of one CG run. Q's and h's entries never change once a
+    column is in (columns are only appended), so the solve for an active set seen in the previous
+    call's last step (the warm start's set, as a rule) is that step's result, bit for bit; it is
+    reused instead of factorized again."""
     K = len(h)
     A = [int(i) for i in (A_init if A_init is not None else []) if 0 <= i < K] or [int(np.argmax(h))]
     lam_A, A_arr = None, None
     for _ in range(max_outer):
         A_arr = np.asarray(A, dtype=np.int64)
         k = len(A)
-        ones_A = np.ones(k)
-        Q_AA = Q[np.ix_(A_arr, A_arr)]
-        Q_AA[np.diag_indices(k)] += reg       # = Q_AA + reg * I bit for bit (the entries are >= 0)
-        h_A = h[A_arr]
-        try:
-            cf = cho_factor(Q_AA, lower=True, check_finite=False)
-            sol = cho_solve(cf, np.column_stack([h_A, ones_A]), check_finite=False)
-            Q_inv_h, Q_inv_e = sol[:, 0], sol[:, 1]
-        except np.linalg.LinAlgError:
-            Q_inv_h = np.linalg.lstsq(Q_AA, h_A, rcond=None)[0]
-            Q_inv_e = np.linalg.lstsq(Q_AA, ones_A, rcond=None)[0]
-        eQe = float(ones_A @ Q_inv_e)
-        eQh = float(ones_A @ Q_inv_h)
-        mu = (eQh - 1.0) / eQe if abs(eQe) > 1e-30 else 0.0
-        lam_A = Q_inv_h - mu * Q_inv_e
+        key = tuple(A)
+        if memo is not None and memo.get("key") == key:
+            lam_A, mu = memo["lam_A"], memo["mu"]
+        else:
+            ones_A = np.ones(k)
+            Q_AA = Q[np.ix_(A_arr, A_arr)]
+            Q_AA[np.diag_indices(k)] += reg       # = Q_AA + reg * I bit for bit (the entries are >= 0)
+            h_A = h[A_arr]
+            try:
+                cf = cho_factor(Q_AA, lower=True, check_finite=False)
+                sol = cho_solve(cf, np.column_stack([h_A, ones_A]), check_finite=False)
+                Q_inv_h, Q_inv_e = sol[:, 0], sol[:, 1]
+            except np.linalg.LinAlgError:
+                Q_inv_h = np.linalg.lstsq(Q_AA, h_A, rcond=None)[0]
+                Q_inv_e = np.linalg.lstsq(Q_AA, ones_A, rcond=None)[0]
+            eQe = float(ones_A @ Q_inv_e)
+            eQh = float(ones_A @ Q_inv_h)
+            mu = (eQh - 1.0) / eQe if abs(eQe) > 1e-30 else 0.0
+            lam_A = Q_inv_h - mu * Q_inv_e
+            if memo is not None:
+                memo.update(key=key, lam_A=lam_A, mu=mu)
         if k > 0 and float(lam_A.min()) < -tol:
             del A[int(np.argmin(lam_A))]
             continue
@@ -230,6 +241,7 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
         keys = [bytes(col0)]
     setup_s = time.perf_counter() - t_setup
     qp_s = price_s = 0.0
+    qp_memo = {}
     UB, rc_final, stop, margins, trace, picked = math.inf, math.nan, "max_iters", [], [], []
     t_total = time.perf_counter()
     it = 0
@@ -239,7 +251,7 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
             break
         t = time.perf_counter()
         Qv, hv = gram.view()
-        lam_new, A_warm = solve_qp_native(Qv, hv, A_init=A_warm)
+        lam_new, A_warm = solve_qp_native(Qv, hv, A_init=A_warm, memo=qp_memo)
         pout.apply_delta(lam_new - lam)
         lam = lam_new
         QL = Qv @ lam
