@@ -264,6 +264,31 @@ def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
         its.append(int(r.iterations))
     torch.cuda.synchronize()
     ts = time.perf_counter() - t0
+    # the screen of config 4's B = 10,000 draws (rows, perturbation, ||P_b - p_fit|| and ||p_b - p_hat||):
+    # on the GPU over all draws, and the host builder (the reference's block builder) on a sample
+    from rumb import _lib
+    from rumb.rum_solver import context
+    D = BS.Draws(panel, m, a, p, B=10000, weights="multinomial", seed=0)
+    r_n, eps_n, _ = BS.scaling(D.R)
+    fit = boot.session.fit
+    gd = _lib.DrawRows(context(), D.W, D.offered, D.chose, D.row_menu, D.p_hat)
+    gd.screen(fit, eps_n * r_n)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gd.screen(fit, eps_n * r_n)
+    torch.cuda.synchronize()
+    t_gpu = time.perf_counter() - t0
+    sample = 512
+    t0 = time.perf_counter()
+    for lo in range(0, sample, 256):
+        rows = D.rows(np.arange(lo, lo + 256))
+        P = BS.perturb(D.p_hat, rows, r_n, eps_n)
+        np.sqrt(np.einsum("ij,ij->i", P - fit, P - fit))
+        np.sqrt(np.einsum("ij,ij->i", rows - D.p_hat, rows - D.p_hat))
+    t_host = (time.perf_counter() - t0) * D.B / sample
+    gd.close()
+    screen = {"draws": D.B, "rows": D.M, "gpu_s": t_gpu, "host_s": t_host, "host_sample_draws": sample,
+              "host_threads": 1}
     line = {"metric": "n=20 bootstrap draws/s at abs gap 5e-4 (batched vs one at a time)",
             "value": batch_draws / tb, "unit": "draws/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic",
@@ -271,7 +296,8 @@ def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
                        "slots": boot.last_batch["slots"], "iters_batched": boot.iters[idx].tolist()},
             "one_at_a_time": {"value": single_draws / ts, "unit": "draws/s", "draws": single_draws,
                               "iters": its},
-            "ratio_batched_over_one_at_a_time": (batch_draws / tb) / (single_draws / ts)}
+            "ratio_batched_over_one_at_a_time": (batch_draws / tb) / (single_draws / ts),
+            "screen": screen}
     print(json.dumps(line), flush=True)
 
 

@@ -242,6 +242,34 @@ RUMB_API int rumb_cg_pricer_destroy(rumb_cg_pricer *pricer);
  * reference, which always scans.) */
 RUMB_API int rumb_cg_pricer_info(const rumb_cg_pricer *pricer, long long *list_entries, long long *list_bytes);
 
+/* ---------------------------------------------------------------- bootstrap draws
+ * Resampled shares of a respondent panel on the GPU (replaces the host block builder
+ * solver/inference/draws.py:273-285 and the screen solver/inference/bootstrap.py:290-306).
+ * B draws, each a row of R respondent weights W (row-major B x R; integer counts). Respondent r
+ * was offered menu u offered_count times and chose row j chose_count times, given as lists:
+ * offered_ptr[u]..offered_ptr[u+1] index (offered_resp, offered_count) for menu u (n_menus + 1
+ * offsets), chose_ptr[j]..chose_ptr[j+1] index (chose_resp, chose_count) for row j (M + 1
+ * offsets); row_menu[j] = row j's menu. Draw b's row j is chose / seen with
+ * seen = sum_r W[b, r] offered[r, row_menu[j]] and chose = sum_r W[b, r] chose[r, j], and p_hat[j]
+ * where seen <= 0 (bit for bit the host's values: the sums are exact). At most 20,480
+ * respondents. All arrays are host memory; create copies them to the context's GPU. */
+typedef struct rumb_draws rumb_draws;
+RUMB_API int rumb_draws_create(rumb_ctx *ctx, long long B, int R, long long M, int n_menus, const double *W,
+                               const int64_t *offered_ptr, const int32_t *offered_resp,
+                               const double *offered_count, const int64_t *chose_ptr, const int32_t *chose_resp,
+                               const double *chose_count, const int32_t *row_menu, const double *p_hat,
+                               rumb_draws **out);
+/* The draws idx[0..count) as rows of out (count x M, host): perturbed = 1 gives
+ * p_hat + scale (p_b - p_hat) (the Hong-Li perturbation, scale = eps_n r_n), 0 the shares p_b. */
+RUMB_API int rumb_draws_rows(rumb_draws *draws, const int64_t *idx, long long count, int perturbed, double scale,
+                             double *out);
+/* The screen over all B draws: dev[b] = ||p_b - p_hat|| and, with fit (M values, a RUM point),
+ * ub[b] = ||p_hat + scale (p_b - p_hat) - fit||, an upper bound of draw b's distance. dev or ub
+ * may be NULL; ub needs fit. The norms are float64 sums in a fixed order (equal to a host sum
+ * to rounding). */
+RUMB_API int rumb_draws_screen(rumb_draws *draws, const double *fit, double scale, double *dev, double *ub);
+RUMB_API int rumb_draws_destroy(rumb_draws *draws);
+
 /* ---------------------------------------------------------------- profiling */
 typedef struct {
     char name[64];            /* kernel and launch shape */

@@ -7,6 +7,7 @@
 
 #include "bm.cuh"
 #include "ctx.cuh"
+#include "draws.cuh"
 #include "mlp.cuh"
 #include "pricer.cuh"
 
@@ -274,6 +275,61 @@ int rumb_cg_pricer_destroy(rumb_cg_pricer *pr) {
         rumb::pricer_destroy(pr->p);
     }
     delete pr;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+// ---------------------------------------------------------------- bootstrap draws
+int rumb_draws_create(rumb_ctx *ctx, long long B, int R, long long M, int n_menus, const double *W,
+                      const int64_t *offered_ptr, const int32_t *offered_resp, const double *offered_count,
+                      const int64_t *chose_ptr, const int32_t *chose_resp, const double *chose_count,
+                      const int32_t *row_menu, const double *p_hat, rumb_draws **out) {
+    RUMB_API_BEGIN
+    NEED_CTX(ctx);
+    if (!out) rumb::fail(RUMB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    ctx->c.join_in();
+    rumb_draws *h = new rumb_draws();
+    try {
+        h->d = rumb::draws_create(ctx->c, B, R, M, n_menus, W, offered_ptr, offered_resp, offered_count, chose_ptr,
+                                  chose_resp, chose_count, row_menu, p_hat);
+    } catch (...) {
+        delete h;
+        throw;
+    }
+    h->device = ctx->c.device;
+    ctx->c.join_out();
+    *out = h;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_draws_rows(rumb_draws *d, const int64_t *idx, long long count, int perturbed, double scale, double *out) {
+    RUMB_API_BEGIN
+    if (!d || !d->d) rumb::fail(RUMB_E_INVAL, "draws is NULL");
+    rumb::DeviceGuard dg(d->device);
+    rumb::draws_rows(d->d, idx, count, perturbed, scale, out);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_draws_screen(rumb_draws *d, const double *fit, double scale, double *dev, double *ub) {
+    RUMB_API_BEGIN
+    if (!d || !d->d) rumb::fail(RUMB_E_INVAL, "draws is NULL");
+    rumb::DeviceGuard dg(d->device);
+    rumb::draws_screen(d->d, fit, scale, dev, ub);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_draws_destroy(rumb_draws *d) {
+    RUMB_API_BEGIN
+    if (!d) return RUMB_OK;
+    {
+        rumb::DeviceGuard dg(d->device);
+        rumb::draws_destroy(d->d);
+    }
+    delete d;
     return RUMB_OK;
     RUMB_API_END
 }

@@ -113,6 +113,11 @@ _SIGS = {
     "rumb_cg_price": ([_vp, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _vp,
                        ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
     "rumb_cg_pricer_destroy": ([_vp], ctypes.c_int),
+    "rumb_draws_create": ([_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, _vp, _vp, _vp, _vp,
+                           _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)], ctypes.c_int),
+    "rumb_draws_rows": ([_vp, _vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),
+    "rumb_draws_screen": ([_vp, _vp, ctypes.c_double, _vp, _vp], ctypes.c_int),
+    "rumb_draws_destroy": ([_vp], ctypes.c_int),
     "rumb_cg_pricer_info": ([_vp, _vp, _vp], ctypes.c_int),
     "rumb_bm_iterate": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, _vp, _vp, _vp,
                          ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -429,6 +434,59 @@ class MLP:
         check(load().rumb_mlp_train(self.h, _p(X), _p(T), X.shape[0], int(epochs), int(batch), float(lr), int(seed),
                                     ctypes.byref(loss)))
         return loss.value
+
+
+class DrawRows:
+    """Bootstrap draws on one GPU (see rumb_draws_create): W is B x R respondent weights; offered
+    and chose are the panel's (respondent x menu) and (respondent x row) count matrices (scipy
+    sparse); row_menu maps rows to menus."""
+
+    def __init__(self, ctx, W, offered, chose, row_menu, p_hat):
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        B, R = W.shape
+        oT = offered.T.tocsr()
+        cT = chose.T.tocsr()
+        optr = np.ascontiguousarray(oT.indptr, dtype=np.int64)
+        oresp = np.ascontiguousarray(oT.indices, dtype=np.int32)
+        ocnt = np.ascontiguousarray(oT.data, dtype=np.float64)
+        cptr = np.ascontiguousarray(cT.indptr, dtype=np.int64)
+        cresp = np.ascontiguousarray(cT.indices, dtype=np.int32)
+        ccnt = np.ascontiguousarray(cT.data, dtype=np.float64)
+        row_menu = np.ascontiguousarray(row_menu, dtype=np.int32)
+        p_hat = np.ascontiguousarray(p_hat, dtype=np.float64)
+        self.B, self.R, self.M = int(B), int(R), int(p_hat.size)
+        h = ctypes.c_void_p()
+        check(load().rumb_draws_create(ctx.h, self.B, self.R, self.M, int(oT.shape[0]), _p(W), _p(optr), _p(oresp),
+                                       _p(ocnt), _p(cptr), _p(cresp), _p(ccnt), _p(row_menu), _p(p_hat),
+                                       ctypes.byref(h)))
+        self.h, self.ctx = h, ctx
+
+    def rows(self, idx, scale=None):
+        """Draws idx as rows (len(idx) x M): the shares, or with scale p_hat + scale (p_b - p_hat)."""
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        out = np.empty((idx.size, self.M))
+        check(load().rumb_draws_rows(self.h, _p(idx), idx.size, 0 if scale is None else 1,
+                                     0.0 if scale is None else float(scale), _p(out)))
+        return out
+
+    def screen(self, fit, scale):
+        """(dev, ub) over all draws: ||p_b - p_hat|| and ||p_hat + scale (p_b - p_hat) - fit||."""
+        dev, ub = np.empty(self.B), np.empty(self.B)
+        f = None if fit is None else np.ascontiguousarray(fit, dtype=np.float64)
+        check(load().rumb_draws_screen(self.h, None if f is None else _p(f), float(scale), _p(dev),
+                                       None if f is None else _p(ub)))
+        return dev, (ub if f is not None else None)
+
+    def close(self):
+        if self.h:
+            load().rumb_draws_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Pricer:

@@ -266,12 +266,22 @@ class Bootstrap:
         self.L0, self.U0 = r.lb, r.ub
         self.time["certificate"] += time.perf_counter() - t0
 
+    def _draw_rows(self):
+        """The draws on the GPU (built on first use): rows and the screen's norms."""
+        if getattr(self, "_gdraws", None) is None:
+            from . import _lib
+            from .rum_solver import context
+            d = self.draws
+            self._gdraws = _lib.DrawRows(context(), d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+        return self._gdraws
+
     def _screen(self):
+        """dev_b = ||p_b - p_hat|| and U_b = min(U_b, ||perturb(p_b) - p_fit||) for every draw, on the
+        GPU (the rows are the host's bit for bit; the norms agree to rounding)."""
         t0, fit = time.perf_counter(), self.session.fit
-        for lo in range(0, self.B, 256):
-            idx = np.arange(lo, min(self.B, lo + 256))
-            P = perturb(self.p_hat, self.draws.rows(idx), self.r_n, self.eps_n)
-            self.U[idx] = np.minimum(self.U[idx], np.sqrt(np.einsum("ij,ij->i", P - fit, P - fit)))
+        self.dev, ub = self._draw_rows().screen(fit, self.eps_n * self.r_n)
+        if ub is not None:
+            self.U = np.minimum(self.U, ub)
         self.n_screened = int((self.U < self.tau[0]).sum())
         self.screened = True
         self.time["screen"] += time.perf_counter() - t0
@@ -337,7 +347,7 @@ class Bootstrap:
         if idx.size == 0:
             return
         tau_lo, tau_hi = self.tau
-        P = perturb(self.p_hat, self.draws.rows(idx), self.r_n, self.eps_n)
+        P = self._draw_rows().rows(idx, self.eps_n * self.r_n)       # = perturb(p_hat, draws.rows(idx), ...)
         rum, s = self.rum, self.session
         if s.method == "bm_admm" and rum.n >= 8 and rum._single.size == 0:
             from .rum_solver import context
