@@ -242,6 +242,30 @@ RUMB_API int rumb_cg_pricer_destroy(rumb_cg_pricer *pricer);
  * reference, which always scans.) */
 RUMB_API int rumb_cg_pricer_info(const rumb_cg_pricer *pricer, long long *list_entries, long long *list_bytes);
 
+/* The CG master's column bookkeeping on the pricer's GPU (replaces the host maintainers
+ * solver/flow_cg/qp_bitset_incremental.py:36-141 and the column builder
+ * solver/flow_cg/cg_core.py:63-80; the QP stays with the caller). alts[mp] = each row's
+ * alternative and p_obs[mp] = its observed share, in the pricer's x-major row order; up to
+ * max_cols columns. Columns are packed bits (W = ceil(mp / 64) words, bit s = row s). */
+typedef struct rumb_cg_master rumb_cg_master;
+RUMB_API int rumb_cg_master_create(rumb_cg_pricer *pricer, const int32_t *alts, const double *p_obs, int max_cols,
+                                   rumb_cg_master **out);
+/* Append a column: the column of the ranking rank_pos[n] (row s is 1 when its alternative is
+ * the best-ranked member of its menu), or the packed column bits_in (exactly one of the two).
+ * bits_out (W words, may be NULL) receives the column; gram_row (k + 1 values, may be NULL) the
+ * new column's Gram entries Q[k][0..k] (popcounts; k = the new column's index). *index = k. */
+RUMB_API int rumb_cg_master_add_column(rumb_cg_master *master, const int32_t *rank_pos, const uint64_t *bits_in,
+                                       uint64_t *bits_out, double *gram_row, int *index);
+/* p_out += sum_t delta[t] V[:, cols[t]] with cols increasing, each row adding in that order (the
+ * host maintainer's float64 sums, bit for bit), then the residual p_obs - p_out as float32 for the
+ * next pricing. */
+RUMB_API int rumb_cg_master_apply(rumb_cg_master *master, const int32_t *cols, const double *delta, int count);
+/* Price the current residual with the master's pricer (rumb_cg_price's outputs). */
+RUMB_API int rumb_cg_master_price(rumb_cg_master *master, double *vmax, int32_t *rank_pos, double *margin);
+/* p_out[mp] to host memory. */
+RUMB_API int rumb_cg_master_p_out(rumb_cg_master *master, double *out);
+RUMB_API int rumb_cg_master_destroy(rumb_cg_master *master);
+
 /* ---------------------------------------------------------------- bootstrap draws
  * Resampled shares of a respondent panel on the GPU (replaces the host block builder
  * solver/inference/draws.py:273-285 and the screen solver/inference/bootstrap.py:290-306).

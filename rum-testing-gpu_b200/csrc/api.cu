@@ -6,6 +6,7 @@
 #include <new>
 
 #include "bm.cuh"
+#include "cgmaster.cuh"
 #include "ctx.cuh"
 #include "draws.cuh"
 #include "mlp.cuh"
@@ -275,6 +276,79 @@ int rumb_cg_pricer_destroy(rumb_cg_pricer *pr) {
         rumb::pricer_destroy(pr->p);
     }
     delete pr;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+// ---------------------------------------------------------------- CG master
+#define NEED_MASTER(h)                                                 \
+    if (!(h) || !(h)->m) rumb::fail(RUMB_E_INVAL, "master is NULL");  \
+    rumb::DeviceGuard _dg((h)->device)
+
+int rumb_cg_master_create(rumb_cg_pricer *pr, const int32_t *alts, const double *p_obs, int max_cols,
+                          rumb_cg_master **out) {
+    RUMB_API_BEGIN
+    if (!pr || !pr->p) rumb::fail(RUMB_E_INVAL, "pricer is NULL");
+    if (!out) rumb::fail(RUMB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    rumb::DeviceGuard dg(pr->device);
+    rumb_cg_master *h = new rumb_cg_master();
+    try {
+        h->m = rumb::cgmaster_create(pr->p, alts, p_obs, max_cols);
+    } catch (...) {
+        delete h;
+        throw;
+    }
+    h->device = pr->device;
+    *out = h;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_master_add_column(rumb_cg_master *h, const int32_t *rank_pos, const uint64_t *bits_in, uint64_t *bits_out,
+                              double *gram_row, int *index) {
+    RUMB_API_BEGIN
+    NEED_MASTER(h);
+    int k = rumb::cgmaster_add_column(h->m, rank_pos, bits_in, bits_out, gram_row);
+    if (index) *index = k;
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_master_apply(rumb_cg_master *h, const int32_t *cols, const double *delta, int count) {
+    RUMB_API_BEGIN
+    NEED_MASTER(h);
+    rumb::cgmaster_apply(h->m, cols, delta, count);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_master_price(rumb_cg_master *h, double *vmax, int32_t *rank_pos, double *margin) {
+    RUMB_API_BEGIN
+    NEED_MASTER(h);
+    if (!vmax || !rank_pos || !margin) rumb::fail(RUMB_E_INVAL, "NULL output");
+    rumb::cgmaster_price(h->m, vmax, rank_pos, margin);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_master_p_out(rumb_cg_master *h, double *out) {
+    RUMB_API_BEGIN
+    NEED_MASTER(h);
+    if (!out) rumb::fail(RUMB_E_INVAL, "out is NULL");
+    rumb::cgmaster_p_out(h->m, out);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
+int rumb_cg_master_destroy(rumb_cg_master *h) {
+    RUMB_API_BEGIN
+    if (!h) return RUMB_OK;
+    {
+        rumb::DeviceGuard dg(h->device);
+        rumb::cgmaster_destroy(h->m);
+    }
+    delete h;
     return RUMB_OK;
     RUMB_API_END
 }

@@ -667,6 +667,10 @@ void pricer_info(const Pricer *P, long long *list_entries, long long *list_bytes
 void pricer_destroy(Pricer *P) { delete P; }
 
 int pricer_device(const Pricer *P) { return P->c->device; }
+Ctx &pricer_ctx(const Pricer *P) { return *P->c; }
+int pricer_n(const Pricer *P) { return P->n; }
+ll pricer_rows(const Pricer *P) { return P->mp; }
+const ull *pricer_menus(const Pricer *P) { return P->menus.as<ull>(); }
 
 // One sweep over the lattice on the context's stream, ending with the backtrace (stream storage)
 // or the readout (mask storage) into P->out.

@@ -113,6 +113,13 @@ _SIGS = {
     "rumb_cg_price": ([_vp, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _vp,
                        ctypes.POINTER(ctypes.c_double), _vp], ctypes.c_int),
     "rumb_cg_pricer_destroy": ([_vp], ctypes.c_int),
+    "rumb_cg_master_create": ([_vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "rumb_cg_master_add_column": ([_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "rumb_cg_master_apply": ([_vp, _vp, _vp, ctypes.c_int], ctypes.c_int),
+    "rumb_cg_master_price": ([_vp, ctypes.POINTER(ctypes.c_double), _vp, ctypes.POINTER(ctypes.c_double)],
+                             ctypes.c_int),
+    "rumb_cg_master_p_out": ([_vp, _vp], ctypes.c_int),
+    "rumb_cg_master_destroy": ([_vp], ctypes.c_int),
     "rumb_draws_create": ([_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, _vp, _vp, _vp, _vp,
                            _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)], ctypes.c_int),
     "rumb_draws_rows": ([_vp, _vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),
@@ -434,6 +441,57 @@ class MLP:
         check(load().rumb_mlp_train(self.h, _p(X), _p(T), X.shape[0], int(epochs), int(batch), float(lr), int(seed),
                                     ctypes.byref(loss)))
         return loss.value
+
+
+class CgMaster:
+    """The CG master's column bookkeeping on a pricer's GPU (see rumb_cg_master_create)."""
+
+    def __init__(self, pricer, alts, p_obs, max_cols):
+        alts = np.ascontiguousarray(alts, dtype=np.int32)
+        p_obs = np.ascontiguousarray(p_obs, dtype=np.float64)
+        self.M, self.n, self.W = int(p_obs.size), pricer.n, (int(p_obs.size) + 63) // 64
+        h = ctypes.c_void_p()
+        check(load().rumb_cg_master_create(pricer.h, _p(alts), _p(p_obs), int(max_cols), ctypes.byref(h)))
+        self.h, self.pricer, self.K = h, pricer, 0
+
+    def add_column(self, rank_pos=None, bits=None):
+        """(index, packed column bits uint64[W], Gram row float64[index + 1])."""
+        out = np.empty(self.W, dtype=np.uint64)
+        row = np.empty(self.K + 1)
+        k = ctypes.c_int()
+        rp = None if rank_pos is None else np.ascontiguousarray(rank_pos, dtype=np.int32)
+        b = None if bits is None else np.ascontiguousarray(bits, dtype=np.uint64)
+        check(load().rumb_cg_master_add_column(self.h, None if rp is None else _p(rp), None if b is None else _p(b),
+                                               _p(out), _p(row), ctypes.byref(k)))
+        self.K += 1
+        return k.value, out, row
+
+    def apply(self, cols, delta):
+        cols = np.ascontiguousarray(cols, dtype=np.int32)
+        delta = np.ascontiguousarray(delta, dtype=np.float64)
+        check(load().rumb_cg_master_apply(self.h, _p(cols), _p(delta), int(cols.size)))
+
+    def price(self):
+        vmax, margin = ctypes.c_double(), ctypes.c_double()
+        rank = np.zeros(self.n, dtype=np.int32)
+        check(load().rumb_cg_master_price(self.h, ctypes.byref(vmax), _p(rank), ctypes.byref(margin)))
+        return vmax.value, rank, margin.value
+
+    def p_out(self):
+        out = np.empty(self.M)
+        check(load().rumb_cg_master_p_out(self.h, _p(out)))
+        return out
+
+    def close(self):
+        if self.h:
+            load().rumb_cg_master_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class DrawRows:

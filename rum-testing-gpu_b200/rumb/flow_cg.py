@@ -114,6 +114,80 @@ class PoutMaintainer:
             np.add.at(self.p_out, self.pos[int(a)], float(delta[a]))
 
 
+class _HostMaster:
+    """Column bookkeeping on the host (the reference's maintainers): for pricers that are not the
+    library's (scripted pricers in tests)."""
+
+    def __init__(self, prob, p_obs, max_K):
+        self.prob, self.p_obs = prob, p_obs
+        self.gram = GramMaintainer(p_obs.size, p_obs, max_K)
+        self.pout = PoutMaintainer(p_obs.size)
+
+    def add_ranking(self, rank_pos):
+        return self.add_col(ranking_column(self.prob.menus, self.prob.alts, rank_pos, self.prob.n))
+
+    def add_col(self, col):
+        self.gram.add_column(col.astype(np.float64))
+        self.pout.add_column(col)
+        return col
+
+    def view(self):
+        return self.gram.view()
+
+    def apply_delta(self, delta):
+        self.pout.apply_delta(delta)
+
+    def price(self):
+        return self.prob.pricer.price((self.p_obs - self.pout.p_out).astype(np.float32))
+
+    def p_out(self):
+        return self.pout.p_out.copy()
+
+
+class _DeviceMaster:
+    """Column bookkeeping on the pricer's GPU (rumb_cg_master_*): the column of a ranking, its Gram
+    row, p_out and the float32 residual stay on the device, bit for bit the host maintainers'
+    values; Q and h = V'p_obs (numpy's sum, as the reference) are kept here for the QP."""
+
+    def __init__(self, prob, p_obs, max_K):
+        from . import _lib
+        self.dev = _lib.CgMaster(prob.pricer, prob.alts, p_obs, max_K)
+        self.gram = GramMaintainer(p_obs.size, p_obs, max_K)
+        self.M = p_obs.size
+
+    def _store(self, k, bits, row):
+        g = self.gram
+        if k >= g.cap:
+            g._grow(min(g.max_K, 2 * g.cap))
+        col = np.unpackbits(bits.view(np.uint8), bitorder="little")[:self.M]
+        g.bits[k] = bits
+        g.Q[k, :k] = row[:k]
+        g.Q[:k, k] = row[:k]
+        g.Q[k, k] = row[k]
+        g.h[k] = float(g.phat[np.where(col > 0.5)[0]].sum())
+        g.K = k + 1
+        return col
+
+    def add_ranking(self, rank_pos):
+        return self._store(*self.dev.add_column(rank_pos=rank_pos))
+
+    def add_col(self, col):
+        return self._store(*self.dev.add_column(bits=_pack(col)))
+
+    def view(self):
+        return self.gram.view()
+
+    def apply_delta(self, delta):
+        a = np.where(np.abs(delta) > 1e-12)[0]
+        self.dev.apply(a, delta[a])
+
+    def price(self):
+        return self.dev.price()
+
+    def p_out(self):
+        return self.dev.p_out()
+
+
 def project_simplex(y):
     n = y.size
     u = np.sort(y)[::-1]
@@ -217,27 +291,25 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
     p_sq = float(p_obs @ p_obs)
     lb_best, gap_rel = 0.0, math.inf
     n_init = len(init_columns) if init_columns is not None else 0
-    gram = GramMaintainer(M, p_obs, max_K=max_iters + 2 + n_init)
-    pout = PoutMaintainer(M)
+    from . import _lib
+    master = (_DeviceMaster if isinstance(prob.pricer, _lib.Pricer) else _HostMaster)(prob, p_obs,
+                                                                                      max_iters + 2 + n_init)
     if n_init:
         cols = [np.ascontiguousarray(np.asarray(c, dtype=np.uint8)) for c in init_columns]
         for c in cols:
-            gram.add_column(c.astype(np.float64))
-            pout.add_column(c)
+            master.add_col(c)
         K = n_init
         lam = (np.asarray(init_lambda, dtype=np.float64).copy() if init_lambda is not None else np.full(K, 1.0 / K))
         lam = np.maximum(lam, 0.0)
         lam /= lam.sum()
-        pout.apply_delta(lam)
+        master.apply_delta(lam)
         A_warm = [int(i) for i in np.where(lam > 1e-12)[0]] or [0]
         keys = [bytes(c) for c in cols]
     else:
         perm0 = np.random.RandomState(seed).permutation(n)
-        col0 = ranking_column(prob.menus, prob.alts, perm0, n)
-        gram.add_column(col0.astype(np.float64))
-        pout.add_column(col0)
+        col0 = master.add_ranking(perm0)
         K, lam, A_warm = 1, np.array([1.0]), [0]
-        pout.apply_delta(np.array([1.0]))
+        master.apply_delta(np.array([1.0]))
         keys = [bytes(col0)]
     setup_s = time.perf_counter() - t_setup
     qp_s = price_s = 0.0
@@ -250,9 +322,9 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
             stop = "time_limit"
             break
         t = time.perf_counter()
-        Qv, hv = gram.view()
+        Qv, hv = master.view()
         lam_new, A_warm = solve_qp_native(Qv, hv, A_init=A_warm, memo=qp_memo)
-        pout.apply_delta(lam_new - lam)
+        master.apply_delta(lam_new - lam)
         lam = lam_new
         QL = Qv @ lam
         lql = float(lam @ QL)
@@ -265,9 +337,8 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
                 stop = "phi_ub"
                 break
         qp_s += time.perf_counter() - t
-        residual = p_obs - pout.p_out
         t = time.perf_counter()
-        vmax, rank_pos, margin = prob.pricer.price(residual.astype(np.float32))
+        vmax, rank_pos, margin = master.price()      # the float32 residual p_obs - p_out
         price_s += time.perf_counter() - t
         margins.append(margin)
         if record_columns:
@@ -293,15 +364,13 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
         if fw_gap < rc_tol:
             stop = "rc"
             break
-        col = ranking_column(prob.menus, prob.alts, rank_pos, n)
+        col = master.add_ranking(rank_pos)
         keys.append(bytes(col))
-        gram.add_column(col.astype(np.float64))
-        pout.add_column(col)
         K += 1
         lam = np.concatenate([lam, [0.0]])
     wall_s = time.perf_counter() - t_total
     return dict(wall_s=wall_s, setup_s=setup_s, trace=trace, margins=margins, iters=it, n_cols=K, lam=lam,
-                p_out=pout.p_out.copy(), columns=[np.frombuffer(k, dtype=np.uint8).copy() for k in keys],
+                p_out=master.p_out(), columns=[np.frombuffer(k, dtype=np.uint8).copy() for k in keys],
                 rc_final=rc_final, distance=UB, lb=lb_best, gap_rel=gap_rel, stop_reason=stop, qp_s=qp_s,
                 price_s=price_s, picked=picked)
 

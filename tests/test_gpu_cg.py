@@ -132,6 +132,44 @@ def test_cg_trajectory_matches_oracle(ctx, mode):
     assert mine["distance"] == ref["ub"] and mine["lb"] == ref["lb"]
 
 
+@pytest.mark.parametrize("mode", ["mask", "u24"])
+def test_device_master_equals_host_master(ctx, mode):
+    """The column bookkeeping on the GPU (rumb_cg_master_*) and the reference's host maintainers give
+    the same run bit for bit: every column, lambda, p_out and the bounds (n = 14, warm restart too)."""
+    from rumb import flow_cg
+    cd, mp = PI.gen_medium(14, mult=3)
+    n = 14
+
+    class HostPricer:                      # not a _lib.Pricer: the loop keeps its books on the host
+        def __init__(self, inner):
+            self.inner = inner
+
+        def price(self, s):
+            return self.inner.price(s)
+
+    prob = flow_cg.CGProblem(ctx, n, cd[:, 0], cd[:, 1], mode)
+    dev = flow_cg.solve_cg(prob, cd[:, 2], max_iters=150, gap_abs_tol=1e-7, record_columns=True)
+    inner = prob.pricer
+    prob.pricer = HostPricer(inner)
+    host = flow_cg.solve_cg(prob, cd[:, 2], max_iters=150, gap_abs_tol=1e-7, record_columns=True)
+    assert dev["n_cols"] == host["n_cols"] and len(dev["picked"]) == len(host["picked"])
+    for a, b in zip(dev["picked"], host["picked"]):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(dev["columns"], host["columns"]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(dev["lam"], host["lam"])
+    np.testing.assert_array_equal(dev["p_out"], host["p_out"])
+    assert dev["distance"] == host["distance"] and dev["lb"] == host["lb"]
+    # a warm restart from the kept columns
+    prob.pricer = inner
+    kw = dict(init_columns=dev["columns"], init_lambda=dev["lam"], max_iters=20, gap_abs_tol=1e-9)
+    dev2 = flow_cg.solve_cg(prob, cd[:, 2], **kw)
+    prob.pricer = HostPricer(inner)
+    host2 = flow_cg.solve_cg(prob, cd[:, 2], **kw)
+    np.testing.assert_array_equal(dev2["p_out"], host2["p_out"])
+    np.testing.assert_array_equal(dev2["lam"], host2["lam"])
+
+
 def test_cg_columns_on_config3_residuals(ctx):
     """n = 18, 0.5 % density: the GPU loop's residual scores at several iterations, priced again by
     the oracle, give the same columns."""
