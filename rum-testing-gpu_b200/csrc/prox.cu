@@ -11,7 +11,10 @@
 // Staging two arrays instead of three (x and x2 read through registers into the relaxed point xo,
 // plus one bit per element for x2 > 0; 7 CTAs per SM instead of 5 in float64) measured 45.6
 // against 47.2 us in float64 and 34.7 against 32.4 us in float32: more resident CTAs barely help,
-// the per-menu dependent work is what bounds the kernel.
+// the per-menu dependent work is what bounds the kernel. Running the elementwise parts (the
+// relaxed point, v, q, the threshold value; u and z') element by element over the tile, with one
+// thread per menu for the threshold alone and the stores fused into the second pass, measured
+// 51.5 against 47.3 us in float64 and 36.7 against 32.2 us in float32.
 #include "prox.cuh"
 
 namespace rumb {
