@@ -166,7 +166,8 @@ __device__ __forceinline__ float w_of(const PricerArgs &A, int x, ull D, bool in
 
 // One popcount layer k of the sweep.
 //
-// layer_eval_kernel: a CTA of 1024 threads covers PE_R = 128 consecutive ranks with PE_G = 8
+// layer_eval_kernel: a CTA of 1024 threads covers PE_R = 128 consecutive ranks (32 ranks and 256
+// threads for the layers too small to give every SM two such CTAs) with PE_G = 8
 // groups of alternatives (warp w: ranks 32 (w mod 4) .., group w / 4 = the x with x mod 8 equal to
 // it), so a layer of C ranks spreads over C / 128 CTAs. Each thread walks its group's x from high
 // to low, keeps the candidate with `>=` (ties -> lowest x); the eight group winners of a rank are
@@ -182,17 +183,20 @@ __device__ __forceinline__ float w_of(const PricerArgs &A, int x, ull D, bool in
 // block min / max, step, rintf quantization of every value (u16 / u24 modes).
 constexpr int PE_R = 128, PE_G = 8;
 static_assert((PE_R / 32) * PE_G == 32 && (PE_G & (PE_G - 1)) == 0, "32 warps; PE_G a power of two");
+// Layers whose 128-rank CTAs would not give every SM two of them run 32 ranks per CTA (8 warps).
+constexpr int PE_R_SMALL = 32;
 
-template <bool MASK>
-__global__ void __launch_bounds__(1024) layer_eval_kernel(PricerArgs A, float *vals) {
-    __shared__ float pbest[PE_G][PE_R];
-    __shared__ signed char pbx[PE_G][PE_R];
+template <bool MASK, int PR>
+__global__ void __launch_bounds__(PR * PE_G) layer_eval_kernel(PricerArgs A, float *vals) {
+    static_assert(PR % 32 == 0 && (PR / 32) * PE_G <= 32, "at most 32 warps");
+    __shared__ float pbest[PE_G][PR];
+    __shared__ signed char pbx[PE_G][PR];
     __shared__ ull sbin[MASK ? 1 : BIN_MAX];
     const int n = A.n, k = A.k;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rg = w % (PE_R / 32), xg = w / (PE_R / 32);
+    const int rg = w % (PR / 32), xg = w / (PR / 32);
     const int loc = rg * 32 + lane;
-    const ull r = (ull)blockIdx.x * PE_R + loc;
+    const ull r = (ull)blockIdx.x * PR + loc;
     const bool valid = r < A.count;
     if (!MASK) {
         stage_binom(sbin, A.binom, n);
@@ -682,8 +686,16 @@ static void run_sweep(Pricer *P, const float *scores) {
     const ll *offs = P->offsets.as<ll>();
     auto layer = [&](PricerArgs &A, bool mask, float *vals) {
         auto thread_kernel = [&]() {
-            if (mask) layer_eval_kernel<true><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, vals);
-            else layer_eval_kernel<false><<<(unsigned)((A.count + PE_R - 1) / PE_R), 1024, 0, st>>>(A, vals);
+            if ((long long)A.count < 2LL * num_sms(c.device) * PE_R) {
+                constexpr int PR = PE_R_SMALL;
+                const unsigned grid = (unsigned)((A.count + PR - 1) / PR);
+                if (mask) layer_eval_kernel<true, PR><<<grid, PR * PE_G, 0, st>>>(A, vals);
+                else layer_eval_kernel<false, PR><<<grid, PR * PE_G, 0, st>>>(A, vals);
+            } else {
+                const unsigned grid = (unsigned)((A.count + PE_R - 1) / PE_R);
+                if (mask) layer_eval_kernel<true, PE_R><<<grid, PE_R * PE_G, 0, st>>>(A, vals);
+                else layer_eval_kernel<false, PE_R><<<grid, PE_R * PE_G, 0, st>>>(A, vals);
+            }
             RUMB_LAUNCH("layer_eval_kernel");
         };
         auto wide_kernel = [&]() {
