@@ -125,6 +125,79 @@ def test_gram_and_pout_maintainers():
     np.testing.assert_allclose(po.p_out, V @ lam, atol=1e-14)
 
 
+def test_gram_maintainer_growth():
+    """Q and h stay V'V and V'p_hat while the storage doubles (256 -> 512 columns)."""
+    rng = np.random.default_rng(4)
+    M = 200
+    ph = rng.random(M)
+    g = flow_cg.GramMaintainer(M, ph, max_K=600)
+    cols = [(rng.random(M) < 0.3).astype(np.uint8) for _ in range(300)]
+    for c in cols:
+        g.add_column(c.astype(np.float64))
+    V = np.stack(cols, axis=1).astype(np.float64)
+    Q, h = g.view()
+    assert g.cap == 512
+    np.testing.assert_array_equal(Q, V.T @ V)
+    np.testing.assert_allclose(h, V.T @ ph, rtol=1e-13)
+
+
+def test_qp_memo_is_bit_identical():
+    """The master's reuse of the previous call's last active-set solve changes no bit of lambda or
+    the support over a CG-like sequence of growing Gram matrices."""
+    rng = np.random.default_rng(5)
+    M, K = 400, 120
+    ph = rng.dirichlet(np.ones(M)) * 30
+    g = flow_cg.GramMaintainer(M, ph, max_K=K)
+    A_plain = A_memo = [0]
+    memo = {}
+    hits = 0
+    for k in range(K):
+        g.add_column((rng.random(M) < 0.35).astype(np.float64))
+        Q, h = g.view()
+        hits += memo.get("key") == tuple(A_memo)
+        lam1, A_plain = flow_cg.solve_qp_native(Q, h, A_init=A_plain)
+        lam2, A_memo = flow_cg.solve_qp_native(Q, h, A_init=A_memo, memo=memo)
+        np.testing.assert_array_equal(lam1, lam2)
+        assert A_plain == A_memo
+    assert hits > K // 2
+
+
+def test_cg_loop_matches_oracle_with_a_scripted_pricer():
+    """The host CG loop (with its master pieces and the QP memo) and the oracle's CG loop, driven by
+    the same scripted pricer, take the same columns and reach the same bounds bit for bit."""
+    import oracle as O
+    n = 9
+    m, a, p = mixture_instance(n, 0.5, K=8, N=60, seed=3)
+
+    def scripted(scores, menus, alts):
+        s = np.bincount(alts, weights=scores.astype(np.float64), minlength=n)
+        order = np.argsort(-s, kind="stable")
+        rank = np.empty(n, dtype=np.int32)
+        rank[order] = np.arange(n, dtype=np.int32)
+        col = O.ranking_column(n, menus, alts, rank)
+        return float(scores.astype(np.float64)[col > 0].sum()), rank, 0.0
+
+    class Prob:
+        pass
+
+    prob = Prob()
+    prob.n = n
+    prob.menus, prob.alts, _, _, prob.perm = flow_cg.prepare_choice_data(m, a, p, n)
+
+    class Pricer:
+        def price(self, scores):
+            return scripted(scores, prob.menus, prob.alts)
+
+    prob.pricer = Pricer()
+    mine = flow_cg.solve_cg(prob, p, max_iters=60, gap_abs_tol=1e-9, record_columns=True)
+    ref = O.cg_solve(n, m, a, p, max_iters=60, gap_abs_tol=1e-9,
+                     pricer=lambda sc: scripted(sc, prob.menus, prob.alts))
+    assert len(mine["picked"]) == len(ref["columns"])
+    for x, y in zip(mine["picked"], ref["columns"]):
+        np.testing.assert_array_equal(x, y)
+    assert mine["distance"] == ref["ub"] and mine["lb"] == ref["lb"]
+
+
 def test_generators_shapes_and_determinism():
     n, m, a, p = config_instance("n10_all_k20")
     assert np.unique(m).size == 1013 and m.size == 5110
