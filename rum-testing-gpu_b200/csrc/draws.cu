@@ -175,11 +175,9 @@ static void launch(const Draws &D, ll count, const ll *idx, int perturbed, doubl
                    double *rows, double *dev, double *ub) {
     cudaStream_t st = D.c->own;
     const size_t smem = (size_t)D.R * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        RUMB_CUDA(cudaFuncSetAttribute(draw_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-        attr = true;
-    }
+    // the opt-in above 48 KB is a per-device attribute: set it on the draws' device when it is needed
+    if (smem > 48 * 1024)
+        RUMB_CUDA(cudaFuncSetAttribute(draw_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (ll lo = 0; lo < count; lo += 65535) {
         const ll nb = std::min<ll>(65535, count - lo);
         draw_rows_kernel<<<(unsigned)nb, DR_THREADS, smem, st>>>(args_of(D), idx ? idx + lo : nullptr, perturbed, scale,
