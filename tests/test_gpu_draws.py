@@ -15,6 +15,8 @@ def _cases():
     panel, (m, a, p) = panel_instance(10, 0.3, 80, 8, 5, seed=7)
     yield "n10_panel80", panel, m, a, p, 40, "multinomial"
     yield "n10_panel80_reject", panel, m, a, p, 40, "multinomial_reject"
+    panel, (m, a, p) = panel_instance(10, 0.3, 7000, 8, 5, seed=8)       # weights above 48 KB of shared memory
+    yield "n10_panel7000", panel, m, a, p, 16, "multinomial"
     n, m, a, p, panel = config_instance("n20_d1pct_panel520")
     yield "n20_d1pct_panel520", panel, m, a, p, 48, "multinomial"
 
