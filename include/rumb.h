@@ -241,6 +241,11 @@ RUMB_API int rumb_cg_pricer_destroy(rumb_cg_pricer *pricer);
  * their device bytes with the offsets. Either pointer may be NULL. (No counterpart in the
  * reference, which always scans.) */
 RUMB_API int rumb_cg_pricer_info(const rumb_cg_pricer *pricer, long long *list_entries, long long *list_bytes);
+/* sweep_max64 (solver/flow_cg/pricing_stream.py:236-249) on the pricer's rows: V[full] of the
+ * longest path with float64 scores (host memory, the pricer's row order), two float64 layers of
+ * C(n, n/2) ranks live (allocated on the first call, kept with the pricer). The Frank-Wolfe bound's
+ * sweep where its float64 slab does not fit (solver/common/transforms.py:117-129). */
+RUMB_API int rumb_cg_pricer_max64(rumb_cg_pricer *pricer, const double *scores, double *vmax);
 
 /* The CG master's column bookkeeping on the pricer's GPU (replaces the host maintainers
  * solver/flow_cg/qp_bitset_incremental.py:36-141 and the column builder

@@ -15,6 +15,7 @@ Files written:
   ref_bm_f64.cu     scatter_obs, the fused elementwise kernels of solve_kadmm_v2 (as _mk_ew
                     wraps them), prox_all, bfly_blk, bfly_co, bfly_blk2 with `typedef double real`
   ref_cert64.cu     outwt64, massg64, extract64, lpath64
+  ref_max64.cu      bf_stream_max64 (solver/flow_cg/pricing_stream.py _SRC64: the float64 max sweep)
   ref_pricing.cu    bf_stream_f32 / bf_stream_u16 / bf_stream_u24 (BLOCK etc. substituted as the
                     module does) and bf_update
 """
@@ -87,6 +88,7 @@ def extract(root):
     pricing = _string(src.left) % consts
     pricing += "\n\n" + _string(_assigned(bfp, "_BF_UPDATE_SRC"))
     open(os.path.join(OUT, "ref_pricing.cu"), "w").write(pricing + "\n")
+    open(os.path.join(OUT, "ref_max64.cu"), "w").write(_string(_assigned(stream, "_SRC64")) + "\n")
     open(os.path.join(OUT, "consts.txt"), "w").write(repr(consts) + "\n")
     return OUT
 

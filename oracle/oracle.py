@@ -69,6 +69,8 @@ def lib():
         L.ora_price_stream.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ullp, _fp,
                                        _llp, _dp, _ip, _dp, _fp]
         L.ora_ranking_column.argtypes = [ctypes.c_int, ctypes.c_longlong, _ullp, _ip, _ip, _u8p]
+        L.ora_sweep_max64.argtypes = [ctypes.c_int, _ullp, _dp, _llp]
+        L.ora_sweep_max64.restype = ctypes.c_double
         L.ora_set_threads.argtypes = [ctypes.c_int]
         L.ora_get_threads.restype = ctypes.c_int
         _LIB = L
@@ -301,6 +303,27 @@ def price_stream(n, menus, scores, offsets, mode="u24", k_pred=None, fma_decode=
                            _ptr(scores, _fp), _ptr(offsets, _llp), ctypes.byref(vmax), _ptr(rank, _ip),
                            ctypes.byref(margin), _ptr(steps, _fp))
     return vmax.value, rank, margin.value, steps
+
+
+def sweep_max64(n, menus, scores, offsets):
+    """V[full] of the float64 max sweep (solver/flow_cg/pricing_stream.py:236-249); x-major rows."""
+    menus = np.ascontiguousarray(menus, dtype=np.uint64)
+    scores = np.ascontiguousarray(scores, dtype=np.float64)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    return float(lib().ora_sweep_max64(int(n), _ptr(menus, _ullp), _ptr(scores, _dp), _ptr(offsets, _llp)))
+
+
+def fw_lb_stream64(n, menu, alt, y, phat):
+    """fw_lb_stream64 (solver/common/transforms.py:117-129): the float64 Frank-Wolfe bound at the
+    point y through the two-layer max sweep; rows in any order."""
+    alt = np.asarray(alt, dtype=np.int64)
+    y = np.asarray(y, dtype=np.float64)
+    r = np.asarray(phat, dtype=np.float64) - y
+    perm = np.argsort(alt, kind="stable")
+    offsets = np.concatenate(([0], np.cumsum(np.bincount(alt, minlength=n)))).astype(np.int64)
+    vmax = sweep_max64(n, np.asarray(menu, dtype=np.uint64)[perm], r[perm], offsets)
+    rc = vmax - float(r @ y)
+    return float(np.sqrt(max(0.0, float(r @ r) - 2.0 * rc)))
 
 
 def price_mask(n, menus, scores, offsets):

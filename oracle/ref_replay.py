@@ -115,6 +115,8 @@ def _mods():
         _MODS["bm"] = _Module(os.path.join(REF, "ref_bm_f64.cu"))
         _MODS["cert"] = _Module(os.path.join(REF, "ref_cert64.cu"))
         _MODS["pricing"] = _Module(os.path.join(REF, "ref_pricing.cu"), options=("--std=c++11",))
+        if os.path.exists(os.path.join(REF, "ref_max64.cu")):
+            _MODS["max64"] = _Module(os.path.join(REF, "ref_max64.cu"), options=("--std=c++11",))
     return _MODS
 
 
@@ -255,6 +257,26 @@ def price_stream(menus, alts, scores, offsets, n, mode="u24", k_pred=None):
     for j, e in enumerate(elems):
         rank_pos[e] = pos + int(order[j])
     return vmax, rank_pos, margin, layer_step
+
+
+def sweep_max64(menus, scores, offsets, n):
+    """sweep_max64 (solver/flow_cg/pricing_stream.py:236-249) with the reference's bf_stream_max64:
+    V[full] in float64 with two live layers; rows x-major, scores float64."""
+    import torch
+    L = _Launcher(_mods()["max64"])
+    counts = [math.comb(n, k) for k in range(n + 1)]
+    buf = [torch.zeros(max(counts), dtype=torch.float64, device="cuda") for _ in range(2)]
+    gm = torch.from_numpy(np.ascontiguousarray(menus, dtype=np.uint64).view(np.int64)).cuda()
+    gs = torch.from_numpy(np.ascontiguousarray(scores, dtype=np.float64)).cuda()
+    go = torch.from_numpy(np.asarray(offsets, dtype=np.uint64).view(np.int64)).cuda()
+    binom = torch.from_numpy(_binom(n).view(np.int64)).cuda()
+    prev, cur = 0, 1
+    for k in range(1, n + 1):
+        L.launch("bf_stream_max64", (counts[k] + 255) // 256, 256,
+                 [binom, (_I, n), (_I, k), (_ULL, counts[k]), buf[prev], buf[cur], gm, gs, go])
+        prev, cur = cur, prev
+    torch.cuda.synchronize()
+    return float(buf[prev][0].item())
 
 
 # ------------------------------------------------------------------ BM-ADMM timing replay

@@ -461,6 +461,56 @@ static void stream_layer(int mode, int fma_decode, int n, int k, ull count, cons
     free(vals);
 }
 
+/* sweep_max64 (solver/flow_cg/pricing_stream.py:190-249): V[full] = the longest path over the
+ * subset lattice with float64 scores, two rank-indexed layers live: for every k-subset D (colex
+ * rank r), V[D] = max over x in D of V[D \ {x}] + w(x, D), w a sequential float64 sum of x's row
+ * scores whose menu is a subset of D, in row order. Only the maximum is kept (no predecessors). */
+double ora_sweep_max64(int n, const ull *menus, const double *scores, const ll *offsets) {
+    ull *binom = binom_table(n);
+    ull cap = 1;
+    for (int k = 0; k <= n; ++k) if (binom[n * (n + 1) + k] > cap) cap = binom[n * (n + 1) + k];
+    double *prev = (double *)calloc((size_t)cap, sizeof(double));
+    double *cur = (double *)calloc((size_t)cap, sizeof(double));
+    for (int k = 1; k <= n; ++k) {
+        ull count = binom[n * (n + 1) + k];
+        for (ull r = 0; r < count; ++r) {
+            /* elements of the subset of rank r, ascending */
+            int el[64];
+            ull rr = r, D = 0ULL;
+            int b = n - 1;
+            for (int t = k; t >= 1; --t) {
+                while (binom[b * (n + 1) + t] > rr) --b;
+                el[t - 1] = b;
+                D |= 1ULL << b;
+                rr -= binom[b * (n + 1) + t];
+                --b;
+            }
+            double best = 0.0;
+            int seen = 0;
+            for (int j = 0; j < k; ++j) {
+                /* rank of D without el[j]: the elements below keep their positions, those above move down one */
+                ull rp = 0;
+                for (int i = 0; i < k; ++i) {
+                    if (i == j) continue;
+                    int pos = i < j ? i : i - 1;
+                    rp += binom[el[i] * (n + 1) + pos + 1];
+                }
+                double w = 0.0;
+                int x = el[j];
+                for (ll i = offsets[x]; i < offsets[x + 1]; ++i)
+                    if ((menus[i] & D) == menus[i]) w += scores[i];
+                double cand = prev[rp] + w;
+                if (!seen || cand > best) { best = cand; seen = 1; }
+            }
+            cur[r] = best;
+        }
+        double *t = prev; prev = cur; cur = t;
+    }
+    double v = prev[0];
+    free(prev); free(cur); free(binom);
+    return v;
+}
+
 /* StreamPricer.price: the sweep, then the backtrace through the stored predecessor layers and
  * the mask DP on the sub-lattice of the node reached at layer k_pred
  * (solver/flow_cg/pricing_stream.py:302-412). Returns 0; vmax (float64 decode as the host does),

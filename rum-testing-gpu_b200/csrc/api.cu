@@ -260,6 +260,16 @@ int rumb_cg_price(rumb_cg_pricer *pr, const float *scores, int on_device, double
     RUMB_API_END
 }
 
+int rumb_cg_pricer_max64(rumb_cg_pricer *pr, const double *scores, double *vmax) {
+    RUMB_API_BEGIN
+    if (!pr || !pr->p) rumb::fail(RUMB_E_INVAL, "pricer is NULL");
+    if (!scores || !vmax) rumb::fail(RUMB_E_INVAL, "scores / vmax must not be NULL");
+    rumb::DeviceGuard dg(pr->device);
+    rumb::pricer_max64(pr->p, scores, vmax);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
 int rumb_cg_pricer_info(const rumb_cg_pricer *pr, long long *list_entries, long long *list_bytes) {
     RUMB_API_BEGIN
     if (!pr || !pr->p) rumb::fail(RUMB_E_INVAL, "pricer is NULL");

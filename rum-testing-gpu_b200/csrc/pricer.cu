@@ -242,6 +242,71 @@ __global__ void __launch_bounds__(PR * PE_G) layer_eval_kernel(PricerArgs A, flo
     else vals[r] = b;
 }
 
+// The float64 max sweep (sweep_max64, the Frank-Wolfe bound's longest path when the float64 slab
+// does not fit): the same layer mapping with float64 scores and values, only the maximum kept. Each
+// w(x, D) is a sequential float64 sum over the same rows in row order (cover lists or the row scan)
+// and the maximum is exact, so V[full] is the reference kernel's bit for bit.
+template <int PR>
+__global__ void __launch_bounds__(PR * PE_G) max64_layer_kernel(PricerArgs A, const double *scores,
+                                                                 const double *vprev, double *vcur) {
+    static_assert(PR % 32 == 0 && (PR / 32) * PE_G <= 32, "at most 32 warps");
+    __shared__ double pbest[PE_G][PR];
+    __shared__ signed char pok[PE_G][PR];
+    __shared__ ull sbin[BIN_MAX];
+    const int n = A.n, k = A.k;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rg = w % (PR / 32), xg = w / (PR / 32);
+    const int loc = rg * 32 + lane;
+    const ull r = (ull)blockIdx.x * PR + loc;
+    const bool valid = r < A.count;
+    stage_binom(sbin, A.binom, n);
+    __syncthreads();
+    const ull D = valid ? colex_unrank(r, k, n, sbin) : 0ULL;
+    const ull pbase = A.lbase + r * (ull)k;
+    double best = 0.0;
+    bool seen = false;
+    for (int x = n - 1; x >= 0; --x) {
+        if ((x & (PE_G - 1)) != xg) continue;            // uniform per warp
+        const bool in = valid && ((D >> x) & 1ULL);
+        const int j = __popcll(D & ((1ULL << x) - 1ULL));
+        const ll lo = A.offsets[x];
+        double wsum = 0.0;
+        if (A.wmode == W_SCAN) {
+            if (__any_sync(0xffffffffu, in)) {
+                for (ll i = lo; i < A.offsets[x + 1]; ++i) {
+                    const ull Dp = __ldg(A.menus + i);
+                    const double sc = __ldg(scores + i);
+                    if (in && (Dp & D) == Dp) wsum = __dadd_rn(wsum, sc);
+                }
+            }
+        } else if (in) {
+            const unsigned b = __ldg(A.loffs + pbase + j), e = __ldg(A.loffs + pbase + j + 1);
+            if (A.wmode == W_LIST16) {
+                const uint16_t *ent = (const uint16_t *)A.lent;
+                for (unsigned i = b; i < e; ++i) wsum = __dadd_rn(wsum, __ldg(scores + lo + __ldg(ent + i)));
+            } else {
+                const uint32_t *ent = (const uint32_t *)A.lent;
+                for (unsigned i = b; i < e; ++i) wsum = __dadd_rn(wsum, __ldg(scores + lo + __ldg(ent + i)));
+            }
+        }
+        if (in) {
+            const double cand = __dadd_rn(vprev[colex_rank_without(r, D, x, j, n, sbin)], wsum);
+            if (!seen || cand > best) { best = cand; seen = true; }
+        }
+    }
+    pbest[xg][loc] = best;
+    pok[xg][loc] = seen ? 1 : 0;
+    __syncthreads();
+    if (xg != 0 || !valid) return;
+    double b = 0.0;
+    bool any = false;
+    for (int g = 0; g < PE_G; ++g) {
+        if (!pok[g][loc]) continue;
+        if (!any || pbest[g][loc] > b) { b = pbest[g][loc]; any = true; }
+    }
+    vcur[r] = b;
+}
+
 // The same layer for long lists (the top layers, where a subset's lists hold up to all of x's
 // rows): one CTA per rank, warp w takes the alternatives x = w, w + NW, ... in D. The warp walks
 // pair (D, x)'s list 32 entries at a time (coalesced index loads, 32 score gathers in flight, the
@@ -509,6 +574,7 @@ struct Pricer {
     std::vector<ull> lbase;                 // first pair index per layer (n+2)
     DevBuf lbase_dev, loffs, lent;
     std::vector<char> wide;                 // per layer: layer_wide_kernel (1) or layer_eval_kernel (0)
+    DevBuf d64[2], s64;                     // the float64 max sweep's two layers and scores (on first use)
 };
 
 // Mean cover-list length from which a layer runs layer_wide_kernel (measured at n = 18: a mean of
@@ -661,6 +727,45 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
     P->wide.assign(n + 1, 0);
     if (!scan) build_cover_lists(*P, menus);
     return P.release();
+}
+
+void pricer_max64(Pricer *P, const double *scores_host, double *vmax) {
+    Ctx &c = *P->c;
+    cudaStream_t st = c.own;
+    const int n = P->n;
+    ull cap = 0;
+    for (ull v : P->counts) cap = v > cap ? v : cap;
+    P->s64.ensure((size_t)std::max<ll>(P->mp, 1) * 8);
+    for (int i = 0; i < 2; ++i) P->d64[i].ensure((size_t)cap * 8);
+    if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->s64.ptr, scores_host, (size_t)P->mp * 8, cudaMemcpyHostToDevice, st));
+    int cur = 0, prev = 1;
+    RUMB_CUDA(cudaMemsetAsync(P->d64[prev].ptr, 0, 8, st));     // layer 0: V[empty set] = 0
+    for (int k = 1; k <= n; ++k) {
+        PricerArgs A{};
+        A.n = n;
+        A.k = k;
+        A.count = P->counts[k];
+        A.binom = P->binom.as<ull>();
+        A.menus = P->menus.as<ull>();
+        A.offsets = P->offsets.as<ll>();
+        A.wmode = P->wmode;
+        A.loffs = P->loffs.as<unsigned>();
+        A.lent = P->lent.ptr;
+        A.lbase = P->wmode == W_SCAN ? 0 : P->lbase[k];
+        const double *vp = P->d64[prev].as<double>();
+        double *vc = P->d64[cur].as<double>();
+        if ((long long)A.count < 2LL * num_sms(c.device) * PE_R) {
+            max64_layer_kernel<PE_R_SMALL><<<(unsigned)((A.count + PE_R_SMALL - 1) / PE_R_SMALL), PE_R_SMALL * PE_G,
+                                             0, st>>>(A, P->s64.as<double>(), vp, vc);
+        } else {
+            max64_layer_kernel<PE_R><<<(unsigned)((A.count + PE_R - 1) / PE_R), PE_R * PE_G, 0, st>>>(
+                A, P->s64.as<double>(), vp, vc);
+        }
+        RUMB_LAUNCH("max64_layer_kernel");
+        std::swap(cur, prev);
+    }
+    RUMB_CUDA(cudaMemcpyAsync(vmax, P->d64[prev].ptr, 8, cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
 }
 
 void pricer_info(const Pricer *P, long long *list_entries, long long *list_bytes) {

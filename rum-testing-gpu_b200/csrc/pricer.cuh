@@ -11,6 +11,7 @@ void pricer_price(Pricer *P, const float *scores, int on_device, double *vmax, i
                   float *layer_step_out);
 int pricer_device(const Pricer *P);
 void pricer_info(const Pricer *P, long long *list_entries, long long *list_bytes);
+void pricer_max64(Pricer *P, const double *scores_host, double *vmax);
 // the pricer's context, n, row count and device rows (x-major menus), for the CG master
 Ctx &pricer_ctx(const Pricer *P);
 int pricer_n(const Pricer *P);

@@ -126,6 +126,7 @@ _SIGS = {
     "rumb_draws_screen": ([_vp, _vp, ctypes.c_double, _vp, _vp], ctypes.c_int),
     "rumb_draws_destroy": ([_vp], ctypes.c_int),
     "rumb_cg_pricer_info": ([_vp, _vp, _vp], ctypes.c_int),
+    "rumb_cg_pricer_max64": ([_vp, _vp, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "rumb_bm_iterate": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, _vp, _vp, _vp,
                          ctypes.c_int, ctypes.c_int], ctypes.c_int),
 }
@@ -560,6 +561,15 @@ class Pricer:
                                            0 if k_pred is None else int(k_pred), int(bool(fma_decode)),
                                            ctypes.byref(h)))
         self.h, self.n, self.mp, self.mode, self.ctx = h, int(n), menus.size, mode, ctx
+
+    def max64(self, scores):
+        """V[full] of the float64 max sweep over float64 scores in the pricer's row order."""
+        scores = np.ascontiguousarray(scores, dtype=np.float64)
+        if scores.size != self.mp:
+            raise ValueError("expected %d scores" % self.mp)
+        v = ctypes.c_double()
+        check(load().rumb_cg_pricer_max64(self.h, _p(scores), ctypes.byref(v)))
+        return v.value
 
     @property
     def list_entries(self):

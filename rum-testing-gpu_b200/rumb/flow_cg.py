@@ -376,6 +376,32 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
 
 
 # ------------------------------------------------------------------ certified runner
+def sweep_max64_bytes(n, rows):
+    """Device bytes of the float64 max sweep: two float64 layers of C(n, n//2) ranks, the rows
+    (menu + score) and the tables (solver/flow_cg/pricing_stream.py:228-231)."""
+    return 2 * 8 * math.comb(n, n // 2) + 16 * int(rows) + 8 * (n + 1) * (n + 2) + 4096
+
+
+def fw_lb_stream64(prob, y, phat):
+    """fw_lb_stream64 (solver/common/transforms.py:117-129) on a CGProblem's pricer: the float64
+    Frank-Wolfe bound at the point y (rows in input order) through the two-layer max sweep."""
+    y = np.asarray(y, dtype=np.float64)
+    r = np.asarray(phat, dtype=np.float64) - y
+    vmax = prob.pricer.max64(r[prob.perm])
+    rc = vmax - float(r @ y)
+    return float(np.sqrt(max(0.0, float(r @ r) - 2.0 * rc)))
+
+
+def lb_layout(n, rows, budget):
+    """_flow_cg_lb's choice (solver/rum_solver.py:926-938): the float64 bound from its slab when
+    the slab fits, else two lattice layers at a time, else the pricing bound lowered by delta."""
+    if 16 * (n << (n - 1)) + 16 * (1 << n) <= budget:
+        return "slab"
+    if sweep_max64_bytes(n, rows) <= budget:
+        return "two layers"
+    return "pricing sweep"
+
+
 def _cg_stops(below, above, margin):
     kw = {}
     if below is not None:
@@ -418,11 +444,17 @@ def run_flow_cg(t, ctx):
         st["p_fit"] = p_fit
         st["ub"] = float(np.linalg.norm(p_fit - t.p))
         lb_prev = st["lb"]
+        from . import defaults
+        from .rum_solver import gpu_free_bytes
+        layout = lb_layout(n, g.M, defaults.AUTO["gpu_memory_fraction"] * gpu_free_bytes())
         if below is not None and st["ub"] < below:
             lb = lb_prev
+        elif layout == "slab":
+            lb = ctx.fw_lb64(n, g.menu.astype(np.uint32), g.alternative.astype(np.int32), p_fit, t.p)
+        elif layout == "two layers":
+            lb = fw_lb_stream64(prob, p_fit, t.p)
         else:
-            lb = ctx.fw_lb64(n, g.menu.astype(np.uint32), g.alternative.astype(np.int32), p_fit, t.p) \
-                if n <= 30 else float(r["lb"]) - delta
+            lb = float(r["lb"]) - delta
         st["lb"] = max(lb_prev, lb)
         st["iterations"] = int(r["n_cols"])
         st["setup"] += float(r["setup_s"])
@@ -432,8 +464,8 @@ def run_flow_cg(t, ctx):
             st["trace"][-1] = st["trace"][-1][:2] + (st["ub"], st["lb"])
         st["info"].update(pricing=engine, p_float32_shift=delta,
                           pricing_margin=max(r["margins"]) if r["margins"] else 0.0, restarts=attempt,
-                          lb_dtype="float64" if n <= 30 else a["dtype"], lb_layout="slab" if n <= 30 else "pricing sweep",
-                          lb_rigorous=n <= 30, qp_s=round(r["qp_s"], 3), price_s=round(r["price_s"], 3))
+                          lb_dtype=a["dtype"] if layout == "pricing sweep" else "float64", lb_layout=layout,
+                          lb_rigorous=layout != "pricing sweep", qp_s=round(r["qp_s"], 3), price_s=round(r["price_s"], 3))
         if getattr(t, "keep", False):
             st["keep"] = dict(columns=r["columns"], lam=r["lam"])
         if (below is not None and st["ub"] < below) or (above is not None and st["lb"] >= above):

@@ -105,6 +105,40 @@ def test_cover_lists_wide_alternative(ctx):
         b.close()
 
 
+@pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
+def test_max64_sweep_bit_exact(ctx, name, cd, n):
+    """The float64 max sweep (rumb_cg_pricer_max64, cover lists and row scan) equals the oracle's and
+    the reference's own bf_stream_max64 kernel bit for bit."""
+    import ref_replay
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    rng = np.random.RandomState(13)
+    for lists in (True, False):
+        pr = _lib.Pricer(ctx, n, menus, offsets, mode="u24", lists=lists)
+        for trial in range(2):
+            s = rng.randn(menus.size) * (1.0 if trial == 0 else 1e-3)
+            v = pr.max64(s)
+            assert v == O.sweep_max64(n, menus, s, offsets)
+            if ref_replay.available() and "max64" in ref_replay._mods():
+                assert v == ref_replay.sweep_max64(menus, s, offsets, n)
+        pr.close()
+
+
+def test_two_layer_bound_equals_slab_bound(ctx):
+    """fw_lb_stream64 through the max sweep and the slab-based float64 bound (rumb_fw_lb64) agree."""
+    from rumb import flow_cg
+    cd, mp = PI.gen_medium(14, mult=3)
+    n = 14
+    prob = flow_cg.CGProblem(ctx, n, cd[:, 0], cd[:, 1], "u24")
+    rng = np.random.RandomState(2)
+    p = cd[:, 2]
+    for _ in range(3):
+        y = np.clip(p + 0.05 * rng.randn(p.size), 0.0, 1.0)
+        a = flow_cg.fw_lb_stream64(prob, y, p)
+        b = ctx.fw_lb64(n, cd[:, 0].astype(np.uint32), cd[:, 1].astype(np.int32), y, p)
+        assert abs(a - b) <= 1e-11 * max(1.0, b)
+        assert a == O.fw_lb_stream64(n, cd[:, 0], cd[:, 1], y, p)
+
+
 def test_mask_and_f32_stream_identical(ctx):
     cd, mp = PI.gen_medium(14, mult=4)
     menus, alts, p32, offsets, _ = O.cg_layout(14, cd[:, 0], cd[:, 1], cd[:, 2])

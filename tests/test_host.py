@@ -125,6 +125,19 @@ def test_gram_and_pout_maintainers():
     np.testing.assert_allclose(po.p_out, V @ lam, atol=1e-14)
 
 
+def test_flow_cg_lower_bound_layout():
+    """The reference's choice of the final lower bound's form by device memory: the float64 slab,
+    else two float64 lattice layers, else the pricing bound."""
+    assert flow_cg.lb_layout(18, 23568, 180e9) == "slab"
+    slab = 16 * (30 << 29) + 16 * (1 << 30)
+    two = flow_cg.sweep_max64_bytes(30, 10 ** 5)
+    assert two < slab
+    assert flow_cg.lb_layout(30, 10 ** 5, slab) == "slab"
+    assert flow_cg.lb_layout(30, 10 ** 5, slab - 1) == "two layers"
+    assert flow_cg.lb_layout(30, 10 ** 5, two - 1) == "pricing sweep"
+    assert flow_cg.sweep_max64_bytes(33, 0) == 2 * 8 * math.comb(33, 16) + 8 * 34 * 35 + 4096
+
+
 def test_gram_maintainer_growth():
     """Q and h stay V'V and V'p_hat while the storage doubles (256 -> 512 columns)."""
     rng = np.random.default_rng(4)

@@ -39,6 +39,39 @@ def test_certificate_pieces_match_reference(n):
     np.testing.assert_array_equal(idx, g["slab_idx_%d" % n])
 
 
+@pytest.mark.parametrize("n", [3, 4, 5, 6, 8, 10])
+def test_oracle_two_layer_bound_matches_reference(n):
+    """fw_lb_stream64 (the float64 max sweep, two layers live) gives the reference's slab-based
+    Frank-Wolfe bound at the golden points."""
+    g = _load("certificate.npz")
+    idx = np.asarray(g["zeta_obs_%d" % n], dtype=np.int64)
+    x = idx >> (n - 1)
+    rest = idx & ((1 << (n - 1)) - 1)
+    menu = ((rest >> x) << (x + 1)) | (rest & ((1 << x) - 1)) | (1 << x)
+    lb = O.fw_lb_stream64(n, menu, x, g["fwlb_y_%d" % n], g["fwlb_p_%d" % n])
+    assert abs(lb - g["fwlb_v_%d" % n][0]) <= 1e-11 * max(1.0, lb)
+
+
+@pytest.mark.parametrize("n", [4, 6, 7])
+def test_oracle_max_sweep_is_the_best_ranking(n):
+    """V[full] of the float64 max sweep is the largest summed score over all n! rankings."""
+    rng = np.random.default_rng(n)
+    menus_all = [m for m in range(1, 1 << n) if bin(m).count("1") >= 2]
+    rows = [(m, x) for m in menus_all if rng.random() < 0.6 for x in range(n) if (m >> x) & 1]
+    menu = np.array([r[0] for r in rows], dtype=np.int64)
+    alt = np.array([r[1] for r in rows], dtype=np.int64)
+    menus, alts, _, offsets, perm = O.cg_layout(n, menu, alt, np.zeros(len(rows)))
+    scores = rng.standard_normal(len(rows))
+    best = -np.inf
+    for order in itertools.permutations(range(n)):
+        rank = np.empty(n, dtype=np.int32)
+        rank[list(order)] = np.arange(n)
+        col = O.ranking_column(n, menus, alts, rank)
+        best = max(best, float(scores[col > 0].sum()))
+    v = O.sweep_max64(n, menus, scores, offsets)
+    assert abs(v - best) <= 1e-12 * max(1.0, abs(best))
+
+
 def test_master_qp_matches_reference():
     g = _load("qp.npz")
     for t in range(4):
