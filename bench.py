@@ -233,7 +233,7 @@ def run_pricing(args, rank):
 
 
 def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
-    """Workload bootstrap_n20 (n = 20, 1 % menus, a 520-respondent panel of 30
+    """Workload bootstrap_n20 (n20_d1pct_panel520: n = 20, 1 % menus, a 520-respondent panel of 30
     menus each, K = 30): certify p_hat, then solve open draws to abs 5e-4 from p_hat's state,
     batched (rumb_bm_solve_batch, all draws resident) against one at a time (Session.solve), both
     float64. Wall time around each phase with the device synchronized on both sides; the one-at-a-
@@ -264,7 +264,7 @@ def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
         its.append(int(r.iterations))
     torch.cuda.synchronize()
     ts = time.perf_counter() - t0
-    # the screen of config 4's B = 10,000 draws (rows, perturbation, ||P_b - p_fit|| and ||p_b - p_hat||):
+    # the screen of 10,000 draws of this panel (rows, perturbation, ||P_b - p_fit|| and ||p_b - p_hat||):
     # on the GPU over all draws, and the host builder (the reference's block builder) on a sample
     from rumb import _lib
     from rumb.rum_solver import context
