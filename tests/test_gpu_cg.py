@@ -139,6 +139,34 @@ def test_two_layer_bound_equals_slab_bound(ctx):
         assert a == O.fw_lb_stream64(n, cd[:, 0], cd[:, 1], y, p)
 
 
+def test_master_and_max64_reject_bad_input(ctx):
+    """The CG master and the float64 sweep refuse bad arguments with an error."""
+    n = 8
+    cd, mp = PI.gen_medium(n, mult=2)
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode="mask")
+    with pytest.raises(ValueError):
+        pr.max64(np.zeros(menus.size + 1))
+    with pytest.raises(_lib.RumbError):                     # an alternative out of range
+        bad = alts.copy()
+        bad[0] = n
+        _lib.CgMaster(pr, bad, p32.astype(np.float64), 4)
+    m = _lib.CgMaster(pr, alts, p32.astype(np.float64), 2)
+    with pytest.raises(_lib.RumbError):                     # not a permutation
+        m.add_column(rank_pos=np.zeros(n, dtype=np.int32))
+    k, bits, row = m.add_column(rank_pos=np.arange(n, dtype=np.int32))
+    assert k == 0 and row[0] == float(np.unpackbits(bits.view(np.uint8)).sum())
+    with pytest.raises(_lib.RumbError):                     # a column the master does not hold
+        m.apply(np.array([1]), np.array([0.5]))
+    m.add_column(rank_pos=np.arange(n, dtype=np.int32)[::-1].copy())
+    with pytest.raises(_lib.RumbError):                     # columns not increasing
+        m.apply(np.array([1, 0]), np.array([0.5, 0.5]))
+    with pytest.raises(_lib.RumbError):                     # beyond max_cols
+        m.add_column(rank_pos=np.arange(n, dtype=np.int32))
+    m.close()
+    pr.close()
+
+
 def test_mask_and_f32_stream_identical(ctx):
     cd, mp = PI.gen_medium(14, mult=4)
     menus, alts, p32, offsets, _ = O.cg_layout(14, cd[:, 0], cd[:, 1], cd[:, 2])

@@ -47,3 +47,22 @@ def test_draw_rows_and_screen_match_host(ctx, name, panel, m, a, p, B, weights):
     with pytest.raises(_lib.RumbError):
         g.rows(np.array([B], dtype=np.int64))
     g.close()
+
+
+def test_draws_reject_bad_input(ctx):
+    """Bad panels are refused on the host with an error, before anything reaches the GPU."""
+    import scipy.sparse as sp
+    panel, (m, a, p) = panel_instance(8, 0.4, 20, 4, 3, seed=2)
+    d = BS.Draws(panel, m, a, p, B=4, weights="multinomial", seed=0)
+    with pytest.raises(_lib.RumbError):                     # a row's menu out of range
+        bad = d.row_menu.copy()
+        bad[0] = d.offered.shape[1]
+        _lib.DrawRows(ctx, d.W, d.offered, d.chose, bad, d.p_hat)
+    with pytest.raises(_lib.RumbError):                     # a respondent beyond R
+        off = sp.csr_array((np.ones(1), ([d.R], [0])), shape=(d.R + 1, d.offered.shape[1]))
+        _lib.DrawRows(ctx, d.W, off, d.chose, d.row_menu, d.p_hat)
+    g = _lib.DrawRows(ctx, d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+    with pytest.raises(_lib.RumbError):                     # a draw index out of range
+        g.rows(np.array([-1], dtype=np.int64))
+    assert g.rows(np.zeros(0, dtype=np.int64)).shape == (0, d.M)
+    g.close()
