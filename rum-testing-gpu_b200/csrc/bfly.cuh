@@ -205,12 +205,8 @@ inline void bf_launch_pass(const BfArgs<T, TI> &A, int n, cudaStream_t st) {
         RUMB_LAUNCH("bfly_small");
         return;
     }
-    static bool attr_set = false;
-    if (!attr_set) {
-        RUMB_CUDA(cudaFuncSetAttribute(bfly_pass<T, TI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(sizeof(T) << BF_MAX_TILE_LOG)));
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> optin{0};
+    smem_optin(bfly_pass<T, TI>, (int)(sizeof(T) << BF_MAX_TILE_LOG), optin);
     ll tiles = A.Nloc >> (A.s == 0 ? A.B : A.B + 5);
     size_t smem = (size_t)sizeof(T) << (A.s == 0 ? A.B : A.B + 5);
     if (g_prof) {

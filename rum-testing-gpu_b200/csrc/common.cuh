@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -90,6 +91,18 @@ __host__ __device__ __forceinline__ ull compress_bit(ull mask, int x) {
 }
 __host__ __device__ __forceinline__ ull expand_bit(ull rest, int x) {
     return (rest & ((1ULL << x) - 1ULL)) | ((rest >> x) << (x + 1));
+}
+
+// The opt-in for more than 48 KB of dynamic shared memory is an attribute of a kernel on one
+// device: set it once per (kernel, device), `done` holding one bit per device already set.
+template <class K>
+inline void smem_optin(K *kernel, int bytes, std::atomic<unsigned long long> &done) {
+    int dev = 0;
+    RUMB_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ULL << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
+    RUMB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.fetch_or(bit, std::memory_order_release);
 }
 
 inline int num_sms(int dev) {

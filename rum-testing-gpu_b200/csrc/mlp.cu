@@ -286,11 +286,8 @@ static CUtensorMap bf16_map(const bf16 *ptr, ll rows, ll cols) {
 static void gemm(const bf16 *A, const bf16 *B, GemmArgs g, cudaStream_t st) {
     if (g.M % GM_BM || g.N % GM_BN || g.K % GM_BK || g.M <= 0 || g.N <= 0 || g.K <= 0)
         fail(RUMB_E_INVAL, "GEMM: M and N multiples of 128, K a multiple of 64");
-    static bool attr = false;
-    if (!attr) {
-        RUMB_CUDA(cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GM_SMEM));
-        attr = true;
-    }
+    static std::atomic<unsigned long long> optin{0};
+    smem_optin(umma_gemm_kernel, (int)GM_SMEM, optin);
     CUtensorMap ta = bf16_map(A, g.M, g.K), tb = bf16_map(B, g.N, g.K);
     dim3 grid((unsigned)(g.N / GM_BN), (unsigned)(g.M / GM_BM));
     if (g_prof) prof_begin("umma_gemm", 2.0 * ((double)g.M * g.K + (double)g.N * g.K) + 4.0 * g.M * g.N, st);

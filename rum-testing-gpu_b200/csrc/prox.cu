@@ -191,13 +191,9 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
 // ---------------------------------------------------------------- launchers
 template <class T, int N>
 static void launch_tile_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
-    static bool attr = false;   // the opt-in above 48 KB, once per kernel
+    static std::atomic<unsigned long long> optin{0};   // the opt-in above 48 KB, per device
     const size_t smem = prox_tile_smem<T>(N);
-    if (!attr) {
-        RUMB_CUDA(cudaFuncSetAttribute(prox_tile_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-        attr = true;
-    }
+    smem_optin(prox_tile_kernel<T, N>, (int)smem, optin);
     dim3 grid((unsigned)(1LL << (N - PT_M)), (unsigned)slots);
     prox_tile_kernel<T, N><<<grid, PT_THREADS, smem, st>>>(P);
     RUMB_LAUNCH("prox_tile_kernel");

@@ -348,13 +348,9 @@ inline std::vector<XfShape> xf_plan(int nb, int lo_bits = 12) {
 
 template <class T, class TI, int L, int RB, int WB, int KIND>
 inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st, int slots = 1) {
-    static bool attr = false;
+    static std::atomic<unsigned long long> optin{0};
     size_t smem = (size_t)sizeof(T) << (RB + WB + 5);
-    if (!attr) {
-        RUMB_CUDA(cudaFuncSetAttribute(xform_pass<T, TI, L, RB, WB, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-        attr = true;
-    }
+    smem_optin(xform_pass<T, TI, L, RB, WB, KIND>, (int)smem, optin);
     ll tiles = (A.Nloc >> (L ? A.B : A.B + 5)) * n;
     if (g_prof) {
         double S = (double)A.Nloc * n * slots, e = sizeof(T), ei = sizeof(TI);
