@@ -1,0 +1,39 @@
+"""Generates tests/golden/draws.npz by running the reference's own bootstrap draws (CPU code).
+
+    python tests/golden/make_draws_golden.py <reference root>
+
+It imports solver/inference/draws.py from the path given (read-only, never copied): for a seeded
+respondent panel (rumb.instances.panel_instance, n = 8) it records the reference's weight rows and
+every draw's rows (Draws.rows, solver/inference/draws.py:151-159,247-285) for both weight schemes.
+The tests compare the library's draws (host builder and GPU kernel) against this file; nothing at
+test time reads the reference itself.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "rum-testing-gpu_b200"))
+
+
+def main(ref_root):
+    sys.path.insert(0, ref_root)
+    from solver.inference import draws as RD
+    from rumb.instances import panel_instance
+    panel, (m, a, p) = panel_instance(8, 0.4, 40, 6, 4, seed=21)
+    out = dict(panel_respondent=np.asarray(panel["respondent"], dtype=np.int64),
+               panel_menu=np.asarray(panel["menu"], dtype=np.int64),
+               panel_chosen=np.asarray(panel["chosen"], dtype=np.int64),
+               menu=np.asarray(m, dtype=np.int64), alternative=np.asarray(a, dtype=np.int64),
+               p_hat=np.asarray(p, dtype=np.float64))
+    for weights in ("multinomial", "multinomial_reject"):
+        d = RD.Draws(panel, m, a, p, B=12, weights=weights, seed=5)
+        out["W_" + weights] = np.asarray(d.W, dtype=np.float64)
+        out["rows_" + weights] = np.asarray(d.rows(np.arange(12)), dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "draws.npz"), **out)
+    print("wrote", os.path.join(HERE, "draws.npz"))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

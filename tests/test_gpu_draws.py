@@ -49,6 +49,18 @@ def test_draw_rows_and_screen_match_host(ctx, name, panel, m, a, p, B, weights):
     g.close()
 
 
+def test_gpu_rows_match_reference_golden(ctx):
+    """The GPU rows equal the reference's own draws (tests/golden/draws.npz) bit for bit."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "draws.npz"))
+    panel = dict(respondent=g["panel_respondent"], menu=g["panel_menu"], chosen=g["panel_chosen"])
+    for w in ("multinomial", "multinomial_reject"):
+        d = BS.Draws(panel, g["menu"], g["alternative"], g["p_hat"], B=12, weights=w, seed=5)
+        gd = _lib.DrawRows(ctx, d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+        np.testing.assert_array_equal(gd.rows(np.arange(12)), g["rows_" + w])
+        gd.close()
+
+
 def test_draws_reject_bad_input(ctx):
     """Bad panels are refused on the host with an error, before anything reaches the GPU."""
     import scipy.sparse as sp

@@ -125,6 +125,18 @@ def test_gram_and_pout_maintainers():
     np.testing.assert_allclose(po.p_out, V @ lam, atol=1e-14)
 
 
+def test_draws_match_reference_golden():
+    """The bootstrap's draws (weights and every draw's rows) equal the reference's own Draws bit for
+    bit, both weight schemes (tests/golden/make_draws_golden.py)."""
+    from rumb import bootstrap as BS
+    g = np.load(os.path.join(GOLD, "draws.npz"))
+    panel = dict(respondent=g["panel_respondent"], menu=g["panel_menu"], chosen=g["panel_chosen"])
+    for w in ("multinomial", "multinomial_reject"):
+        d = BS.Draws(panel, g["menu"], g["alternative"], g["p_hat"], B=12, weights=w, seed=5)
+        np.testing.assert_array_equal(d.W, g["W_" + w])
+        np.testing.assert_array_equal(d.rows(np.arange(12)), g["rows_" + w])
+
+
 def test_flow_cg_lower_bound_layout():
     """The reference's choice of the final lower bound's form by device memory: the float64 slab,
     else two float64 lattice layers, else the pricing bound."""
