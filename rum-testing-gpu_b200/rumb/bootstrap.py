@@ -35,7 +35,7 @@ import json
 import math
 import os
 import time
-from dataclasses import dataclass
+from dataclasses import asdict, dataclass
 
 import numpy as np
 import scipy.sparse as sp
@@ -83,6 +83,38 @@ def decide(L, U, tau_lo, tau_hi):
     d[np.asarray(L) >= tau_hi] = ABOVE
     d[np.asarray(U) < tau_lo] = BELOW
     return d
+
+
+def check_alpha(alpha):
+    alpha = float(alpha)
+    if not 0.0 < alpha < 1.0:
+        raise ValueError("alpha must lie in (0, 1); got %r" % alpha)
+    return alpha
+
+
+def quantile_band(L, U, alpha):
+    """(Q(L), Q(U)): the (1 - alpha)-quantile of the draws' distances lies between these
+    (solver/inference/hong_li.py:102-107); only a draw whose bracket overlaps it moves either end."""
+    return (float(np.quantile(np.asarray(L, dtype=np.float64), 1.0 - alpha)),
+            float(np.quantile(np.asarray(U, dtype=np.float64), 1.0 - alpha)))
+
+
+def ci_lower(L0, U0, L, U, alpha, r_n, eps_n):
+    """The one-sided interval's lower end as (value, the upper end of its bracket, (q_lo, q_hi))
+    (solver/inference/hong_li.py:81-90): value = L0 - q_hi / r_n with q_hi the (1 - alpha)-quantile
+    of (U_b - L0) / eps_n, and the exact end lies below U0 - q_lo / r_n, q_lo the same quantile of
+    (L_b - U0) / eps_n (the end grows with dist(p_hat) and falls with every dist(P_b))."""
+    q_hi = float(np.quantile((np.asarray(U, dtype=np.float64) - L0) / eps_n, 1.0 - alpha))
+    q_lo = float(np.quantile((np.asarray(L, dtype=np.float64) - U0) / eps_n, 1.0 - alpha))
+    return L0 - q_hi / r_n, U0 - q_lo / r_n, (q_lo, q_hi)
+
+
+def distance_interval(L0, U0, dev, alpha):
+    """The two-sided interval (lower, upper, c) with c the (1 - alpha)-quantile of ||p_b - p_hat||
+    (solver/inference/hong_li.py:93-99): dist is 1-Lipschitz, so [max(0, L0 - c), U0 + c] needs no
+    draw solved."""
+    c = float(np.quantile(np.asarray(dev, dtype=np.float64), 1.0 - alpha))
+    return max(0.0, L0 - c), U0 + c, c
 
 
 class Draws:
@@ -158,6 +190,32 @@ class PValue:
     dist_hat: tuple
     time: float
     draws_per_s: float
+
+
+@dataclass
+class Interval:
+    """The one-sided (1 - alpha) interval [lower, inf) (solver/inference/bootstrap.py's Interval)."""
+    lower: float
+    lower_bracket: tuple
+    lower_clipped: float
+    upper: float
+    alpha: float
+    q: tuple
+    reject: bool
+    n_solved: int
+    time: float
+
+
+@dataclass
+class DistanceInterval:
+    """The two-sided (1 - alpha) interval [max(0, L0 - c), U0 + c] (solver/inference/bootstrap.py:108-118)."""
+    lower: float
+    upper: float
+    alpha: float
+    half_width: float
+    dist_hat: tuple
+    reject: bool
+    time: float
 
 
 def _dist(group):
@@ -258,13 +316,24 @@ class Bootstrap:
         return (self.s * self.L0, self.s * self.U0)
 
     def _certify(self):
+        """p_hat's bracket at the current tolerances (a later, tighter one only narrows it)."""
         t0 = time.perf_counter()
         r = self.session.solve(self.p_hat, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_time=self.max_time,
                                keep=True)
         if not math.isfinite(r.ub):
             raise RuntimeError("p_hat could not be certified: %s (%s)" % (r.status, r.message))
-        self.L0, self.U0 = r.lb, r.ub
+        self.L0 = r.lb if self.L0 is None else max(self.L0, r.lb)
+        self.U0 = r.ub if self.U0 is None else min(self.U0, r.ub)
         self.time["certificate"] += time.perf_counter() - t0
+
+    def _start(self):
+        """p_hat certified and every draw screened (once)."""
+        if self.L0 is None:
+            self._certify()
+        if not self.screened:
+            if self.session.fit is None:          # resumed before the screen: certify again
+                self._certify()
+            self._screen()
 
     def _draw_rows(self):
         """The draws on the GPU (built on first use): rows and the screen's norms."""
@@ -443,6 +512,58 @@ class Bootstrap:
         self.screened, self.n_screened = rec["screen"]["done"], rec["screen"]["n_below"]
         self.results, self.time = rec["results"], rec["time"]
 
+    def confidence_interval(self, alpha=0.05):
+        """The certified one-sided interval [lower, inf) (solver/inference/bootstrap.py:212-240):
+        draws are solved to tolerance, largest upper bound first, only while their bracket overlaps
+        the band [Q(L), Q(U)] of the quantile; up to `refine` rounds tighten the tolerances ten-fold
+        (p_hat certified again) while the lower end's bracket is wider than 2 abs_tol."""
+        alpha, t0 = check_alpha(alpha), time.perf_counter()
+        self._start()
+        n0 = int(np.isfinite(self.tol_full).sum())
+        batch = max(1, math.ceil(alpha * self.B / 4))
+        saved = (self.abs_tol, self.rel_tol)
+        tol_a, tol_r = saved
+        try:
+            for rnd in range(int(self.settings["refine"]) + 1):
+                if rnd:
+                    low, high, _ = ci_lower(self.L0, self.U0, self.L, self.U, alpha, self.r_n, self.eps_n)
+                    if high - low <= 2 * saved[0]:
+                        break
+                    tol_a, tol_r = tol_a / 10, tol_r / 10
+                    self.abs_tol, self.rel_tol = tol_a, tol_r
+                    if self.U0 - self.L0 > tol_a:
+                        self._certify()
+                while True:
+                    q_l, q_u = quantile_band(self.L, self.U, alpha)
+                    hot = np.flatnonzero((self.U >= q_l) & (self.L <= q_u) & (self.tol_full > tol_a))
+                    if hot.size == 0:
+                        break
+                    self.solve_draws(np.sort(hot[np.argsort(-self.U[hot], kind="stable")[:batch]]), stops=False)
+        finally:
+            self.abs_tol, self.rel_tol = saved
+        low, high, q = ci_lower(self.L0, self.U0, self.L, self.U, alpha, self.r_n, self.eps_n)
+        res = Interval(lower=low, lower_bracket=(low, high), lower_clipped=max(0.0, low), upper=math.inf,
+                       alpha=alpha, q=q, reject=low > 0, n_solved=int(np.isfinite(self.tol_full).sum()) - n0,
+                       time=time.perf_counter() - t0)
+        self.results["confidence_interval"][repr(alpha)] = asdict(res)
+        self._save_checkpoint()
+        return res
+
+    def distance_interval(self, alpha=0.05):
+        """The certified two-sided interval [max(0, L0 - c), U0 + c], c the (1 - alpha)-quantile of
+        ||p_b - p_hat|| (solver/inference/bootstrap.py:242-255): p_hat's certificate and the screen's
+        pass over the draws (on the GPU), no draw solved."""
+        alpha, t0 = check_alpha(alpha), time.perf_counter()
+        self._start()
+        if getattr(self, "dev", None) is None:
+            self.dev, _ = self._draw_rows().screen(None, self.eps_n * self.r_n)
+        lower, upper, c = distance_interval(self.L0, self.U0, self.dev, alpha)
+        res = DistanceInterval(lower=lower, upper=upper, alpha=alpha, half_width=c, dist_hat=(self.L0, self.U0),
+                               reject=lower > 0, time=time.perf_counter() - t0)
+        self.results["distance_interval"][repr(alpha)] = asdict(res)
+        self._save_checkpoint()
+        return res
+
     def p_value(self, alpha=0.05, max_draws=None, group=None):
         """The test's p-value. Under torch.distributed (group: a process group, or the default one
         when it is initialized) every rank certifies p_hat on its own GPU, takes rank 0's band,
@@ -454,10 +575,7 @@ class Bootstrap:
             self._certify()
             if world > 1:
                 self.L0, self.U0 = _broadcast_band(self.L0, self.U0, group)
-        if not self.screened:
-            if self.session.fit is None:          # resumed before the screen: certify again
-                self._certify()
-            self._screen()
+        self._start()
         if self.U0 > ZERO:
             dec = decide(self.L, self.U, *self.tau)
             todo = np.flatnonzero((dec == UNDECIDED) & ~self.solved)

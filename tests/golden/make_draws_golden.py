@@ -4,7 +4,8 @@
 
 It imports solver/inference/draws.py from the path given (read-only, never copied): for a seeded
 respondent panel (rumb.instances.panel_instance, n = 8) it records the reference's weight rows and
-every draw's rows (Draws.rows, solver/inference/draws.py:151-159,247-285) for both weight schemes.
+every draw's rows (Draws.rows, solver/inference/draws.py:151-159,247-285) for both weight schemes,
+and the interval formulas (solver/inference/hong_li.py:81-107) on seeded brackets.
 The tests compare the library's draws (host builder and GPU kernel) against this file; nothing at
 test time reads the reference itself.
 """
@@ -31,6 +32,18 @@ def main(ref_root):
         d = RD.Draws(panel, m, a, p, B=12, weights=weights, seed=5)
         out["W_" + weights] = np.asarray(d.W, dtype=np.float64)
         out["rows_" + weights] = np.asarray(d.rows(np.arange(12)), dtype=np.float64)
+    # the interval formulas (solver/inference/hong_li.py:81-107) on seeded brackets
+    from solver.inference import hong_li as HL
+    rng = np.random.default_rng(9)
+    L = rng.random(200) * 3.0
+    U = L + rng.random(200) * 0.5
+    dev = rng.random(200)
+    out["hl_L"], out["hl_U"], out["hl_dev"] = L, U, dev
+    for j, alpha in enumerate((0.05, 0.1, 0.5)):
+        low, high, q = HL.ci_lower(1.2, 1.3, L, U, alpha, 22.8, 0.124)
+        out["hl_ci_%d" % j] = np.array([low, high, q[0], q[1]])
+        out["hl_di_%d" % j] = np.array(HL.distance_interval(1.2, 1.3, dev, alpha))
+        out["hl_band_%d" % j] = np.array(HL.quantile_band(L, U, alpha))
     np.savez_compressed(os.path.join(HERE, "draws.npz"), **out)
     print("wrote", os.path.join(HERE, "draws.npz"))
 

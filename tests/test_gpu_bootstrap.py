@@ -33,3 +33,30 @@ def test_batched_and_sequential_bootstrap_agree():
     assert r1.n_solved == todo.size
     # every bracket of the batch contains the one-at-a-time bracket's distance
     assert np.all(b1.L <= b2.U + 1e-9) and np.all(b2.L <= b1.U + 1e-9)
+
+
+def test_distance_and_confidence_intervals():
+    """distance_interval needs only the screen's norms (equal to the host's); confidence_interval
+    solves to tolerance every draw left in the final quantile band, and the lower end from every
+    draw solved lies in its reported bracket."""
+    n = 10
+    panel, (m, a, p) = panel_instance(n, 0.3, 80, 8, 5, seed=7)
+    rum = RUM(m, a, p, num_alternatives=n)
+    b = rum.bootstrap(panel=panel, B=24, weights="multinomial", seed=1, method="bm_admm",
+                      method_args={"dtype": "float64"})
+    alpha = 0.1
+    di = b.distance_interval(alpha)
+    rows = b.draws.rows(np.arange(24))
+    dev = np.sqrt(np.einsum("ij,ij->i", rows - b.p_hat, rows - b.p_hat))
+    np.testing.assert_allclose(b.dev, dev, rtol=1e-12, atol=0)
+    c = float(np.quantile(b.dev, 1 - alpha))
+    assert di.half_width == c and di.lower == max(0.0, b.L0 - c) and di.upper == b.U0 + c
+    ci = b.confidence_interval(alpha)
+    assert ci.lower <= ci.lower_bracket[1] and ci.upper == np.inf
+    q_l, q_u = BS.quantile_band(b.L, b.U, alpha)
+    hot = (b.U >= q_l) & (b.L <= q_u)
+    assert np.all(b.tol_full[hot] <= b.abs_tol)
+    # every draw solved to tolerance: the lower end then lies in the bracket
+    b.solve_draws(np.arange(24), stops=False)
+    low, high, _ = BS.ci_lower(b.L0, b.U0, b.L, b.U, alpha, b.r_n, b.eps_n)
+    assert ci.lower - 1e-9 <= low <= ci.lower_bracket[1] + 1e-9

@@ -137,6 +137,18 @@ def test_draws_match_reference_golden():
         np.testing.assert_array_equal(d.rows(np.arange(12)), g["rows_" + w])
 
 
+def test_interval_formulas_match_reference_golden():
+    from rumb import bootstrap as BS
+    g = np.load(os.path.join(GOLD, "draws.npz"))
+    for j, alpha in enumerate((0.05, 0.1, 0.5)):
+        low, high, q = BS.ci_lower(1.2, 1.3, g["hl_L"], g["hl_U"], alpha, 22.8, 0.124)
+        np.testing.assert_array_equal([low, high, q[0], q[1]], g["hl_ci_%d" % j])
+        np.testing.assert_array_equal(BS.distance_interval(1.2, 1.3, g["hl_dev"], alpha), g["hl_di_%d" % j])
+        np.testing.assert_array_equal(BS.quantile_band(g["hl_L"], g["hl_U"], alpha), g["hl_band_%d" % j])
+    with pytest.raises(ValueError):
+        BS.check_alpha(1.0)
+
+
 def test_flow_cg_lower_bound_layout():
     """The reference's choice of the final lower bound's form by device memory: the float64 slab,
     else two float64 lattice layers, else the pricing bound."""
