@@ -92,6 +92,13 @@ def check_alpha(alpha):
     return alpha
 
 
+def locked(n_above, n_open, B, alpha):
+    """Whether the decision at alpha can no longer change while n_open draws are undecided or
+    unsolved (solver/inference/hong_li.py:74-78): counting all of them above still rejects, or the
+    draws certified above already exceed alpha."""
+    return (n_above + n_open) / B <= alpha or n_above / B > alpha
+
+
 def quantile_band(L, U, alpha):
     """(Q(L), Q(U)): the (1 - alpha)-quantile of the draws' distances lies between these
     (solver/inference/hong_li.py:102-107); only a draw whose bracket overlaps it moves either end."""
@@ -190,6 +197,8 @@ class PValue:
     dist_hat: tuple
     time: float
     draws_per_s: float
+    T: tuple = ()               # (r_n L0, r_n U0): the test statistic's bracket
+    stopped_early: bool = False # stop_when_decided ended the solves with draws still open
 
 
 @dataclass
@@ -564,11 +573,14 @@ class Bootstrap:
         self._save_checkpoint()
         return res
 
-    def p_value(self, alpha=0.05, max_draws=None, group=None):
-        """The test's p-value. Under torch.distributed (group: a process group, or the default one
-        when it is initialized) every rank certifies p_hat on its own GPU, takes rank 0's band,
-        solves every world-th open draw starting at its rank, and one all_gather of (L, U, solved)
-        gives every rank the whole record; draws are independent, so nothing else is exchanged."""
+    def p_value(self, alpha=0.05, stop_when_decided=False, max_draws=None, group=None):
+        """The test's p-value. stop_when_decided: solve the open draws in chunks and stop once the
+        decision at alpha is locked (the remaining draws cannot change it; one process only).
+        Under torch.distributed (group: a process group, or the default one when it is initialized)
+        every rank certifies p_hat on its own GPU, takes rank 0's band, solves every world-th open
+        draw starting at its rank, and one all_gather of (L, U, solved) gives every rank the whole
+        record; draws are independent, so nothing else is exchanged."""
+        alpha = check_alpha(alpha)
         t0 = time.perf_counter()
         rank, world, group = _dist(group)
         if self.L0 is None:
@@ -582,7 +594,14 @@ class Bootstrap:
             if max_draws is not None:
                 todo = todo[:max_draws]
             mine = todo[rank::world] if world > 1 else todo
-            if mine.size:
+            if stop_when_decided and world == 1:
+                chunk = max(64, int(self.batch_slots or 0))
+                for lo in range(0, mine.size, chunk):
+                    dec = decide(self.L, self.U, *self.tau)
+                    if locked(int((dec == ABOVE).sum()), int((dec == UNDECIDED).sum()), self.B, alpha):
+                        break
+                    self.solve_draws(mine[lo:lo + chunk])
+            elif mine.size:
                 self.solve_draws(mine)
             if world > 1:
                 self.L, self.U, self.solved = _gather_record(self.L, self.U, self.solved, group)
@@ -595,4 +614,6 @@ class Bootstrap:
                       certain=p_hi <= alpha or p_lo > alpha, n_below=int((dec == BELOW).sum()), n_above=above,
                       n_undecided=und, n_screened=self.n_screened, n_solved=solved, B=self.B, tau=self.tau,
                       dist_hat=(self.L0, self.U0), time=time.perf_counter() - t0,
-                      draws_per_s=solved / self.time["solve"] if self.time["solve"] > 0 else float("nan"))
+                      draws_per_s=solved / self.time["solve"] if self.time["solve"] > 0 else float("nan"),
+                      T=(self.r_n * self.L0, self.r_n * self.U0),
+                      stopped_early=bool(stop_when_decided and und > 0 and locked(above, und, self.B, alpha)))

@@ -44,6 +44,9 @@ def main(ref_root):
         out["hl_ci_%d" % j] = np.array([low, high, q[0], q[1]])
         out["hl_di_%d" % j] = np.array(HL.distance_interval(1.2, 1.3, dev, alpha))
         out["hl_band_%d" % j] = np.array(HL.quantile_band(L, U, alpha))
+    grid = [(a_, o_, 100, al) for a_ in (0, 3, 5, 9) for o_ in (0, 2, 6) for al in (0.05, 0.1)]
+    out["hl_locked_in"] = np.array(grid, dtype=np.float64)
+    out["hl_locked"] = np.array([HL.locked(int(a_), int(o_), int(b_), al) for a_, o_, b_, al in grid])
     np.savez_compressed(os.path.join(HERE, "draws.npz"), **out)
     print("wrote", os.path.join(HERE, "draws.npz"))
 

@@ -16,7 +16,7 @@ B = 41
 
 def _fake(rank_u0=None):
     b = object.__new__(BS.Bootstrap)
-    b.B, b.s, b.n_screened = B, 2.0, 0
+    b.B, b.s, b.r_n, b.n_screened = B, 2.0, 4.0, 0
     b.L, b.U = np.zeros(B), np.full(B, np.inf)
     b.solved = np.zeros(B, dtype=bool)
     b.L0 = b.U0 = None

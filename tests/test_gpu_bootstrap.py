@@ -60,3 +60,15 @@ def test_distance_and_confidence_intervals():
     b.solve_draws(np.arange(24), stops=False)
     low, high, _ = BS.ci_lower(b.L0, b.U0, b.L, b.U, alpha, b.r_n, b.eps_n)
     assert ci.lower - 1e-9 <= low <= ci.lower_bracket[1] + 1e-9
+
+
+def test_p_value_stop_when_decided():
+    """Stopping once the decision is locked gives the full run's decision with no more solves."""
+    n = 10
+    panel, (m, a, p) = panel_instance(n, 0.3, 80, 8, 5, seed=7)
+    rum = RUM(m, a, p, num_alternatives=n)
+    kw = dict(panel=panel, B=24, weights="multinomial", seed=1, method="bm_admm", method_args={"dtype": "float64"})
+    full = rum.bootstrap(**kw).p_value(0.1)
+    early = rum.bootstrap(**kw).p_value(0.1, stop_when_decided=True)
+    assert early.reject == full.reject and early.n_solved <= full.n_solved
+    assert early.T == (early.dist_hat[0] * np.sqrt(80), early.dist_hat[1] * np.sqrt(80))

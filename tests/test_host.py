@@ -145,6 +145,8 @@ def test_interval_formulas_match_reference_golden():
         np.testing.assert_array_equal([low, high, q[0], q[1]], g["hl_ci_%d" % j])
         np.testing.assert_array_equal(BS.distance_interval(1.2, 1.3, g["hl_dev"], alpha), g["hl_di_%d" % j])
         np.testing.assert_array_equal(BS.quantile_band(g["hl_L"], g["hl_U"], alpha), g["hl_band_%d" % j])
+    for (a_, o_, b_, al), want in zip(g["hl_locked_in"], g["hl_locked"]):
+        assert BS.locked(int(a_), int(o_), int(b_), al) == bool(want)
     with pytest.raises(ValueError):
         BS.check_alpha(1.0)
 
