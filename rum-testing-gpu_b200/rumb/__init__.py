@@ -6,5 +6,10 @@ host side, with the reference's interface:
 
     from rumb import RUM
     res = RUM(menu, alternative, p_hat).calculate_distance(method="bm_admm")
+
+    from rumb import cells_from_panel              # rum's rows from a panel / replies table
+    rum = RUM(*cells_from_panel(panel, 25), num_alternatives=25)
+    pv = rum.bootstrap(panel=panel).p_value()
 """
 from .rum_solver import RUM, Result, Session  # noqa: F401
+from .draws import cells_from_panel  # noqa: F401

@@ -41,10 +41,10 @@ import numpy as np
 import scipy.sparse as sp
 
 from . import defaults
+from .draws import Draws, MenuDraws, cells_from_panel  # noqa: F401  (re-exported)
 
 BELOW, ABOVE, UNDECIDED = 0, 1, 2
 ZERO = 1e-9
-REDRAW_ROUNDS = 10000
 VERSION = 1                      # the record format's version (solver/inference/bootstrap.py:48)
 NEVER = 127                      # exit_flag of a draw that was never solved
 # a batched draw's stop reason as the Session's exit flag (1 tol, 5 threshold, 0 time, -1 iters,
@@ -124,61 +124,6 @@ def distance_interval(L0, U0, dev, alpha):
     return max(0.0, L0 - c), U0 + c, c
 
 
-class Draws:
-    """B resampled p_hat's from a respondent panel (respondent, menu, chosen columns)."""
-
-    def __init__(self, panel, menu, alternative, p_hat, B, weights="multinomial_reject", seed=0):
-        if weights not in ("multinomial", "multinomial_reject"):
-            raise ValueError("weights must be 'multinomial' or 'multinomial_reject'")
-        resp = np.asarray(panel["respondent"])
-        pm = np.asarray(panel["menu"], dtype=np.int64)
-        pc = np.asarray(panel["chosen"], dtype=np.int64)
-        _, codes = np.unique(resp, return_inverse=True)
-        codes = codes.astype(np.int64)
-        self.input_fingerprint = hashlib.sha256(codes.tobytes() + pm.tobytes() + pc.tobytes()).hexdigest()[:16]
-        R = int(codes.max()) + 1
-        menu, alternative = np.asarray(menu, dtype=np.int64), np.asarray(alternative, dtype=np.int64)
-        M = menu.size
-        rum_menus, row_menu = np.unique(menu, return_inverse=True)
-        m = np.minimum(np.searchsorted(rum_menus, pm), rum_menus.size - 1)
-        used = rum_menus[m] == pm
-        row_key = row_menu * 64 + alternative
-        order = np.argsort(row_key)
-        key = m * 64 + pc
-        pos = np.minimum(np.searchsorted(row_key[order], key), M - 1)
-        hit = used & (row_key[order][pos] == key)
-        self.rows_unused = int((~used).sum())       # panel rows on menus that have no rum row
-        self.offered = sp.csr_array((np.ones(int(used.sum())), (codes[used], m[used])), shape=(R, rum_menus.size))
-        self.chose = sp.csr_array((np.ones(int(hit.sum())), (codes[hit], order[pos[hit]])), shape=(R, M))
-        self.row_menu = row_menu
-        self.p_hat = np.asarray(p_hat, dtype=np.float64)
-        self.B, self.R, self.M, self.weights, self.seed = int(B), R, M, weights, seed
-        rng = np.random.default_rng(seed)
-        W = rng.multinomial(R, np.ones(R) / R, size=self.B).astype(np.float64)
-        self.n_redraws = 0
-        if weights == "multinomial_reject":
-            for _ in range(REDRAW_ROUNDS):
-                bad = np.any(np.asarray((sp.csr_array(W) @ self.offered).todense()) <= 0, axis=1)
-                if not bad.any():
-                    break
-                self.n_redraws += int(bad.sum())
-                W[bad] = rng.multinomial(R, np.ones(R) / R, size=int(bad.sum())).astype(np.float64)
-        self.W = W
-
-    def summary(self):
-        """The record's account of the panel and its draws."""
-        return dict(respondents=self.R, rows_unused=self.rows_unused, redraws=self.n_redraws,
-                    emptied_menu_draws=None)
-
-    def rows(self, idx):
-        """The draws idx as a (len(idx), M) array: weighted shares, p_hat where a menu went unseen."""
-        Wb = sp.csr_array(self.W[np.asarray(idx, dtype=np.int64)])
-        seen = np.asarray((Wb @ self.offered).todense())[:, self.row_menu]
-        chose = np.asarray((Wb @ self.chose).todense())
-        empty = seen <= 0
-        return np.where(empty, self.p_hat, chose / np.where(empty, 1.0, seen))
-
-
 @dataclass
 class PValue:
     p: float
@@ -227,6 +172,28 @@ class DistanceInterval:
     time: float
 
 
+class _HostDrawRows:
+    """rows / screen of the GPU draws, computed block by block on the host as the reference does."""
+
+    def __init__(self, draws, p_hat):
+        self.d, self.p_hat = draws, np.asarray(p_hat, dtype=np.float64)
+
+    def rows(self, idx, scale=None):
+        rows = self.d.rows(idx)
+        return rows if scale is None else self.p_hat + scale * (rows - self.p_hat)
+
+    def screen(self, fit, scale):
+        dev = np.empty(self.d.B)
+        ub = None if fit is None else np.empty(self.d.B)
+        for lo, hi, block in self.d.blocks():
+            D = block - self.p_hat
+            dev[lo:hi] = np.sqrt(np.einsum("ij,ij->i", D, D))
+            if fit is not None:
+                E = (self.p_hat + scale * (block - self.p_hat)) - fit
+                ub[lo:hi] = np.sqrt(np.einsum("ij,ij->i", E, E))
+        return dev, ub
+
+
 def _dist(group):
     """(rank, world, group) of the process group the draws are sharded over (1 rank without one)."""
     try:
@@ -268,22 +235,33 @@ def _gather_record(L, U, solved, group):
 
 class Bootstrap:
     def __init__(self, rum, n=None, panel=None, replies=None, B=None, weights=None, seed=None, r_n=None, eps_n=None,
-                 method=None, method_args=None, abs_tol=None, rel_tol=None, max_time=None, draw_time=None,
-                 batch_slots=0, verbose=False, learned=False, train_draws=512, mlp_hidden=(1024, 1024, 1024),
-                 mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=False, seed_net=0, checkpoint=None):
+                 method=None, method_args=None, abs_tol=None, rel_tol=None, refine=None, max_time=None,
+                 draw_time=None, batch_slots=0, verbose=False, learned=False, train_draws=512,
+                 mlp_hidden=(1024, 1024, 1024), mlp_epochs=100, mlp_batch=128, mlp_lr=1e-3, y0_state=False,
+                 seed_net=0, checkpoint=None):
         d = defaults.BOOTSTRAP
-        if panel is None or replies is not None:
-            raise ValueError("this bootstrap takes a respondent panel (panel=)")
+        pick = lambda value, key: d[key] if value is None else value      # noqa: E731
         self.rum, self.p_hat = rum, rum.choice_probability
-        self.B = int(d["B"] if B is None else B)
-        self.abs_tol = float(d["abs_tol"] if abs_tol is None else abs_tol)
-        self.rel_tol = float(d["rel_tol"] if rel_tol is None else rel_tol)
-        self.max_time = float(d["max_time"] if max_time is None else max_time)
-        self.draw_time = float(d["draw_time"] if draw_time is None else draw_time)
-        self.draws = Draws(panel, rum.menu, rum.alternative, self.p_hat, self.B,
-                           d["weights"] if weights is None else weights, d["seed"] if seed is None else seed)
-        self.n = self.draws.R if n is None else int(n)
+        self.B = int(pick(B, "B"))
+        self.abs_tol, self.rel_tol = float(pick(abs_tol, "abs_tol")), float(pick(rel_tol, "rel_tol"))
+        self.refine = int(pick(refine, "refine"))
+        self.max_time = float(pick(max_time, "max_time"))
+        self.draw_time = float(pick(draw_time, "draw_time"))
+        if self.abs_tol < 0 or self.rel_tol < 0 or self.abs_tol + self.rel_tol == 0 or self.refine < 0:
+            raise ValueError("abs_tol and rel_tol must be >= 0 and not both 0, and refine >= 0")
+        if (panel is None) == (replies is None):
+            raise ValueError("give the choices behind p_hat once: panel= (respondent, menu, chosen; respondents are "
+                             "resampled) or replies= (menu, chosen; each menu's replies are resampled)")
+        if panel is not None:
+            self.draws = Draws(panel, rum.menu, rum.alternative, self.p_hat, self.B, pick(weights, "weights"),
+                               pick(seed, "seed"))
+        elif weights not in (None, MenuDraws.weights):
+            raise ValueError("weights = %r is for panel=; replies= are resampled menu by menu" % (weights,))
+        else:
+            self.draws = MenuDraws(replies, rum.menu, rum.alternative, self.p_hat, self.B, pick(seed, "seed"))
+        self.n = int(self.draws.default_n if n is None else n)
         self.r_n, self.eps_n, self.s = scaling(self.n, r_n, eps_n)
+        self.draws.check_n(self.n)
         self.session = rum.session(method=method, method_args=method_args)
         self.batch_slots = batch_slots
         self.L, self.U = np.zeros(self.B), np.full(self.B, np.inf)
@@ -299,10 +277,10 @@ class Bootstrap:
         # the record (solver/inference/bootstrap.py:159-180,356-400): settings, fingerprints and
         # per draw the bracket, the tightest tolerances asked and the last exit flag
         self.method, self.method_args = method, method_args
-        self.settings = dict(n=self.n, input="panel", B=self.B, weights=self.draws.weights, seed=self.draws.seed,
-                             r_n=self.r_n, eps_n=self.eps_n, method=method, method_args=method_args,
-                             abs_tol=self.abs_tol, rel_tol=self.rel_tol, refine=d["refine"], max_time=self.max_time,
-                             draw_time=self.draw_time, weighted=False)
+        self.settings = dict(n=self.n, input=self.draws.input, B=self.B, weights=self.draws.weights,
+                             seed=self.draws.seed, r_n=self.r_n, eps_n=self.eps_n, method=method,
+                             method_args=method_args, abs_tol=self.abs_tol, rel_tol=self.rel_tol, refine=self.refine,
+                             max_time=self.max_time, draw_time=self.draw_time, weighted=False)
         self.fingerprints = {"data": _sha(np.column_stack([np.asarray(rum.menu, dtype=np.float64),
                                                            np.asarray(rum.alternative, dtype=np.float64),
                                                            self.p_hat])),
@@ -345,12 +323,17 @@ class Bootstrap:
             self._screen()
 
     def _draw_rows(self):
-        """The draws on the GPU (built on first use): rows and the screen's norms."""
+        """The draws' rows and the screen's norms (built on first use): on the GPU for integer panel
+        weights, whose counts are exact in any order; with the reference's block arithmetic on the
+        host for real weights and replies, whose float64 sums depend on their order."""
         if getattr(self, "_gdraws", None) is None:
-            from . import _lib
-            from .rum_solver import context
             d = self.draws
-            self._gdraws = _lib.DrawRows(context(), d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+            if getattr(d, "integer_weights", False):
+                from . import _lib
+                from .rum_solver import context
+                self._gdraws = _lib.DrawRows(context(), d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+            else:
+                self._gdraws = _HostDrawRows(d, self.p_hat)
         return self._gdraws
 
     def _screen(self):
@@ -360,6 +343,7 @@ class Bootstrap:
         self.dev, ub = self._draw_rows().screen(fit, self.eps_n * self.r_n)
         if ub is not None:
             self.U = np.minimum(self.U, ub)
+        self.fingerprints["draws"] = self.draws.fingerprint      # set by a host pass over the blocks
         self.n_screened = int((self.U < self.tau[0]).sum())
         self.screened = True
         self.time["screen"] += time.perf_counter() - t0
@@ -533,7 +517,7 @@ class Bootstrap:
         saved = (self.abs_tol, self.rel_tol)
         tol_a, tol_r = saved
         try:
-            for rnd in range(int(self.settings["refine"]) + 1):
+            for rnd in range(self.refine + 1):
                 if rnd:
                     low, high, _ = ci_lower(self.L0, self.U0, self.L, self.U, alpha, self.r_n, self.eps_n)
                     if high - low <= 2 * saved[0]:

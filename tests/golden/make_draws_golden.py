@@ -4,7 +4,8 @@
 
 It imports solver/inference/draws.py from the path given (read-only, never copied): for a seeded
 respondent panel (rumb.instances.panel_instance, n = 8) it records the reference's weight rows and
-every draw's rows (Draws.rows, solver/inference/draws.py:151-159,247-285) for both weight schemes,
+every draw's rows (Draws.rows, solver/inference/draws.py:151-159,247-285) for every weight scheme,
+a replies table's draws (MenuDraws) and cells (cells_from_panel), three refusal messages,
 and the interval formulas (solver/inference/hong_li.py:81-107) on seeded brackets.
 The tests compare the library's draws (host builder and GPU kernel) against this file; nothing at
 test time reads the reference itself.
@@ -28,10 +29,29 @@ def main(ref_root):
                panel_chosen=np.asarray(panel["chosen"], dtype=np.int64),
                menu=np.asarray(m, dtype=np.int64), alternative=np.asarray(a, dtype=np.int64),
                p_hat=np.asarray(p, dtype=np.float64))
-    for weights in ("multinomial", "multinomial_reject"):
+    for weights in RD.WEIGHTS:
         d = RD.Draws(panel, m, a, p, B=12, weights=weights, seed=5)
         out["W_" + weights] = np.asarray(d.W, dtype=np.float64)
         out["rows_" + weights] = np.asarray(d.rows(np.arange(12)), dtype=np.float64)
+    # a replies table (the panel without respondents) and its own rows
+    replies = dict(menu=out["panel_menu"], chosen=out["panel_chosen"])
+    rm, ra, rp = RD.cells_from_panel(replies, 8)
+    out["rep_menu"], out["rep_alt"], out["rep_p"] = rm, ra, rp
+    md = RD.MenuDraws(replies, rm, ra, rp, B=12, seed=5)
+    out["rows_replies"] = np.asarray(md.rows(np.arange(12)), dtype=np.float64)
+    am, aa, ap = RD.cells_from_panel(panel, 8, alternatives=[0])
+    out["alt0_menu"], out["alt0_alt"], out["alt0_p"] = am, aa, ap
+    # the messages of three refusals
+    msgs = []
+    for bad in (lambda: RD.Draws(panel, m, a, p + 0.01, B=2),
+                lambda: RD.Draws(dict(respondent=out["panel_respondent"], menu=out["panel_menu"]), m, a, p, B=2),
+                lambda: RD.Draws(panel, np.r_[m, 255], np.r_[a, 0], np.r_[p, 0.5], B=2)):
+        try:
+            bad()
+            msgs.append("")
+        except ValueError as e:
+            msgs.append(str(e))
+    out["errors"] = np.array(msgs)
     # the interval formulas (solver/inference/hong_li.py:81-107) on seeded brackets
     from solver.inference import hong_li as HL
     rng = np.random.default_rng(9)

@@ -72,3 +72,28 @@ def test_p_value_stop_when_decided():
     early = rum.bootstrap(**kw).p_value(0.1, stop_when_decided=True)
     assert early.reject == full.reject and early.n_solved <= full.n_solved
     assert early.T == (early.dist_hat[0] * np.sqrt(80), early.dist_hat[1] * np.sqrt(80))
+
+
+@pytest.mark.parametrize("source", ["poisson", "mammen", "exponential", "replies"])
+def test_bootstrap_weight_schemes_and_replies(source):
+    """Every weight scheme and the replies table run the whole test: integer weights through the
+    GPU draws, real weights and replies through the host blocks; the screen's bounds are real
+    distances (U_b >= the certified lower bound of a solved draw)."""
+    from rumb import cells_from_panel
+    n = 10
+    panel, _ = panel_instance(n, 0.3, 80, 8, 5, seed=7)
+    if source == "replies":
+        table = dict(menu=panel["menu"], chosen=panel["chosen"])
+        rum = RUM(*cells_from_panel(table, n), num_alternatives=n)
+        b = rum.bootstrap(replies=table, B=16, seed=1, method="bm_admm", method_args={"dtype": "float64"})
+    else:
+        rum = RUM(*cells_from_panel(panel, n), num_alternatives=n)
+        b = rum.bootstrap(panel=panel, B=16, weights=source, seed=1, method="bm_admm",
+                          method_args={"dtype": "float64"})
+    pv = b.p_value(0.1)
+    assert 0.0 <= pv.p <= 1.0 and pv.B == 16
+    assert b.draws.integer_weights == (source == "poisson")
+    P = b._draw_rows().rows(np.arange(16), b.eps_n * b.r_n)
+    np.testing.assert_array_equal(P, BS.perturb(b.p_hat, b.draws.rows(np.arange(16)), b.r_n, b.eps_n))
+    solved = np.flatnonzero(b.solved)
+    assert np.all(b.L[solved] <= b.U[solved] + 1e-9)

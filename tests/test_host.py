@@ -126,15 +126,35 @@ def test_gram_and_pout_maintainers():
 
 
 def test_draws_match_reference_golden():
-    """The bootstrap's draws (weights and every draw's rows) equal the reference's own Draws bit for
-    bit, both weight schemes (tests/golden/make_draws_golden.py)."""
-    from rumb import bootstrap as BS
+    """The bootstrap's draws equal the reference's own (tests/golden/make_draws_golden.py) bit for
+    bit: every weight scheme's weights and rows, a replies table's draws and cells, the cells of one
+    alternative, and the refusals' messages."""
+    from rumb import draws as D
     g = np.load(os.path.join(GOLD, "draws.npz"))
     panel = dict(respondent=g["panel_respondent"], menu=g["panel_menu"], chosen=g["panel_chosen"])
-    for w in ("multinomial", "multinomial_reject"):
-        d = BS.Draws(panel, g["menu"], g["alternative"], g["p_hat"], B=12, weights=w, seed=5)
+    for w in D.WEIGHTS:
+        d = D.Draws(panel, g["menu"], g["alternative"], g["p_hat"], B=12, weights=w, seed=5)
         np.testing.assert_array_equal(d.W, g["W_" + w])
         np.testing.assert_array_equal(d.rows(np.arange(12)), g["rows_" + w])
+        np.testing.assert_array_equal(d.rows(np.array([11, 0, 5])), g["rows_" + w][[11, 0, 5]])
+    replies = dict(menu=g["panel_menu"], chosen=g["panel_chosen"])
+    rm, ra, rp = D.cells_from_panel(replies, 8)
+    np.testing.assert_array_equal(rm, g["rep_menu"])
+    np.testing.assert_array_equal(ra, g["rep_alt"])
+    np.testing.assert_array_equal(rp, g["rep_p"])
+    md = D.MenuDraws(replies, rm, ra, rp, B=12, seed=5)
+    np.testing.assert_array_equal(md.rows(np.arange(12)), g["rows_replies"])
+    am, aa, ap = D.cells_from_panel(panel, 8, alternatives=[0])
+    np.testing.assert_array_equal(am, g["alt0_menu"])
+    np.testing.assert_array_equal(ap, g["alt0_p"])
+    m, a, p = g["menu"], g["alternative"], g["p_hat"]
+    bad = (lambda: D.Draws(panel, m, a, p + 0.01, B=2),
+           lambda: D.Draws(dict(respondent=g["panel_respondent"], menu=g["panel_menu"]), m, a, p, B=2),
+           lambda: D.Draws(panel, np.r_[m, 255], np.r_[a, 0], np.r_[p, 0.5], B=2))
+    for f, msg in zip(bad, g["errors"]):
+        with pytest.raises(ValueError) as e:
+            f()
+        assert str(e.value) == str(msg)
 
 
 def test_interval_formulas_match_reference_golden():
@@ -260,6 +280,7 @@ def test_bootstrap_draws_and_formulas():
     assert rows.shape == (20, p.size)
     # a draw with every respondent weighted once reproduces p_hat
     d.W[0] = 1.0
+    d._cache = (None, None, 0)                  # the weights changed under the kept block
     np.testing.assert_allclose(d.rows([0])[0], p, atol=1e-12)
     # shares stay shares
     sums = np.zeros((20, np.unique(m).size))
