@@ -284,7 +284,8 @@ class Bootstrap:
         self.fingerprints = {"data": _sha(np.column_stack([np.asarray(rum.menu, dtype=np.float64),
                                                            np.asarray(rum.alternative, dtype=np.float64),
                                                            self.p_hat])),
-                             "panel": self.draws.input_fingerprint, "draws": None}
+                             self.draws.input: self.draws.input_fingerprint, "draws": None}
+        self.certificates = []      # every certification of p_hat, as the reference records them
         self.tol_stop = np.full(self.B, np.inf)
         self.tol_full = np.full(self.B, np.inf)
         self.flag = np.full(self.B, NEVER, dtype=np.int8)
@@ -309,6 +310,10 @@ class Bootstrap:
                                keep=True)
         if not math.isfinite(r.ub):
             raise RuntimeError("p_hat could not be certified: %s (%s)" % (r.status, r.message))
+        self.certificates.append(dict(abs_tol=self.abs_tol, rel_tol=self.rel_tol, lb=r.lb, ub=r.ub,
+                                      exit_flag=r.exit_flag, status=r.status, message=r.message,
+                                      iterations=r.iterations, time=r.time, method=r.method,
+                                      method_args=r.method_args, machine=r.machine))
         self.L0 = r.lb if self.L0 is None else max(self.L0, r.lb)
         self.U0 = r.ub if self.U0 is None else min(self.U0, r.ub)
         self.time["certificate"] += time.perf_counter() - t0
@@ -466,11 +471,11 @@ class Bootstrap:
         s = self.session
         return dict(version=VERSION, settings=self.settings, fingerprints=self.fingerprints,
                     plan=dict(method=s.method, method_args=s.method_args, auto_reason=s.auto_reason),
-                    p_hat=dict(lb=self.L0, ub=self.U0, certificates=[]),
+                    p_hat=dict(lb=self.L0, ub=self.U0, certificates=getattr(self, "certificates", [])),
                     tau=None if self.L0 is None else list(self.tau),
                     scaling=dict(r_n=self.r_n, eps_n=self.eps_n, s=self.s),
                     screen=dict(done=self.screened, n_below=self.n_screened),
-                    panel=self.draws.summary(),
+                    **{self.draws.input: self.draws.summary()},
                     draws=dict(lb=self.L.tolist(), ub=self.U.tolist(), tol_stop=self.tol_stop.tolist(),
                                tol_full=self.tol_full.tolist(), exit_flag=self.flag.tolist()),
                     results=self.results, time=self.time, when=time.strftime("%Y-%m-%d %H:%M:%S"))
@@ -491,7 +496,8 @@ class Bootstrap:
         same = dict(version=rec.get("version") == VERSION,
                     settings=json.loads(json.dumps(self.settings, default=_plain)) == rec.get("settings"),
                     data=rec.get("fingerprints", {}).get("data") == self.fingerprints["data"],
-                    panel=rec.get("fingerprints", {}).get("panel") == self.fingerprints["panel"])
+                    **{self.draws.input: rec.get("fingerprints", {}).get(self.draws.input)
+                       == self.fingerprints[self.draws.input]})
         if not all(same.values()):
             raise ValueError("checkpoint %s belongs to another run (differs in: %s); delete it or pass another path"
                              % (path, ", ".join(k for k, v in same.items() if not v)))
@@ -504,6 +510,7 @@ class Bootstrap:
         self.L0, self.U0 = rec["p_hat"]["lb"], rec["p_hat"]["ub"]
         self.screened, self.n_screened = rec["screen"]["done"], rec["screen"]["n_below"]
         self.results, self.time = rec["results"], rec["time"]
+        self.certificates = rec["p_hat"].get("certificates", [])
 
     def confidence_interval(self, alpha=0.05):
         """The certified one-sided interval [lower, inf) (solver/inference/bootstrap.py:212-240):
@@ -594,10 +601,13 @@ class Bootstrap:
         und = int((dec == UNDECIDED).sum())
         p_lo, p_hi = above / self.B, (above + und) / self.B
         solved = int(self.solved.sum())
-        return PValue(p=p_hi, p_lo=p_lo, p_hi=p_hi, alpha=alpha, reject=p_hi <= alpha,
+        res = PValue(p=p_hi, p_lo=p_lo, p_hi=p_hi, alpha=alpha, reject=p_hi <= alpha,
                       certain=p_hi <= alpha or p_lo > alpha, n_below=int((dec == BELOW).sum()), n_above=above,
                       n_undecided=und, n_screened=self.n_screened, n_solved=solved, B=self.B, tau=self.tau,
                       dist_hat=(self.L0, self.U0), time=time.perf_counter() - t0,
                       draws_per_s=solved / self.time["solve"] if self.time["solve"] > 0 else float("nan"),
                       T=(self.r_n * self.L0, self.r_n * self.U0),
                       stopped_early=bool(stop_when_decided and und > 0 and locked(above, und, self.B, alpha)))
+        self.results.setdefault("p_value", {})[repr(alpha)] = asdict(res)
+        self._save_checkpoint()
+        return res

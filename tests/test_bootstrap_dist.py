@@ -23,6 +23,7 @@ def _fake(rank_u0=None):
     b.screened = False
     b.session = types.SimpleNamespace(fit=np.zeros(1))
     b.time = dict(certificate=0.0, screen=0.0, solve=0.0)
+    b.results, b.checkpoint = {"p_value": {}}, None
     b.seen = []
 
     def certify():
