@@ -320,3 +320,28 @@ def test_bootstrap_record_checkpoint_and_resume(fake_gpu, tmp_path):
     assert (r.L0, r.U0) == (0.5, 0.6) and r.screened and r.solved.sum() == 4
     with pytest.raises(ValueError, match="belongs to another run"):
         rum.bootstrap(panel=panel, B=12, weights="multinomial", seed=1, method="bm_admm", checkpoint=path)
+
+
+def test_bootstrap_inputs_refused(fake_gpu):
+    """The bootstrap's constructor refuses what the reference refuses: both tables or neither,
+    weights with replies, tolerances that cannot stop, an n that the replies cannot give."""
+    from rumb import cells_from_panel
+    panel, _ = panel_instance(8, 0.4, 30, 5, 3, seed=4)
+    replies = dict(menu=panel["menu"], chosen=panel["chosen"])
+    rum = rum_solver.RUM(*cells_from_panel(panel, 8), num_alternatives=8)
+    with pytest.raises(ValueError, match="give the choices behind p_hat once"):
+        rum.bootstrap(panel=panel, replies=replies, B=4)
+    with pytest.raises(ValueError, match="give the choices behind p_hat once"):
+        rum.bootstrap(B=4)
+    with pytest.raises(ValueError, match="not both 0"):
+        rum.bootstrap(panel=panel, B=4, abs_tol=0.0, rel_tol=0.0)
+    with pytest.raises(ValueError, match="n = 7, but the panel has 30 respondents"):
+        rum.bootstrap(panel=panel, B=4, n=7)
+    rr = rum_solver.RUM(*cells_from_panel(replies, 8), num_alternatives=8)
+    with pytest.raises(ValueError, match="is for panel="):
+        rr.bootstrap(replies=replies, B=4, weights="poisson")
+    b = rr.bootstrap(replies=replies, B=4)
+    assert b.settings["input"] == "replies" and b.n == b.draws.default_n
+    assert set(b.record()) >= {"replies", "p_hat", "draws", "results"}
+    with pytest.raises(ValueError, match="replies per menu"):
+        rr.bootstrap(replies=replies, B=4, n=10 ** 6)
