@@ -1,10 +1,9 @@
 """Hong and Li's bootstrap on the RUM distance, with the draws solved many at a time on the GPU.
 
-    from rumb import RUM
-    from rumb.instances import cells_from_panel
-    menu, alt, p_hat = cells_from_panel(n, panel["menu"], panel["chosen"])
+    from rumb import RUM, cells_from_panel
+    menu, alt, p_hat = cells_from_panel(panel, n)             # panel: respondent, menu, chosen
     boot = RUM(menu, alt, p_hat, num_alternatives=n).bootstrap(panel=panel, B=10000)
-    print(boot.p_value())
+    print(boot.p_value(), boot.confidence_interval(), boot.distance_interval())
 
 The reference's pipeline (solver/inference/bootstrap.py:182-335, solver/inference/hong_li.py,
 solver/inference/draws.py:161-290), with its formulas and decisions:
@@ -12,6 +11,8 @@ solver/inference/draws.py:161-290), with its formulas and decisions:
     certify   p_hat with a Session (one plan for every solve), keeping its state and fit:
               dist(p_hat) in [L0, U0]; the band tau = s [L0, U0], s = 1 + eps_n r_n
     screen    every draw P_b = p_hat + eps_n r_n (p_hat_b - p_hat): ||p_fit - P_b|| bounds dist(P_b)
+              (on the GPU for integer weights, rumb_draws_*; with the reference's host blocks for
+              real weights and replies)
     solve     the draws still open, warm from p_hat's state, each stopping once it clears the band
               (ub < tau_lo: below; lb >= tau_hi: above). bm_admm solves them together with
               rumb_bm_solve_batch (slots admitted by device memory, retired as they finish);
@@ -24,11 +25,13 @@ solver/inference/draws.py:161-290), with its formulas and decisions:
               at the prediction (certified whatever the prediction); y0_state=True also moves the
               start state's fitted cells there. A poor prediction costs iterations, never
               correctness
-    p-value   p = (#above + #undecided) / B
+    p-value   p = (#above + #undecided) / B (stop_when_decided: stop once the decision is locked)
+    intervals confidence_interval (draws solved to tolerance while they overlap the quantile band)
+              and distance_interval (p_hat's bracket widened by the quantile of ||p_b - p_hat||)
 
-Respondent weights: "multinomial" (R picks with replacement per draw) and "multinomial_reject"
-(redraw a weight row that leaves a menu unseen), drawn from numpy.random.default_rng(seed) in the
-reference's order.
+The draws (rumb.draws, solver/inference/draws.py): a panel's respondents resampled with the
+weights multinomial_reject, multinomial, exponential, poisson or mammen, or a replies table's
+menus resampled one by one, drawn in the reference's order from its seeds.
 """
 import hashlib
 import json
