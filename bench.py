@@ -265,13 +265,13 @@ def run_bootstrap(args, rank, batch_draws=8, single_draws=4):
     torch.cuda.synchronize()
     ts = time.perf_counter() - t0
     # the screen of 10,000 draws of this panel (rows, perturbation, ||P_b - p_fit|| and ||p_b - p_hat||):
-    # on the GPU over all draws, and the host builder (the reference's block builder) on a sample
+    # on the GPU over all draws, and the host builder (rumb.draws, block by block) on a sample
     from rumb import _lib
     from rumb.rum_solver import context
     D = BS.Draws(panel, m, a, p, B=10000, weights="multinomial", seed=0)
     r_n, eps_n, _ = BS.scaling(D.R)
     fit = boot.session.fit
-    gd = _lib.DrawRows(context(), D.W, D.offered, D.chose, D.row_menu, D.p_hat)
+    gd = _lib.DrawRows(context(), D.W, D.lists, D.p_hat)
     gd.screen(fit, eps_n * r_n)
     torch.cuda.synchronize()
     t0 = time.perf_counter()

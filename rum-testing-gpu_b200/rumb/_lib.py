@@ -496,26 +496,24 @@ class CgMaster:
 
 
 class DrawRows:
-    """Bootstrap draws on one GPU (see rumb_draws_create): W is B x R respondent weights; offered
-    and chose are the panel's (respondent x menu) and (respondent x row) count matrices (scipy
-    sparse); row_menu maps rows to menus."""
+    """Bootstrap draws on one GPU (see rumb_draws_create): W is the B x R respondent weights and
+    lists the panel's count lists (rumb.draws.CountLists: per menu the respondents offered it, per
+    row the respondents who chose it, each with its count, and every row's menu)."""
 
-    def __init__(self, ctx, W, offered, chose, row_menu, p_hat):
+    def __init__(self, ctx, W, lists, p_hat):
         W = np.ascontiguousarray(W, dtype=np.float64)
         B, R = W.shape
-        oT = offered.T.tocsr()
-        cT = chose.T.tocsr()
-        optr = np.ascontiguousarray(oT.indptr, dtype=np.int64)
-        oresp = np.ascontiguousarray(oT.indices, dtype=np.int32)
-        ocnt = np.ascontiguousarray(oT.data, dtype=np.float64)
-        cptr = np.ascontiguousarray(cT.indptr, dtype=np.int64)
-        cresp = np.ascontiguousarray(cT.indices, dtype=np.int32)
-        ccnt = np.ascontiguousarray(cT.data, dtype=np.float64)
-        row_menu = np.ascontiguousarray(row_menu, dtype=np.int32)
+        optr = np.ascontiguousarray(lists.menu_ptr, dtype=np.int64)
+        oresp = np.ascontiguousarray(lists.menu_resp, dtype=np.int32)
+        ocnt = np.ascontiguousarray(lists.menu_cnt, dtype=np.float64)
+        cptr = np.ascontiguousarray(lists.row_ptr, dtype=np.int64)
+        cresp = np.ascontiguousarray(lists.row_resp, dtype=np.int32)
+        ccnt = np.ascontiguousarray(lists.row_cnt, dtype=np.float64)
+        row_menu = np.ascontiguousarray(lists.row_menu, dtype=np.int32)
         p_hat = np.ascontiguousarray(p_hat, dtype=np.float64)
         self.B, self.R, self.M = int(B), int(R), int(p_hat.size)
         h = ctypes.c_void_p()
-        check(load().rumb_draws_create(ctx.h, self.B, self.R, self.M, int(oT.shape[0]), _p(W), _p(optr), _p(oresp),
+        check(load().rumb_draws_create(ctx.h, self.B, self.R, self.M, int(optr.size - 1), _p(W), _p(optr), _p(oresp),
                                        _p(ocnt), _p(cptr), _p(cresp), _p(ccnt), _p(row_menu), _p(p_hat),
                                        ctypes.byref(h)))
         self.h, self.ctx = h, ctx

@@ -332,14 +332,14 @@ class Bootstrap:
 
     def _draw_rows(self):
         """The draws' rows and the screen's norms (built on first use): on the GPU for integer panel
-        weights, whose counts are exact in any order; with the reference's block arithmetic on the
-        host for real weights and replies, whose float64 sums depend on their order."""
+        weights, whose counts are exact in any order; on the host (rumb.draws, block by block) for
+        real weights and replies."""
         if getattr(self, "_gdraws", None) is None:
             d = self.draws
             if getattr(d, "integer_weights", False):
                 from . import _lib
                 from .rum_solver import context
-                self._gdraws = _lib.DrawRows(context(), d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+                self._gdraws = _lib.DrawRows(context(), d.W, d.lists, d.p_hat)
             else:
                 self._gdraws = _HostDrawRows(d, self.p_hat)
         return self._gdraws

@@ -1,158 +1,284 @@
-"""The choices behind p_hat, and the bootstrap draws made from them (solver/inference/draws.py).
+"""Bootstrap draws of p_hat, built from the choices behind it (the reference's
+solver/inference/draws.py interface: the same tables, weight schemes, seeds and draws).
 
-Two tables, one row per choice (a DataFrame or a dict of equal-length columns):
+Input tables hold one row per choice, as a DataFrame or a dict of equal-length columns:
 
-    panel     respondent, menu, chosen: people who answered several menus; respondents are
-              resampled, so a respondent's answers move together (Draws)
-    replies   menu, chosen: every reply collected on its own; each menu's replies are resampled on
-              their own (MenuDraws)
+    panel     respondent, menu, chosen   respondents answered several menus and are resampled as a
+                                         whole (Draws)
+    replies   menu, chosen               independent replies, resampled menu by menu (MenuDraws)
 
-A menu is an integer bitmask (bit a = alternative a offered), chosen a member of it. rum's rows
-must be counted from the table (cells_from_panel builds them): p_hat(D, a) = #{rows with menu D
-and chosen a} / #{rows with menu D}.
+A menu is a bitmask of offered alternatives; `chosen` is one of its members. rum's rows are the
+table's shares, p_hat(D, a) = #(menu D, chose a) / #(menu D) (cells_from_panel builds them).
 
-Panel draws give respondent i a weight w_bi and count again,
-    p_hat_b(D, a) = sum_i w_bi #{i's rows: menu D, chosen a} / sum_i w_bi #{i's rows: menu D},
-with the weights drawn in the reference's order, seed for seed:
-    multinomial_reject   times i is picked in R draws with replacement; a draw that leaves a menu of
-                         rum unseen is drawn again (the default)
-    multinomial          the same without the redraw; an unseen menu keeps p_hat
-    exponential, poisson multiplier weights Exp(1) and Poisson(1)
-    mammen               the wild bootstrap: clip(p_hat + sum_i w_bi (chose_i - offered_i p_hat) / N_D, 0, 1)
-Replies draws: menu D's counts are Multinomial(N_D, the shares of D's replies), menu by menu.
+How a panel draw is built here. The panel is reduced once to two count lists in compressed form,
+respondents ascending within each list:
 
-The draws are rebuilt from what makes them a block at a time (at most BLOCK_BYTES of draws), with
-the reference's block size and its dense / sparse choice for the count matrices, so that real
-weights (exponential, mammen) give the reference's float64 sums; integer weights give exact counts
-in any order, which is what lets the GPU build those rows (rumb_draws_*).
+    menu lists   for each of rum's menus D: the respondents offered D and how many times
+    row lists    for each of rum's rows (D, a): the respondents who chose a from D and how many times
+
+A draw gives respondent i a weight w_i, and its row (D, a) is the share
+    sum over a's list of w_i count_i  /  sum over D's list of w_i count_i,
+p_hat where the denominator is 0 (a menu the draw left unseen). These are the lists the GPU
+kernel walks (rumb_draws_*, csrc/draws.cu); the host walks them with segment sums in list order.
+With integer weights (multinomial, multinomial_reject, poisson) every sum is an exact integer, so
+host, GPU and the reference agree bit for bit whatever the order. With real weights (exponential,
+mammen) the float64 sums depend on their order: here they run in list order, the reference's in
+its BLAS product's, and the rows agree to rounding (1e-15 relative).
+
+Weights, drawn in the reference's order so that a seed gives the reference's draws:
+    multinomial_reject   respondent counts of R picks with replacement (rng.multinomial); weight
+                         rows that leave one of rum's menus unseen are drawn again, up to
+                         REDRAW_ROUNDS rounds (the default scheme)
+    multinomial          the same without the redraw: an unseen menu keeps p_hat
+    exponential          Exp(1) multipliers
+    poisson              Poisson(1) multipliers
+    mammen               the wild bootstrap's two-point weights; the row is
+                         clip(p_hat + sum_i w_i (chose_i - offered_i p_hat) / N_D, 0, 1)
+Replies draws: menu D's reply counts ~ Multinomial(N_D, its shares), menus in increasing mask
+order, block k of draws from numpy.random.default_rng([seed, k]); the block size (BLOCK_BYTES of
+float64 draws) is therefore part of the stream.
 """
 import hashlib
 
 import numpy as np
-import scipy.sparse as sp
 
 WEIGHTS = ("multinomial_reject", "multinomial", "exponential", "poisson", "mammen")
 INTEGER_WEIGHTS = ("multinomial_reject", "multinomial", "poisson")
 COLUMNS = ("respondent", "menu", "chosen")
 P_HAT_TOL = 1e-9                # rum's p_hat against the table's counts
-BLOCK_BYTES = 1 << 27           # draws are built at most 128 MB at a time
-DENSE_ENTRIES = 1 << 25         # count matrices stay dense up to this many entries
+BLOCK_BYTES = 1 << 27           # float64 draws built per block (fixes the replies draws' streams)
 REDRAW_ROUNDS = 10000           # multinomial_reject gives up after this many rounds
+_MAX_MENU = 1 << 62             # menus are sets of at most 62 alternatives
+_WORK_BYTES = 1 << 27           # scratch of one segment-sum pass over weight rows
 
 
-def _int_column(x, column, what):
-    if x.dtype.kind == "f":
-        if not np.isfinite(x).all():
-            raise ValueError("%s row %d: missing %s" % (what, np.flatnonzero(~np.isfinite(x))[0], column))
-        frac = np.flatnonzero(x != np.floor(x))
-        if frac.size:
-            raise ValueError("%s row %d: %s %r is not an integer" % (what, frac[0], column, x[frac[0]]))
-    elif x.dtype.kind not in "iu":
-        raise ValueError("the %s's %s column must hold integers" % (what, column))
-    return x.astype(np.int64)
+# ------------------------------------------------------------------ reading a table
+def _as_int(values, table, column):
+    """A column of whole numbers as int64; floats must be finite and integral."""
+    kind = values.dtype.kind
+    if kind in "iu":
+        return values.astype(np.int64)
+    if kind != "f":
+        raise ValueError("the %s's %s column must hold integers" % (table, column))
+    nan = ~np.isfinite(values)
+    if nan.any():
+        raise ValueError("%s row %d: missing %s" % (table, int(np.argmax(nan)), column))
+    off = values != np.floor(values)
+    if off.any():
+        j = int(np.argmax(off))
+        raise ValueError("%s row %d: %s %r is not an integer" % (table, j, column, values[j]))
+    return values.astype(np.int64)
 
 
-def _read_choices(table, what, num_alternatives=None, respondent=False):
-    """(respondent,) menu and chosen of a table, checked; `what` names the table in the errors."""
-    names = COLUMNS if respondent else COLUMNS[1:]
-    missing = [c for c in names if c not in table]
-    if missing:
-        raise ValueError("the %s needs the columns %s and %s; missing: %s"
-                         % (what, ", ".join(names[:-1]), names[-1], ", ".join(missing)))
-    cols = [np.asarray(table[c]) for c in names]
-    if not (all(c.ndim == 1 for c in cols) and len({c.size for c in cols}) == 1):
-        raise ValueError("the %s's columns must be 1-D and of equal length" % what)
-    if cols[0].size == 0:
-        raise ValueError("the %s has no rows" % what)
-    menu, chosen = _int_column(cols[-2], "menu", what), _int_column(cols[-1], "chosen", what)
-    bad = np.flatnonzero((menu <= 0) | (menu >= 1 << 62))
-    if bad.size:
-        raise ValueError("%s row %d: menu mask %d is not a nonempty set of at most 62 alternatives"
-                         % (what, bad[0], menu[bad[0]]))
-    bad = np.flatnonzero((chosen < 0) | (chosen > 61))
-    if bad.size:
-        raise ValueError("%s row %d: chosen %d is not an alternative (0 to 61)" % (what, bad[0], chosen[bad[0]]))
-    bad = np.flatnonzero(((menu >> chosen) & 1) == 0)
-    if bad.size:
-        raise ValueError("%s row %d: chosen %d is not in its menu (mask %d)" % (what, bad[0], chosen[bad[0]],
-                                                                             menu[bad[0]]))
-    if num_alternatives is not None:
-        bad = np.flatnonzero(menu >= 1 << int(num_alternatives))
-        if bad.size:
-            raise ValueError("%s row %d: menu mask %d has alternatives beyond num_alternatives = %d"
-                             % (what, bad[0], menu[bad[0]], num_alternatives))
-    return (cols[0], menu, chosen) if respondent else (menu, chosen)
+def _first(mask):
+    return int(np.argmax(mask))
+
+
+class _Choices:
+    """The checked columns of a choice table: menu and chosen (int64) and, for a panel, the
+    respondent codes 0..R-1 in sorted id order."""
+
+    def __init__(self, table, name, num_alternatives=None, panel=False):
+        cols = COLUMNS if panel else COLUMNS[1:]
+        absent = [c for c in cols if c not in table]
+        if absent:
+            raise ValueError("the %s needs the columns %s and %s; missing: %s"
+                             % (name, ", ".join(cols[:-1]), cols[-1], ", ".join(absent)))
+        raw = {c: np.asarray(table[c]) for c in cols}
+        sizes = {a.size for a in raw.values()}
+        if len(sizes) != 1 or any(a.ndim != 1 for a in raw.values()):
+            raise ValueError("the %s's columns must be 1-D and of equal length" % name)
+        if sizes.pop() == 0:
+            raise ValueError("the %s has no rows" % name)
+        menu = _as_int(raw["menu"], name, "menu")
+        chosen = _as_int(raw["chosen"], name, "chosen")
+        bad = (menu <= 0) | (menu >= _MAX_MENU)
+        if bad.any():
+            j = _first(bad)
+            raise ValueError("%s row %d: menu mask %d is not a nonempty set of at most 62 alternatives"
+                             % (name, j, menu[j]))
+        bad = (chosen < 0) | (chosen > 61)
+        if bad.any():
+            j = _first(bad)
+            raise ValueError("%s row %d: chosen %d is not an alternative (0 to 61)" % (name, j, chosen[j]))
+        bad = ((menu >> chosen) & 1) == 0
+        if bad.any():
+            j = _first(bad)
+            raise ValueError("%s row %d: chosen %d is not in its menu (mask %d)" % (name, j, chosen[j], menu[j]))
+        if num_alternatives is not None:
+            bad = menu >= 1 << int(num_alternatives)
+            if bad.any():
+                j = _first(bad)
+                raise ValueError("%s row %d: menu mask %d has alternatives beyond num_alternatives = %d"
+                                 % (name, j, menu[j], num_alternatives))
+        self.menu, self.chosen = menu, chosen
+        self.codes, self.R = None, 0
+        if panel:
+            self.codes, self.R = self._respondents(raw["respondent"])
+
+    @staticmethod
+    def _respondents(ids):
+        if ids.dtype.kind == "f":
+            nan = ~np.isfinite(ids)
+            if nan.any():
+                raise ValueError("panel row %d: missing respondent" % _first(nan))
+        elif ids.dtype.kind == "O":
+            for j, v in enumerate(ids):
+                if v is None or v != v:
+                    raise ValueError("panel row %d: missing respondent" % j)
+        try:
+            uniq, codes = np.unique(ids, return_inverse=True)
+        except TypeError:
+            raise ValueError("respondent ids must be all numbers or all strings") from None
+        return codes.astype(np.int64).ravel(), int(uniq.size)
 
 
 def read_panel(panel, num_alternatives=None):
     """(respondent codes 0..R-1 in sorted id order, R, menu, chosen) of a panel, checked."""
-    resp, menu, chosen = _read_choices(panel, "panel", num_alternatives, respondent=True)
-    if resp.dtype.kind == "f" and not np.isfinite(resp).all():
-        raise ValueError("panel row %d: missing respondent" % np.flatnonzero(~np.isfinite(resp))[0])
-    if resp.dtype.kind == "O":
-        bad = [i for i, r in enumerate(resp) if r is None or r != r]
-        if bad:
-            raise ValueError("panel row %d: missing respondent" % bad[0])
-    try:
-        ids, codes = np.unique(resp, return_inverse=True)
-    except TypeError:
-        raise ValueError("respondent ids must be all numbers or all strings") from None
-    return codes.astype(np.int64), int(ids.size), menu, chosen
+    t = _Choices(panel, "panel", num_alternatives, panel=True)
+    return t.codes, t.R, t.menu, t.chosen
 
 
 def cells_from_panel(table, num_alternatives=None, alternatives=None):
-    """(menu, alternative, p_hat) counted from a panel or a replies table (a table with a respondent
-    column is checked as a panel): one row per menu of the table and member alternative (or only
-    those in `alternatives`), menus increasing and alternatives increasing within a menu; p_hat is
-    the share of the menu's rows that chose the alternative (0 when never chosen)."""
+    """rum's rows (menu, alternative, p_hat) counted from a panel or a replies table (a table with a
+    respondent column is read as a panel): every menu of the table, increasing, with each member
+    alternative (or each of `alternatives` it offers), increasing; p_hat is the share of the
+    menu's rows that chose the alternative, 0 when none did."""
     if COLUMNS[0] in table:
-        _codes, _R, menu, chosen = read_panel(table, num_alternatives)
+        t = _Choices(table, "panel", num_alternatives, panel=True)
     else:
-        menu, chosen = _read_choices(table, "replies table", num_alternatives)
+        t = _Choices(table, "replies table", num_alternatives)
     n = (int(num_alternatives) if num_alternatives is not None
-         else max(int(menu.max()).bit_length(), int(chosen.max()) + 1))
-    menus, inv, den = np.unique(menu, return_inverse=True, return_counts=True)
-    alts = np.arange(n) if alternatives is None else np.unique(np.asarray(alternatives, dtype=np.int64))
-    if alts.size == 0 or alts[0] < 0 or alts[-1] >= n:
+         else max(int(t.menu.max()).bit_length(), int(t.chosen.max()) + 1))
+    if alternatives is None:
+        keep = np.arange(n)
+    else:
+        keep = np.unique(np.asarray(alternatives, dtype=np.int64))
+    if keep.size == 0 or keep[0] < 0 or keep[-1] >= n:
         raise ValueError("alternatives must be a nonempty list of alternatives from 0 to %d" % (n - 1))
-    j, k = np.nonzero((menus[:, None] >> alts[None, :]) & 1)
-    if j.size == 0:
-        raise ValueError("no menu of the table offers any of the alternatives %s" % alts.tolist())
-    num = np.bincount(inv * n + chosen, minlength=menus.size * n)
-    return menus[j], alts[k], num[j * n + alts[k]] / den[j]
+    menus, inv, offered = np.unique(t.menu, return_inverse=True, return_counts=True)
+    # replies per (menu, chosen): keys menu index * 64 + chosen, counted once
+    pairs, chose = np.unique(inv.ravel().astype(np.int64) * 64 + t.chosen, return_counts=True)
+    wanted = np.zeros(64, dtype=bool)
+    wanted[keep] = True
+    offers = ((menus[:, None] >> np.arange(64)[None, :]) & 1).astype(bool) & wanted[None, :]
+    mi, ai = np.nonzero(offers)                  # menu-major, alternatives increasing
+    if mi.size == 0:
+        raise ValueError("no menu of the table offers any of the alternatives %s" % keep.tolist())
+    key = mi.astype(np.int64) * 64 + ai
+    at = np.minimum(np.searchsorted(pairs, key), pairs.size - 1)
+    num = np.where(pairs[at] == key, chose[at], 0)
+    return menus[mi], ai.astype(np.int64), num / offered[mi]
 
 
-class _Blocks:
-    """B draws held as what rebuilds them, a block of rows_per_block draws at a time (the last block
-    built is kept); a subclass's _build(k) gives (block k, its draws that left a menu unseen)."""
+# ------------------------------------------------------------------ count lists
+def _rum_rows(menu, alternative):
+    """rum's menus (sorted), each row's menu index, and a lookup (menu index, alternative) -> row."""
+    menu, alternative = np.asarray(menu, dtype=np.int64), np.asarray(alternative, dtype=np.int64)
+    menus, row_menu = np.unique(menu, return_inverse=True)
+    keys = row_menu.astype(np.int64) * 64 + alternative
+    order = np.argsort(keys, kind="stable")
+    return menus, row_menu.astype(np.int64), keys[order], order
+
+
+def _menu_index(menus, table_menu):
+    """The index of each table menu among rum's menus, and which table rows have one."""
+    j = np.searchsorted(menus, table_menu)
+    jc = np.minimum(j, menus.size - 1)
+    return jc, menus[jc] == table_menu
+
+
+def _lists(seg, who, nseg, nwho):
+    """CSR lists from (segment, member) pairs with repeats: ptr [nseg + 1], members ascending
+    within a segment (int32) and how often each pair occurred (float64)."""
+    key, cnt = np.unique(seg.astype(np.int64) * nwho + who.astype(np.int64), return_counts=True)
+    s = key // nwho
+    ptr = np.zeros(nseg + 1, dtype=np.int64)
+    np.add.at(ptr, s + 1, 1)
+    return np.cumsum(ptr), (key % nwho).astype(np.int32), cnt.astype(np.float64)
+
+
+class CountLists:
+    """A panel reduced to what its draws are made from (the inputs of rumb_draws_create):
+    menu_ptr / menu_resp / menu_cnt   per rum menu, the respondents offered it and how often
+    row_ptr / row_resp / row_cnt      per rum row, the respondents who chose it and how often
+    row_menu                          each rum row's menu index"""
+
+    def __init__(self, menu_ptr, menu_resp, menu_cnt, row_ptr, row_resp, row_cnt, row_menu, R):
+        self.menu_ptr, self.menu_resp, self.menu_cnt = menu_ptr, menu_resp, menu_cnt
+        self.row_ptr, self.row_resp, self.row_cnt = row_ptr, row_resp, row_cnt
+        self.row_menu = row_menu
+        self.R = int(R)
+        self.n_menus = menu_ptr.size - 1
+        self.M = row_ptr.size - 1
+
+    def menu_sums(self, W):
+        """(rows of W) x (rum menus): sum over each menu's list of w_i count_i."""
+        return _segment_sums(W, self.menu_ptr, self.menu_resp, self.menu_cnt)
+
+    def row_sums(self, W):
+        """(rows of W) x (rum rows): sum over each row's list of w_i count_i."""
+        return _segment_sums(W, self.row_ptr, self.row_resp, self.row_cnt)
+
+
+def _segment_sums(W, ptr, who, cnt):
+    """out[b, j] = sum over k in [ptr[j], ptr[j+1]) of W[b, who[k]] cnt[k], added in list order;
+    0 for an empty list. W rows are processed in chunks of at most _WORK_BYTES of products."""
+    W = np.atleast_2d(W)
+    nseg = ptr.size - 1
+    out = np.zeros((W.shape[0], nseg))
+    full = np.flatnonzero(ptr[1:] > ptr[:-1])
+    if full.size == 0:
+        return out
+    step = max(1, _WORK_BYTES // (8 * max(1, who.size)))
+    for lo in range(0, W.shape[0], step):
+        prod = W[lo:lo + step][:, who] * cnt
+        out[lo:lo + step, full] = np.add.reduceat(prod, ptr[full], axis=1)
+    return out
+
+
+# ------------------------------------------------------------------ draws in blocks
+class _BlockedDraws:
+    """B draws of M rows made block by block (at most BLOCK_BYTES of float64 per block; the last
+    block made is kept). A subclass gives make_block(k) -> (rows, draws that left a menu unseen)."""
+
+    def _setup_blocks(self, width):
+        self.rows_per_block = max(1, min(self.B, BLOCK_BYTES // (8 * width)))
+        self.n_blocks = -(-self.B // self.rows_per_block)
+        self._held = None
+        self.n_empty = None
+        self.fingerprint = None
 
     def block(self, k):
-        if self._cache[0] != k:
-            self._cache = (k,) + self._build(k)
-        return self._cache[1]
+        if self._held is None or self._held[0] != k:
+            rows, empty = self.make_block(k)
+            self._held = (k, rows, empty)
+        return self._held[1]
 
     def blocks(self):
-        """(first, last + 1, draws) for every block; a full pass sets fingerprint (the first 16 hex
-        digits of the sha256 of the B x M float64 draws in order) and n_empty."""
-        h, n_empty = hashlib.sha256(), 0
+        """(first, last + 1, rows) for every block. A full pass sets `fingerprint` (the first 16
+        hex digits of the sha256 of all B x M float64 draws in order) and `n_empty`."""
+        digest, empty = hashlib.sha256(), 0
         for k in range(self.n_blocks):
-            out = self.block(k)
-            n_empty += self._cache[2]
-            h.update(np.ascontiguousarray(out).tobytes())
-            yield k * self.rows_per_block, k * self.rows_per_block + out.shape[0], out
-        self.fingerprint, self.n_empty = h.hexdigest()[:16], n_empty
+            rows = self.block(k)
+            empty += self._held[2]
+            digest.update(np.ascontiguousarray(rows).tobytes())
+            lo = k * self.rows_per_block
+            yield lo, lo + rows.shape[0], rows
+        self.fingerprint, self.n_empty = digest.hexdigest()[:16], empty
 
     def rows(self, idx):
         """The draws idx as a (len(idx), M) array."""
         idx = np.asarray(idx, dtype=np.int64)
         out = np.empty((idx.size, self.M))
-        for k in np.unique(idx // self.rows_per_block):
-            sel = idx // self.rows_per_block == k
-            out[sel] = self.block(int(k))[idx[sel] - k * self.rows_per_block]
+        blk = idx // self.rows_per_block
+        for k in np.unique(blk):
+            at = np.flatnonzero(blk == k)
+            out[at] = self.block(int(k))[idx[at] - k * self.rows_per_block]
         return out
 
 
-class Draws(_Blocks):
+class Draws(_BlockedDraws):
     """B draws of p_hat for rum's rows (menu, alternative, p_hat), made from a respondent panel."""
 
     input = "panel"
@@ -162,57 +288,43 @@ class Draws(_Blocks):
             raise ValueError("unknown weights %r; choose from %s" % (weights, WEIGHTS))
         if int(B) != B or B < 1:
             raise ValueError("B must be a positive integer")
-        codes, R, pm, pc = read_panel(panel)
-        self.input_fingerprint = hashlib.sha256(codes.tobytes() + pm.tobytes() + pc.tobytes()).hexdigest()[:16]
+        t = _Choices(panel, "panel", panel=True)
+        codes, R = t.codes, t.R
+        self.input_fingerprint = hashlib.sha256(codes.tobytes() + t.menu.tobytes()
+                                                + t.chosen.tobytes()).hexdigest()[:16]
         menu, alternative = np.asarray(menu, dtype=np.int64), np.asarray(alternative, dtype=np.int64)
-        p_hat = np.asarray(p_hat, dtype=np.float64)
+        self.p_hat = p_hat = np.asarray(p_hat, dtype=np.float64)
         M = menu.size
-        # panel rows -> rum's menus, and -> rum's rows by (menu, chosen)
-        rum_menus, row_menu = np.unique(menu, return_inverse=True)
-        m = np.minimum(np.searchsorted(rum_menus, pm), rum_menus.size - 1)
-        used = rum_menus[m] == pm
-        row_key = row_menu * 64 + alternative
-        order = np.argsort(row_key)
-        key = m * 64 + pc
-        pos = np.minimum(np.searchsorted(row_key[order], key), M - 1)
-        hit = used & (row_key[order][pos] == key)
-        offered = sp.csr_array((np.ones(int(used.sum())), (codes[used], m[used])), shape=(R, rum_menus.size))
-        chose = sp.csr_array((np.ones(int(hit.sum())), (codes[hit], order[pos[hit]])), shape=(R, M))
-        N = np.asarray(offered.sum(axis=0)).ravel()[row_menu]
+        menus, row_menu, sorted_keys, sorted_rows = _rum_rows(menu, alternative)
+        j, on_rum = _menu_index(menus, t.menu)
+        # the panel rows whose (menu, chosen) is one of rum's rows, and which row
+        want = j * 64 + t.chosen
+        at = np.minimum(np.searchsorted(sorted_keys, want), M - 1)
+        is_row = on_rum & (sorted_keys[at] == want)
+        mptr, mresp, mcnt = _lists(j[on_rum], codes[on_rum], menus.size, R)
+        rptr, rresp, rcnt = _lists(sorted_rows[at[is_row]], codes[is_row], M, R)
+        self.lists = CountLists(mptr, mresp, mcnt, rptr, rresp, rcnt, row_menu.astype(np.int32), R)
+        N = self.lists.menu_sums(np.ones((1, R)))[0][row_menu]        # panel rows per row's menu
         if (N == 0).any():
-            k = int(np.flatnonzero(N == 0)[0])
+            k = _first(N == 0)
             raise ValueError("rum row %d (menu %d): the menu is not in the panel" % (k, menu[k]))
-        c = np.asarray(chose.sum(axis=0)).ravel()
+        c = self.lists.row_sums(np.ones((1, R)))[0]
         gap = np.abs(c / N - p_hat)
         if gap.max() > P_HAT_TOL:
             k = int(np.argmax(gap))
             raise ValueError("rum row %d (menu %d, alternative %d): p_hat = %.6g, but the panel gives %.6g (%d of %d "
                              "rows); build rum with cells_from_panel(panel, ...)"
                              % (k, menu[k], alternative[k], p_hat[k], c[k] / N[k], c[k], N[k]))
-        # sparse (respondent x menu / row) counts, for the GPU draws and the redraw test
-        self.offered, self.chose, self.row_menu = offered, chose, row_menu
-        dense = R * M <= DENSE_ENTRIES
-        self._offered = offered.toarray() if R * rum_menus.size <= DENSE_ENTRIES else offered
-        self._seen = None
-        if weights in ("mammen", "exponential"):        # real weights: per-row counts
-            seen = offered @ sp.csr_array((np.ones(M), (row_menu, np.arange(M))), shape=(rum_menus.size, M))
-        if weights == "mammen":
-            resid = (chose - seen.multiply(p_hat[None, :])).tocsr()
-            self._resid, self._N = (resid.toarray() if dense else resid), np.maximum(N, 1.0)
-        else:
-            self._chose = chose.toarray() if dense else chose
-            if weights == "exponential":
-                self._seen = seen.toarray() if dense else seen
+        self.N = N
         self.B, self.R, self.M, self.weights, self.seed = int(B), R, M, weights, seed
-        self.p_hat = p_hat
-        self.rows_unused = int((~used).sum())           # panel rows on menus that have no rum row
-        self.rows_per_block = max(1, min(self.B, BLOCK_BYTES // (8 * M)))
-        self.n_blocks = -(-self.B // self.rows_per_block)
+        self.rows_unused = int((~on_rum).sum())          # panel rows on menus that have no rum row
         self.n_redraws = self.n_reject_rounds = 0
-        self.n_empty = None
-        self.fingerprint = None
-        self._cache = (None, None, 0)
-        self.W = self._weights(np.random.default_rng(seed))
+        self._setup_blocks(M)
+        self.W = self._draw_weights(np.random.default_rng(seed))
+
+    @property
+    def row_menu(self):
+        return self.lists.row_menu
 
     @property
     def integer_weights(self):
@@ -230,48 +342,55 @@ class Draws(_Blocks):
         return dict(respondents=self.R, rows_unused=self.rows_unused, redraws=self.n_redraws,
                     emptied_menu_draws=self.n_empty)
 
-    def _weights(self, rng):
-        B, R = self.B, self.R
-        if self.weights == "mammen":
-            s5 = np.sqrt(5.0)
-            return np.where(rng.random((B, R)) < (s5 + 1) / (2 * s5), -(s5 - 1) / 2, (s5 + 1) / 2)
+    def _multinomial(self, rng, count):
+        R = self.R
+        return rng.multinomial(R, np.full(R, 1.0 / R), size=count).astype(np.float64)
+
+    def _draw_weights(self, rng):
+        """The B x R weight matrix, drawn as the reference draws it for this scheme and seed."""
+        shape = (self.B, self.R)
         if self.weights == "exponential":
-            return rng.exponential(1.0, size=(B, R))
+            return rng.exponential(1.0, size=shape)
         if self.weights == "poisson":
-            return rng.poisson(1.0, size=(B, R)).astype(np.float64)
-        W = rng.multinomial(R, np.ones(R) / R, size=B).astype(np.float64)
+            return rng.poisson(1.0, size=shape).astype(np.float64)
+        if self.weights == "mammen":
+            r5 = np.sqrt(5.0)
+            low = rng.random(shape) < (r5 + 1.0) / (2.0 * r5)
+            return np.where(low, -(r5 - 1.0) / 2.0, (r5 + 1.0) / 2.0)
+        W = self._multinomial(rng, self.B)
         if self.weights == "multinomial_reject":
+            # a row that saw every menu keeps its weights, so each round tests only the rows just
+            # drawn again (the same rows, in the same order, as testing all of W would find)
+            todo = np.flatnonzero(self.leaves_menu_unseen(W))
             for _ in range(REDRAW_ROUNDS):
-                bad = self._unseen(W)
-                if not bad.any():
+                if todo.size == 0:
                     break
-                self.n_redraws += int(bad.sum())
+                self.n_redraws += int(todo.size)
                 self.n_reject_rounds += 1
-                W[bad] = rng.multinomial(R, np.ones(R) / R, size=int(bad.sum())).astype(np.float64)
+                W[todo] = self._multinomial(rng, int(todo.size))
+                todo = todo[self.leaves_menu_unseen(W[todo])]
         return W
 
-    def _unseen(self, W):
-        """Which weight rows leave some menu of rum with no weight."""
-        step = max(1, BLOCK_BYTES // (8 * self._offered.shape[1]))
-        return np.concatenate([np.any(W[lo:lo + step] @ self._offered <= 0, axis=1)
-                               for lo in range(0, W.shape[0], step)])
+    def leaves_menu_unseen(self, W):
+        """For each weight row: does some rum menu get total weight 0?"""
+        return np.any(self.lists.menu_sums(W) <= 0, axis=1)
 
-    def _build(self, k):
+    def make_block(self, k):
         Wb = self.W[k * self.rows_per_block:(k + 1) * self.rows_per_block]
+        L = self.lists
+        seen = L.menu_sums(Wb)[:, L.row_menu]
+        chose = L.row_sums(Wb)
         if self.weights == "mammen":
-            return np.clip(self.p_hat + np.asarray(Wb @ self._resid) / self._N, 0.0, 1.0), 0
-        seen = (np.asarray(Wb @ self._offered)[:, self.row_menu] if self._seen is None
-                else np.asarray(Wb @ self._seen))
-        chose = np.asarray(Wb @ self._chose)
+            return np.clip(self.p_hat + (chose - seen * self.p_hat) / np.maximum(self.N, 1.0), 0.0, 1.0), 0
         empty = seen <= 0
-        return (np.where(empty, self.p_hat, chose / np.where(empty, 1.0, seen)),
-                int(np.any(empty, axis=1).sum()))
+        rows = np.where(empty, self.p_hat, chose / np.where(empty, 1.0, seen))
+        return rows, int(empty.any(axis=1).sum())
 
 
-class MenuDraws(_Blocks):
+class MenuDraws(_BlockedDraws):
     """B draws of p_hat for rum's rows made from a replies table: each menu's replies resampled on
-    their own (menu D's counts ~ Multinomial(N_D, the shares of D's replies)). Block k is drawn from
-    numpy.random.default_rng([seed, k]), menus in increasing mask order, so any block rebuilds alone."""
+    their own, menu D's counts ~ Multinomial(N_D, the shares of D's replies). Block k comes from
+    numpy.random.default_rng([seed, k]), menus in increasing mask order, so a block rebuilds alone."""
 
     input, weights = "replies", "multinomial"
     integer_weights = False
@@ -279,24 +398,26 @@ class MenuDraws(_Blocks):
     def __init__(self, replies, menu, alternative, p_hat, B=10000, seed=0):
         if int(B) != B or B < 1:
             raise ValueError("B must be a positive integer")
-        pm, pc = _read_choices(replies, "replies table")
-        self.input_fingerprint = hashlib.sha256(pm.tobytes() + pc.tobytes()).hexdigest()[:16]
+        t = _Choices(replies, "replies table")
+        self.input_fingerprint = hashlib.sha256(t.menu.tobytes() + t.chosen.tobytes()).hexdigest()[:16]
         menu, alternative = np.asarray(menu, dtype=np.int64), np.asarray(alternative, dtype=np.int64)
-        p_hat = np.asarray(p_hat, dtype=np.float64)
+        self.p_hat = p_hat = np.asarray(p_hat, dtype=np.float64)
         M = menu.size
-        rum_menus, row_menu = np.unique(menu, return_inverse=True)
-        m = np.minimum(np.searchsorted(rum_menus, pm), rum_menus.size - 1)
-        used = rum_menus[m] == pm
-        N = np.bincount(m[used], minlength=rum_menus.size)
-        if (N == 0).any():
-            k = int(np.flatnonzero(N[row_menu] == 0)[0])
+        menus, row_menu, _, _ = _rum_rows(menu, alternative)
+        j, on_rum = _menu_index(menus, t.menu)
+        N = np.bincount(j[on_rum], minlength=menus.size)
+        if (N[row_menu] == 0).any():
+            k = _first(N[row_menu] == 0)
             raise ValueError("rum row %d (menu %d): the menu is not in the replies" % (k, menu[k]))
-        # every (menu, alternative) chosen at least once, menu-major, and how often
-        support, count = np.unique(m[used] * 64 + pc[used], return_counts=True)
-        row_key = row_menu * 64 + alternative
-        pos = np.minimum(np.searchsorted(support, row_key), support.size - 1)
-        hit = support[pos] == row_key
-        c, den = np.where(hit, count[pos], 0), N[row_menu]
+        # the (menu, alternative) pairs chosen at least once, menu-major, and their counts: the
+        # categories of each menu's multinomial, in the order the draws consume them
+        cat, cnt = np.unique(j[on_rum] * 64 + t.chosen[on_rum], return_counts=True)
+        cat_menu = cat // 64
+        key = row_menu * 64 + alternative
+        at = np.minimum(np.searchsorted(cat, key), cat.size - 1)
+        found = cat[at] == key
+        c = np.where(found, cnt[at], 0)
+        den = N[row_menu]
         gap = np.abs(c / den - p_hat)
         if gap.max() > P_HAT_TOL:
             k = int(np.argmax(gap))
@@ -304,18 +425,14 @@ class MenuDraws(_Blocks):
                              "%d rows); build rum with cells_from_panel(replies, ...)"
                              % (k, menu[k], alternative[k], p_hat[k], c[k] / den[k], c[k], den[k]))
         self.N = N
-        self._shares = count / N[support // 64]
-        self._bounds = np.r_[np.searchsorted(support // 64, np.arange(N.size)), support.size]
-        self._col = np.where(hit, pos, -1)
+        self._cat_share = cnt / N[cat_menu]
+        self._cat_start = np.searchsorted(cat_menu, np.arange(N.size + 1))
+        self._row_cat = np.where(found, at, -1)
         self._den = den.astype(np.float64)
-        self.B, self.M, self.seed, self.p_hat = int(B), M, seed, p_hat
-        self.rows_unused = int((~used).sum())
-        self.rows_per_block = max(1, min(self.B, BLOCK_BYTES // (8 * max(M, support.size))))
-        self.n_blocks = -(-self.B // self.rows_per_block)
+        self.B, self.M, self.seed = int(B), M, seed
+        self.rows_unused = int((~on_rum).sum())
         self.n_redraws = 0
-        self.n_empty = None
-        self.fingerprint = None
-        self._cache = (None, None, 0)
+        self._setup_blocks(max(M, cat.size))
 
     @property
     def default_n(self):
@@ -330,11 +447,13 @@ class MenuDraws(_Blocks):
         return dict(replies=int(self.N.sum()), replies_per_menu=[int(self.N.min()), int(self.N.max())],
                     rows_unused=self.rows_unused)
 
-    def _build(self, k):
-        rows = min(self.rows_per_block, self.B - k * self.rows_per_block)
+    def make_block(self, k):
+        first = k * self.rows_per_block
+        count = min(self.rows_per_block, self.B - first)
         rng = np.random.default_rng([self.seed, k])
-        counts = np.empty((rows, self._shares.size))
-        for j in range(self.N.size):
-            lo, hi = self._bounds[j], self._bounds[j + 1]
-            counts[:, lo:hi] = rng.multinomial(self.N[j], self._shares[lo:hi], size=rows)
-        return np.where(self._col >= 0, counts[:, np.maximum(self._col, 0)], 0.0) / self._den, 0
+        tally = np.empty((count, self._cat_share.size))
+        for d in range(self.N.size):
+            a, b = self._cat_start[d], self._cat_start[d + 1]
+            tally[:, a:b] = rng.multinomial(self.N[d], self._cat_share[a:b], size=count)
+        got = tally[:, np.maximum(self._row_cat, 0)]
+        return np.where(self._row_cat >= 0, got, 0.0) / self._den, 0

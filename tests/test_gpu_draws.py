@@ -1,5 +1,5 @@
 """Bootstrap draws on the GPU (rumb_draws_*): every draw's rows equal the host builder's
-(Draws.rows, the reference's block builder) bit for bit, raw and perturbed, and the screen's norms
+(Draws.rows, the count-list builder) bit for bit, raw and perturbed, and the screen's norms
 equal numpy's to rounding."""
 import numpy as np
 import pytest
@@ -27,7 +27,7 @@ CASES = list(_cases())
 @pytest.mark.parametrize("name,panel,m,a,p,B,weights", CASES, ids=[c[0] for c in CASES])
 def test_draw_rows_and_screen_match_host(ctx, name, panel, m, a, p, B, weights):
     d = BS.Draws(panel, m, a, p, B=B, weights=weights, seed=3)
-    g = _lib.DrawRows(ctx, d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+    g = _lib.DrawRows(ctx, d.W, d.lists, d.p_hat)
     r_n, eps_n, _ = BS.scaling(d.R)
     scale = eps_n * r_n
     idx = np.array([B - 1, 0, 7, 7, 3], dtype=np.int64)
@@ -56,24 +56,27 @@ def test_gpu_rows_match_reference_golden(ctx):
     panel = dict(respondent=g["panel_respondent"], menu=g["panel_menu"], chosen=g["panel_chosen"])
     for w in ("multinomial", "multinomial_reject"):
         d = BS.Draws(panel, g["menu"], g["alternative"], g["p_hat"], B=12, weights=w, seed=5)
-        gd = _lib.DrawRows(ctx, d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+        gd = _lib.DrawRows(ctx, d.W, d.lists, d.p_hat)
         np.testing.assert_array_equal(gd.rows(np.arange(12)), g["rows_" + w])
         gd.close()
 
 
 def test_draws_reject_bad_input(ctx):
     """Bad panels are refused on the host with an error, before anything reaches the GPU."""
-    import scipy.sparse as sp
+    import copy
     panel, (m, a, p) = panel_instance(8, 0.4, 20, 4, 3, seed=2)
     d = BS.Draws(panel, m, a, p, B=4, weights="multinomial", seed=0)
     with pytest.raises(_lib.RumbError):                     # a row's menu out of range
-        bad = d.row_menu.copy()
-        bad[0] = d.offered.shape[1]
-        _lib.DrawRows(ctx, d.W, d.offered, d.chose, bad, d.p_hat)
+        bad = copy.copy(d.lists)
+        bad.row_menu = d.lists.row_menu.copy()
+        bad.row_menu[0] = d.lists.n_menus
+        _lib.DrawRows(ctx, d.W, bad, d.p_hat)
     with pytest.raises(_lib.RumbError):                     # a respondent beyond R
-        off = sp.csr_array((np.ones(1), ([d.R], [0])), shape=(d.R + 1, d.offered.shape[1]))
-        _lib.DrawRows(ctx, d.W, off, d.chose, d.row_menu, d.p_hat)
-    g = _lib.DrawRows(ctx, d.W, d.offered, d.chose, d.row_menu, d.p_hat)
+        bad = copy.copy(d.lists)
+        bad.menu_resp = d.lists.menu_resp.copy()
+        bad.menu_resp[0] = d.R
+        _lib.DrawRows(ctx, d.W, bad, d.p_hat)
+    g = _lib.DrawRows(ctx, d.W, d.lists, d.p_hat)
     with pytest.raises(_lib.RumbError):                     # a draw index out of range
         g.rows(np.array([-1], dtype=np.int64))
     assert g.rows(np.zeros(0, dtype=np.int64)).shape == (0, d.M)

@@ -135,8 +135,11 @@ def test_draws_match_reference_golden():
     for w in D.WEIGHTS:
         d = D.Draws(panel, g["menu"], g["alternative"], g["p_hat"], B=12, weights=w, seed=5)
         np.testing.assert_array_equal(d.W, g["W_" + w])
-        np.testing.assert_array_equal(d.rows(np.arange(12)), g["rows_" + w])
-        np.testing.assert_array_equal(d.rows(np.array([11, 0, 5])), g["rows_" + w][[11, 0, 5]])
+        if w in D.INTEGER_WEIGHTS:          # exact integer sums: bit for bit
+            np.testing.assert_array_equal(d.rows(np.arange(12)), g["rows_" + w])
+        else:                               # real weights: float64 sums in another order
+            np.testing.assert_allclose(d.rows(np.arange(12)), g["rows_" + w], rtol=1e-14, atol=1e-15)
+        np.testing.assert_array_equal(d.rows(np.array([11, 0, 5])), d.rows(np.arange(12))[[11, 0, 5]])
     replies = dict(menu=g["panel_menu"], chosen=g["panel_chosen"])
     rm, ra, rp = D.cells_from_panel(replies, 8)
     np.testing.assert_array_equal(rm, g["rep_menu"])
@@ -280,7 +283,7 @@ def test_bootstrap_draws_and_formulas():
     assert rows.shape == (20, p.size)
     # a draw with every respondent weighted once reproduces p_hat
     d.W[0] = 1.0
-    d._cache = (None, None, 0)                  # the weights changed under the kept block
+    d._held = None                              # the weights changed under the kept block
     np.testing.assert_allclose(d.rows([0])[0], p, atol=1e-12)
     # shares stay shares
     sums = np.zeros((20, np.unique(m).size))
