@@ -224,16 +224,25 @@ def _broadcast_band(L0, U0, group):
     return float(t[0]), float(t[1])
 
 
-def _gather_record(L, U, solved, group):
-    """Every rank's (L, U, solved) combined: a draw's bounds are the tightest any rank found."""
+def _gather_record(L, U, solved, flag, tol_stop, tol_full, group):
+    """Every rank's per-draw record combined: a draw's bounds are the tightest any rank found, its
+    tolerances the tightest any rank reached, and its exit flag the one of a rank that solved it
+    (NEVER when none did)."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
-    t = torch.from_numpy(np.stack([L, U, solved.astype(np.float64)])).to(_device_for(group))
+    t = torch.from_numpy(np.stack([L, U, solved.astype(np.float64), flag.astype(np.float64), tol_stop,
+                                   tol_full])).to(_device_for(group))
     parts = [torch.empty_like(t) for _ in range(world)]
     dist.all_gather(parts, t, group=group)
     allr = torch.stack(parts).cpu().numpy()
-    return allr[:, 0].max(axis=0), allr[:, 1].min(axis=0), allr[:, 2].max(axis=0) > 0
+    flags = allr[:, 3]
+    have = flags != NEVER
+    first = np.argmax(have, axis=0)                       # the lowest rank that solved the draw
+    cols = np.arange(flags.shape[1])
+    flag_all = np.where(have.any(axis=0), flags[first, cols], NEVER).astype(np.int8)
+    return (allr[:, 0].max(axis=0), allr[:, 1].min(axis=0), allr[:, 2].max(axis=0) > 0, flag_all,
+            allr[:, 4].min(axis=0), allr[:, 5].min(axis=0))
 
 
 class Bootstrap:
@@ -491,7 +500,9 @@ class Bootstrap:
         os.replace(tmp, path)
 
     def _save_checkpoint(self):
-        if self.checkpoint:
+        """The record written to the checkpoint path; under torch.distributed by rank 0 alone (every
+        rank holds the same gathered record, and one writer keeps the file whole)."""
+        if self.checkpoint and _dist(getattr(self, "_group", None))[0] == 0:
             self.save(self.checkpoint)
 
     def _resume(self, path):
@@ -572,8 +583,9 @@ class Bootstrap:
         decision at alpha is locked (the remaining draws cannot change it; one process only).
         Under torch.distributed (group: a process group, or the default one when it is initialized)
         every rank certifies p_hat on its own GPU, takes rank 0's band, solves every world-th open
-        draw starting at its rank, and one all_gather of (L, U, solved) gives every rank the whole
-        record; draws are independent, so nothing else is exchanged."""
+        draw starting at its rank, and one all_gather of the per-draw record (L, U, solved, exit flag,
+        tolerances) gives every rank the whole record; draws are independent, so nothing else is
+        exchanged. Rank 0 alone writes the checkpoint."""
         alpha = check_alpha(alpha)
         t0 = time.perf_counter()
         rank, world, group = _dist(group)
@@ -598,7 +610,10 @@ class Bootstrap:
             elif mine.size:
                 self.solve_draws(mine)
             if world > 1:
-                self.L, self.U, self.solved = _gather_record(self.L, self.U, self.solved, group)
+                (self.L, self.U, self.solved, self.flag, self.tol_stop,
+                 self.tol_full) = _gather_record(self.L, self.U, self.solved, self.flag, self.tol_stop,
+                                                 self.tol_full, group)
+        self._group = group
         dec = decide(self.L, self.U, *self.tau)
         above = int((dec == ABOVE).sum())
         und = int((dec == UNDECIDED).sum())
