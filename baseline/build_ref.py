@@ -1,12 +1,13 @@
-"""Extracts the reference's own CUDA kernel sources into oracle/_ref/ -- TEST INFRASTRUCTURE ONLY.
+"""Extracts the reference's own CUDA kernel sources into baseline/_ref/ (the comparison side of
+the parity tests and of bench.py's reference-kernel timing; never the product).
 
-    python oracle/build_ref.py [reference root]
+    python baseline/build_ref.py [reference root]     # default: $RUM_REFERENCE_ROOT, else DEFAULT_ROOT
 
 The reference (mingxiz/rum-testing-gpu) keeps its GPU kernels as CUDA C source strings inside
 Python modules and JIT-compiles them with NVRTC through CuPy. CuPy is not installed here, so this
 script reads those string constants with `ast` (the source text only, never a binary) and writes
-them as .cu files under oracle/_ref/, which is git-ignored and travels to the GPU box. There
-oracle/ref_replay.py compiles them with NVRTC (the compiler CuPy uses, default options) and
+them as .cu files under baseline/_ref/, which is git-ignored and travels to the GPU box. There
+baseline/ref_replay.py compiles them with NVRTC (the compiler CuPy uses, default options) and
 replays the reference's host sequence, for two purposes:
   * pinning the pricer's bit-exactness against the reference's compiled kernels, and
   * timing the reference's float64 BM-ADMM iteration on the same GPU.
@@ -26,6 +27,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# where this recipe finds the reference's source tree unless RUM_REFERENCE_ROOT says otherwise
+DEFAULT_ROOT = "/root/reference"
+
+
+def reference_root():
+    """The reference's source tree, or None when it is not present on this machine."""
+    root = os.environ.get("RUM_REFERENCE_ROOT", DEFAULT_ROOT)
+    return root if os.path.isdir(os.path.join(root, "solver")) else None
 
 
 def _module(root, rel):
@@ -94,4 +103,7 @@ def extract(root):
 
 
 if __name__ == "__main__":
-    print(extract(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    root = sys.argv[1] if len(sys.argv) > 1 else reference_root()
+    if root is None:
+        raise SystemExit("the reference's source tree was not found (set RUM_REFERENCE_ROOT)")
+    print(extract(root))

@@ -1,6 +1,7 @@
-"""The reference's own kernels, JIT-compiled and replayed on the GPU -- TEST INFRASTRUCTURE ONLY.
+"""The reference's own kernels, JIT-compiled and replayed on the GPU: the comparison side of the
+parity tests and of bench.py's reference-kernel timing (never the product).
 
-oracle/build_ref.py writes the reference's CUDA source strings to oracle/_ref/*.cu. This module
+baseline/build_ref.py writes the reference's CUDA source strings to baseline/_ref/*.cu. This module
 compiles them with NVRTC (through cuda-python, the same compiler CuPy drives, default options:
 fmad on, IEEE division) and replays the reference's host sequence with them:
 
@@ -8,11 +9,15 @@ fmad on, IEEE division) and replays the reference's host sequence with them:
                               (solver/flow_cg/pricing_stream.py:302-412, solver/flow_cg/solver.py:169-200)
   BMReplay                    solve_kadmm_v2's float64 iteration (solver/bm_admm/solver.py:240-254)
                               with Bfly2's calibrated stage plan (solver/bm_admm/butterfly2.py:160-230),
-                              replayed as a CUDA graph like the reference's use_graph path, and its
-                              float64 check (push_to_ub64 + fw_lb_rows_gpu) -- for timing only
+                              replayed as a CUDA graph like the reference's use_graph path, its
+                              float64 check (push_to_ub64 + fw_lb_rows_gpu) and the runner's certified
+                              loop: the reference side of the iterate and bracket parity tests, and
+                              of bench.py's reference-kernel timing
+  time_pricing                the reference's pricing kernels on one sweep's layers (bf_stream_u24 /
+                              bf_stream_u16 per layer, bf_update for the mask storage)
 
 Device buffers are torch tensors (plumbing); kernels launch through the CUDA driver API on the
-current torch stream. Only tests/ and bench-side comparison scripts use this module.
+current torch stream. Only tests/ and bench.py's comparison legs use this module.
 """
 import ctypes
 import math
@@ -281,8 +286,9 @@ def sweep_max64(menus, scores, offsets, n):
 
 # ------------------------------------------------------------------ BM-ADMM timing replay
 class BMReplay:
-    """solve_kadmm_v2's float64 iteration and float64 check with the reference's kernels, for
-    timing: t_iter (graph replay of one_iter, like use_graph=True), t_check (push_to_ub64 +
+    """solve_kadmm_v2's float64 iteration and float64 check with the reference's kernels: its
+    state after any number of iterations (state, iterate), its certified bracket (solve), and the
+    timings t_iter (graph replay of one_iter, like use_graph=True) and t_check (push_to_ub64 +
     fw_lb_rows_gpu, eager launches as the reference issues them)."""
 
     def __init__(self, n, menu, alt, p, beta, alpha=1.95, precond_p=math.sqrt(2.0)):
@@ -434,6 +440,82 @@ class BMReplay:
         self._ew("fuse_sy", [self.Ax, (_D, self.alpha), (_D, self.b1), (_D, self.ib1), self.s, self.y])
         self.x2.copy_(self.x2n)
 
+    def state(self):
+        """The ADMM state {x2, s, y, z} as float64 host arrays."""
+        return {k: getattr(self, k).cpu().numpy().copy() for k in ("x2", "s", "y", "z")}
+
+    def _graph(self):
+        """one_iter captured as a CUDA graph, the state left as it was (the reference's use_graph
+        path: a warm-up iteration before capture, then the snapshot restored,
+        solver/bm_admm/solver.py:273-292)."""
+        import torch
+        if getattr(self, "_g", None) is None:
+            snap = [t.clone() for t in (self.x2, self.s, self.y, self.z)]
+            st = torch.cuda.Stream()
+            torch.cuda.synchronize()
+            with torch.cuda.stream(st):
+                self.one_iter()
+                torch.cuda.synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=st):
+                    self.one_iter()
+            torch.cuda.synchronize()
+            for t, v in zip((self.x2, self.s, self.y, self.z), snap):
+                t.copy_(v)
+            torch.cuda.synchronize()
+            self._g = g
+        return self._g
+
+    def iterate(self, iters, graph=False):
+        """`iters` float64 iterations from the current state (eager launches, or graph replays)."""
+        import torch
+        g = self._graph() if graph else None
+        for _ in range(iters):
+            if g is not None:
+                g.replay()
+            else:
+                self.one_iter()
+        torch.cuda.synchronize()
+
+    def solve(self, abs_tol=1e-5, check=50, lb_every=1, max_iter=10 ** 7, time_limit=3600.0):
+        """The reference's certified float64 solve with the runner's hooks: `check` graph-replayed
+        iterations, then the float64 push (upper bound, the best one kept) and every `lb_every`
+        checks the Frank-Wolfe lower bound (the best one kept), until ub - lb <= abs_tol
+        (solver/bm_admm/solver.py:308-352 with ub_arm_immediately, ub_running_min and gap_abs_tol
+        as solver/rum_solver.py:879-905 sets them). Returns the bracket, the iterations, the checks
+        and the wall time of the loop (device synchronized at each check, as the reference's host
+        reads are)."""
+        import time
+        import torch
+        g = self._graph()
+        torch.cuda.synchronize()
+        ub, lb, it, checks, stop = float("nan"), 0.0, 0, 0, "max_iter"
+        t_iter = t_check = 0.0
+        t0 = time.perf_counter()
+        while it < max_iter:
+            a = time.perf_counter()
+            for _ in range(check):
+                g.replay()
+            torch.cuda.synchronize()
+            b = time.perf_counter()
+            it += check
+            u, l = self.check_once(with_lb=(checks % lb_every == 0))
+            checks += 1
+            t_iter += b - a
+            t_check += time.perf_counter() - b
+            ub = u if math.isnan(ub) else min(ub, u)
+            if l is not None:
+                lb = max(lb, l)
+            if ub - lb <= abs_tol:
+                stop = "gap_abs"
+                break
+            if time.perf_counter() - t0 > time_limit:
+                stop = "time_limit"
+                break
+        wall = time.perf_counter() - t0
+        return {"ub": ub, "lb": lb, "iters": it, "checks": checks, "stop_reason": stop, "wall_s": wall,
+                "iter_s": t_iter, "check_s": t_check}
+
     def time_iterations(self, iters=50, graph=True):
         """milliseconds per iteration (CUDA events), replaying a captured one_iter when graph."""
         import torch
@@ -489,8 +571,9 @@ class BMReplay:
             s += B
         return R
 
-    def check_once(self):
-        """push_to_ub64 + fw_lb_rows_gpu on the current iterate: (ub, lb)."""
+    def check_once(self, with_lb=True):
+        """push_to_ub64 + fw_lb_rows_gpu on the current iterate: (ub, lb); lb is None without
+        with_lb."""
         import torch
         n, Nloc, N = self.n, self.Nloc, 1 << self.n
         q = self._bfly_fast(self.x2.clone(), (1.0, -1.0, 0.0, 1.0))
@@ -512,6 +595,8 @@ class BMReplay:
         self.L.launch("extract64", (self.m2 + 255) // 256, 256, [w, outw, mass, rf, (_I, n), (_LL, Nloc)])
         xub = self._bfly_fast(rf, (1.0, 1.0, 0.0, 1.0))
         ub = float(torch.sqrt(torch.sum((xub[self.obs] - self.p) ** 2)).item())
+        if not with_lb:
+            return ub, None
         y = self.x2[self.obs]
         r = self.p - y
         f = float((r @ r).item())
@@ -538,3 +623,70 @@ class BMReplay:
         e1.record()
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
+
+
+# ------------------------------------------------------------------ pricing timing
+def time_pricing(menus, offsets, scores, n, reps=10):
+    """Milliseconds per sweep of the reference's pricing kernels on one sweep's layers, CUDA events
+    around the layer launches only (no host reads between layers, no backtrace): a lower bound of
+    its sweep. Stream storage: bf_stream_u24 / bf_stream_u16 (one 256-thread CTA per 1024 ranks,
+    x-major rows scanned per rank, solver/flow_cg/pricing_stream.py:61-181); mask storage:
+    bf_update (a thread per subset, solver/flow_cg/bf_pricing.py:8-47). Rows x-major."""
+    import torch
+    L = _Launcher(_mods()["pricing"])
+    counts = [math.comb(n, k) for k in range(n + 1)]
+    cap, k_pred = max(counts), n - 10
+    nblk = (cap + 1023) // 1024
+    binom = torch.from_numpy(_binom(n).view(np.int64)).cuda()
+    gm = torch.from_numpy(np.ascontiguousarray(menus, dtype=np.uint64).view(np.int64)).cuda()
+    gs = torch.from_numpy(np.ascontiguousarray(scores, dtype=np.float32)).cuda()
+    go = torch.from_numpy(np.asarray(offsets, dtype=np.uint64).view(np.int64)).cuda()
+    out = {}
+
+    def timed(sweep):
+        for _ in range(2):
+            sweep()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            sweep()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for mode in ("u24", "u16"):
+        vbuf = [torch.zeros(cap, dtype=torch.int16, device="cuda") for _ in range(2)]
+        lbuf = [torch.zeros(cap, dtype=torch.uint8, device="cuda") for _ in range(2)]
+        mbuf = [torch.zeros(nblk, dtype=torch.float32, device="cuda") for _ in range(2)]
+        ebuf = [torch.zeros(nblk, dtype=torch.float32, device="cuda") for _ in range(2)]
+        pred = {k: torch.zeros(counts[k], dtype=torch.uint8, device="cuda") for k in range(max(k_pred, 1), n + 1)}
+        dummy = torch.zeros(1, dtype=torch.uint8, device="cuda")
+
+        def sweep(mode=mode, vbuf=vbuf, lbuf=lbuf, mbuf=mbuf, ebuf=ebuf, pred=pred, dummy=dummy):
+            cur, prev = 0, 1
+            for k in range(1, n + 1):
+                store = 1 if k >= k_pred else 0
+                pk = pred[k] if store else dummy
+                if mode == "u24":
+                    args = [binom, (_I, n), (_I, k), (_ULL, counts[k]), vbuf[prev], lbuf[prev], mbuf[prev], ebuf[prev],
+                            vbuf[cur], lbuf[cur], mbuf[cur], ebuf[cur], pk, (_I, store), gm, gs, go]
+                else:
+                    args = [binom, (_I, n), (_I, k), (_ULL, counts[k]), vbuf[prev], mbuf[prev], ebuf[prev],
+                            vbuf[cur], mbuf[cur], ebuf[cur], pk, (_I, store), gm, gs, go]
+                L.launch("bf_stream_" + mode, (counts[k] + 1023) // 1024, 256, args)
+                cur, prev = prev, cur
+
+        out[mode + "_layers_ms"] = timed(sweep)
+    V = torch.zeros(1 << n, dtype=torch.float32, device="cuda")
+    P = torch.zeros(1 << n, dtype=torch.uint8, device="cuda")
+    gm32 = torch.from_numpy(np.asarray(menus, dtype=np.uint64).astype(np.uint32).view(np.int32)).cuda()
+    states = [torch.from_numpy(_gosper(n, c)).cuda() for c in range(n + 1)]
+
+    def mask_sweep():
+        for c in range(1, n + 1):
+            ns = states[c].numel()
+            L.launch("bf_update", (ns + 255) // 256, 256, [V, P, gm32, gs, go, states[c], (_I, ns)])
+
+    out["mask_layers_ms"] = timed(mask_sweep)
+    return out

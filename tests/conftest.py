@@ -6,7 +6,7 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for sub in ("rum-testing-gpu_b200", "oracle", "tests", os.path.join("tests", "golden")):
+for sub in ("rum-testing-gpu_b200", "oracle", "baseline", "tests", os.path.join("tests", "golden")):
     p = os.path.join(ROOT, sub)
     if p not in sys.path:
         sys.path.insert(0, p)

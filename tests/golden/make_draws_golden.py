@@ -72,4 +72,9 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "baseline"))
+    import build_ref
+    root = sys.argv[1] if len(sys.argv) > 1 else build_ref.reference_root()
+    if root is None:
+        raise SystemExit("the reference's source tree was not found (give it as the argument, or RUM_REFERENCE_ROOT)")
+    main(root)

@@ -2,9 +2,9 @@
 
     python tests/golden/make_replay_golden.py <out.npz>        # on a GPU host, after build()
 
-The reference's kernel source strings are extracted into oracle/_ref by oracle/build_ref.py (at
+The reference's kernel source strings are extracted into baseline/_ref by baseline/build_ref.py (at
 build time, where the reference tree is present), compiled here by NVRTC with the reference's
-options and launched through oracle/ref_replay.py. For seeded instances and seeded float32
+options and launched through baseline/ref_replay.py. For seeded instances and seeded float32
 scores, the file keeps the scores and the reference kernels' outputs: Vmax (float32), rank_pos,
 margin and per-layer steps for the f32, u16 and u24 stream pricers, and Vmax / rank_pos for the
 mask sweep. The instances themselves are regenerated from their seeds by the tests. These are the
@@ -18,7 +18,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-for p in (os.path.join(ROOT, "rum-testing-gpu_b200"), os.path.join(ROOT, "oracle"), os.path.dirname(HERE)):
+for p in (os.path.join(ROOT, "rum-testing-gpu_b200"), os.path.join(ROOT, "oracle"), os.path.join(ROOT, "baseline"),
+          os.path.dirname(HERE)):
     if p not in sys.path:
         sys.path.insert(0, p)
 
@@ -45,7 +46,7 @@ def main(out):
     import oracle as O
     import ref_replay
     if not ref_replay.available():
-        raise SystemExit("oracle/_ref is not built: run build() where the reference tree is present")
+        raise SystemExit("baseline/_ref is not built: run build() where the reference tree is present")
     rec = {}
     for name, n, m, a, p in cases():
         menus, alts, p32, offsets, _ = O.cg_layout(n, m, a, p)

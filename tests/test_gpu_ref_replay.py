@@ -1,6 +1,6 @@
 """The library against the reference's own kernels, JIT-compiled by NVRTC from the reference's
-source strings and replayed (oracle/build_ref.py, oracle/ref_replay.py): Flow-CG pricing must
-agree bit for bit (values, rankings, per-layer steps). Skipped where oracle/_ref was not built
+source strings and replayed (baseline/build_ref.py, baseline/ref_replay.py): Flow-CG pricing must
+agree bit for bit (values, rankings, per-layer steps). Skipped where baseline/_ref was not built
 (it needs the reference's source tree at build time)."""
 import numpy as np
 import pytest
@@ -12,7 +12,7 @@ from rumb import _lib
 from rumb.instances import config_instance
 
 pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not ref_replay.available(), reason="oracle/_ref not built")]
+              pytest.mark.skipif(not ref_replay.available(), reason="baseline/_ref not built")]
 
 
 def _cases():
@@ -51,3 +51,103 @@ def test_mask_pricer_matches_reference_kernel(ctx, name, cd, n):
     v_ref, r_ref = ref_replay.price_mask(menus, scores, offsets, n)
     v, r, _ = pr.price(scores)
     assert v == v_ref and np.array_equal(r, r_ref)
+
+
+# ------------------------------------------------------------------ BM-ADMM against the reference
+def _bm_instance(case):
+    if case == "n14_mix":
+        from rumb.instances import mixture_instance
+        m, a, p = mixture_instance(14, 0.05, K=20, N=300, seed=14)
+        return 14, m, a, p
+    return config_instance(case)[:4]
+
+
+BM_CASES = ["n10_all_k20", "n14_mix", "n18_d1pct_k50"]
+# float64 iterates after 1, 10 and 100 iterations, relative to the largest entry: the library
+# contracts multiply-adds and runs some transforms high bits first, the reference's kernels follow
+# their own stage plan, so the two round differently by a few ulps per iteration
+ITER_TOL = {1: 1e-11, 10: 1e-10, 100: 1e-9}
+
+
+def _max_rel(a, b):
+    return float(np.max(np.abs(a - b))) / max(1.0, float(np.max(np.abs(b))))
+
+
+@pytest.mark.parametrize("case", BM_CASES)
+def test_bm_iterates_match_reference_kernels(ctx, case):
+    """rumb_bm_iterate and the reference's own float64 iteration (solve_kadmm_v2's one_iter with
+    its kernels and calibrated butterfly plan, solver/bm_admm/solver.py:240-254) from the same cold
+    start (solver/bm_admm/solver.py:263-267): x2, s, y, z after 1, 10 and 100 iterations."""
+    n, menu, alt, p = _bm_instance(case)
+    beta = O.beta_default(p.size)
+    ref = ref_replay.BMReplay(n, menu, alt, p, beta)
+    prob = ctx.bm_problem(n, menu, alt, p)
+    par = ctx.bm_params(beta, dtype="float64")
+    st = ctx.bm_iterate(prob, par, None, 0, cold_start=True)
+    r = ref.state()
+    assert _max_rel(st["x2"], r["x2"]) <= 1e-12
+    total = 0
+    for k in (1, 9, 90):
+        st = ctx.bm_iterate(prob, par, st, k)
+        ref.iterate(k)
+        total += k
+        r = ref.state()
+        for name in ("x2", "s", "y", "z"):
+            d = _max_rel(st[name], r[name])
+            assert d <= ITER_TOL[total], (case, name, total, d)
+
+
+@pytest.mark.parametrize("case", BM_CASES)
+def test_oracle_iterates_match_reference_kernels(case):
+    """The oracle's float64 iteration (oracle/rum_oracle.c, the CPU restatement every other
+    BM-ADMM test checks the library against) pinned to the reference's own kernels the same way."""
+    n, menu, alt, p = _bm_instance(case)
+    beta = O.beta_default(p.size)
+    ref = ref_replay.BMReplay(n, menu, alt, p, beta)
+    O.set_threads(0)
+    bm = O.BMOracle(n, menu, alt, p, beta=beta)
+    assert _max_rel(bm.x2, ref.state()["x2"]) <= 1e-12
+    total = 0
+    for k in (1, 9, 90):
+        bm.iterate(k)
+        ref.iterate(k)
+        total += k
+        r = ref.state()
+        for name in ("x2", "s", "y", "z"):
+            d = _max_rel(getattr(bm, name), r[name])
+            assert d <= ITER_TOL[total], (case, name, total, d)
+
+
+_REF_SOLVES = {}
+
+
+def _reference_bracket(case):
+    """The reference's certified float64 bracket of a workload at abs 1e-5, check 50 (its kernels,
+    replayed with the runner's hooks); one run per session."""
+    if case not in _REF_SOLVES:
+        n, menu, alt, p = _bm_instance(case)
+        ref = ref_replay.BMReplay(n, menu, alt, p, O.beta_default(p.size))
+        _REF_SOLVES[case] = ref.solve(abs_tol=1e-5, check=50, lb_every=1)
+    return _REF_SOLVES[case]
+
+
+@pytest.mark.parametrize("dtype", ["float64", "mixed"])
+@pytest.mark.parametrize("case", ["n10_all_k20", "n18_d1pct_k50"])
+def test_certified_bracket_matches_reference_float64(ctx, case, dtype):
+    """The certified bracket at abs 1e-5 (n18_d1pct_k50 is the benchmark workload: n = 18, 1 %
+    menus, K = 50, N = 500) against the reference's float64 bm_admm run with its own kernels: both
+    certified, and each bound within 1e-6 of the reference's. In float64 the library follows the
+    reference's trajectory, so it stops at the same check; mixed (float32 until the float32
+    bracket stalls, then float64) reaches its own certified bracket."""
+    n, menu, alt, p = _bm_instance(case)
+    ref = _reference_bracket(case)
+    assert ref["stop_reason"] == "gap_abs" and ref["ub"] - ref["lb"] <= 1e-5
+    res, _, _ = ctx.bm_solve(ctx.bm_problem(n, menu, alt, p),
+                             ctx.bm_params(O.beta_default(p.size), check=50, abs_tol=1e-5, rel_tol=None,
+                                           dtype=dtype, time_limit=600))
+    assert res["stop_reason"] == "gap_abs", res
+    assert res["lb"] <= res["ub"] and res["ub"] - res["lb"] <= 1e-5
+    assert abs(res["ub"] - ref["ub"]) <= 1e-6, (res["ub"], ref["ub"])
+    assert abs(res["lb"] - ref["lb"]) <= 1e-6, (res["lb"], ref["lb"])
+    if dtype == "float64":
+        assert res["iters"] == ref["iters"], (res["iters"], ref["iters"])
