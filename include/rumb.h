@@ -96,10 +96,12 @@ RUMB_API int rumb_butterfly(rumb_ctx *ctx, int n, int dtype, const void *in, voi
 /* rumb_butterfly with no device allocation (no counterpart in the reference). It stages the slab
  * in a 4 MiB static device array, one per device, instead of the context's scratch, so it holds
  * n <= 16 in either dtype; a larger slab returns RUMB_E_INVAL. The first call on each device looks
- * the array up (cudaGetSymbolAddress) and loads the kernels it launches: make that call before any
- * region where nothing may allocate. Nothing in the array has to start at zero. Every context on a
- * device shares the array: calls on one device must not overlap (they race; nothing serializes
- * them). */
+ * the array up (cudaGetSymbolAddress). Which kernels a call launches depends on n and dtype (n <= 5
+ * takes one small butterfly kernel, larger n one transform kernel per window of the plan), and with
+ * lazy module loading (CUDA's default) the first launch of a kernel can still allocate in the
+ * driver: before a region where nothing may allocate, make one call for every (n, dtype) the region
+ * will use. Nothing in the array has to start at zero. Every context on a device shares the array:
+ * calls on one device must not overlap (they race; nothing serializes them). */
 RUMB_API int rumb_butterfly_noalloc(rumb_ctx *ctx, int n, int dtype, const void *in, void *out, double a,
                                     double b, double c, double d);
 /* out = the per-menu simplex prox of v (all 2^n - 1 menus); xhat holds p_hat at observed entries,
@@ -163,6 +165,14 @@ typedef struct {
 
 /* called once per check with (iterations, seconds since the call, phi, best ub, best lb) */
 typedef void (*rumb_trace_fn)(void *user, long long iter, double wall_s, double phi, double ub, double lb);
+
+/* Device bytes one rumb_bm_solve of (n, mp, dtype) allocates: the state and scratch slabs (both
+ * dtypes for RUMB_MIXED), the snapshot slab of overlapped checks, the float64 certificate slabs and
+ * node arrays, the observation masks and the uploaded rows -- what the caller compares with
+ * rumb_mem_info's free bytes before choosing the method. Computed without touching the device;
+ * ctx may be NULL. 2 <= n <= 30, mp >= 1, else RUMB_E_INVAL. Replaces the reference's planner
+ * sizing (_PLAN["bm_admm"] with _bm_admm_bytes, solver/rum_solver.py:735-770). */
+RUMB_API int rumb_bm_plan(rumb_ctx *ctx, int n, long long mp, int dtype, size_t *bytes);
 
 /* Certified solve. warm: start from a kept state (NULL: the cold start prox(xhat)); keep: if not
  * NULL, receives a new handle holding the final state (free with rumb_bm_state_destroy);
@@ -307,11 +317,12 @@ typedef struct {
     double bytes_per_launch;  /* algorithmic bytes one launch must move */
 } rumb_kernel_stat;
 
-/* Runs `warmup` untimed ADMM iterations from the cold start, then `iters` iterations (plus one
- * float64 check when par->lb_every > 0) with an event pair around every kernel launch, and
- * reports per kernel:
- * launches, total time and algorithmic bytes per launch. Fills at most cap entries. This is the
- * library's counterpart of the reference's per-phase timers (solver/flow_cg/solver.py:174-188). */
+/* Runs `warmup` untimed ADMM iterations from the cold start, then captures `iters` iterations
+ * (plus one float64 check when par->lb_every > 0) as a CUDA graph with an event pair around every
+ * kernel launch, replays it twice and reports per kernel of the second replay: launches, total
+ * time and algorithmic bytes per launch -- the kernels timed as a solve's graph replays run them.
+ * Fills at most cap entries. This is the library's counterpart of the reference's per-phase
+ * timers (solver/flow_cg/solver.py:174-188). */
 RUMB_API int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int warmup,
                              int iters, rumb_kernel_stat *stats, int cap, int *count);
 

@@ -182,6 +182,15 @@ int rumb_fw_lb64(rumb_ctx *ctx, int n, long long mp, const uint32_t *menu, const
     RUMB_API_END
 }
 
+int rumb_bm_plan(rumb_ctx *ctx, int n, long long mp, int dtype, size_t *bytes) {
+    (void)ctx;
+    RUMB_API_BEGIN
+    if (!bytes) rumb::fail(RUMB_E_INVAL, "bm_plan: bytes is NULL");
+    *bytes = rumb::bm_plan_bytes(n, mp, dtype);
+    return RUMB_OK;
+    RUMB_API_END
+}
+
 int rumb_bm_solve(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, const rumb_bm_state *warm,
                   rumb_bm_state **keep, rumb_bm_result *res, double *p_fit, rumb_trace_fn trace, void *user) {
     RUMB_API_BEGIN

@@ -561,6 +561,7 @@ struct BmCoef {
     double Qt[4], Q[4], AQ[4];
     std::vector<double> diag;   // by popcount, nb + 1 entries
     int lo_bits = 12;           // transform window split (tuned)
+    int prox_form = PROX_TILE;  // prox kernel form (tuned)
 };
 
 static BmCoef make_coef(int n, double beta, double alpha, double p) {
@@ -691,9 +692,9 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
     P.active = I.active;
     if (g_prof) {
         double S = (double)P.Nloc * n * K, e = sizeof(T);
-        prof_begin(e == 8 ? "prox_tile<f64>" : "prox_tile<f32>", 5.0 * S * e + 4.0 * (1LL << n), st);
+        prof_begin(e == 8 ? "prox<f64>" : "prox<f32>", 5.0 * S * e + 4.0 * (1LL << n), st);
     }
-    launch_prox_tile<T>(P, st, K);
+    launch_prox_tile<T>(P, st, K, C.prox_form);
     prof_end(st);
 }
 
@@ -733,36 +734,79 @@ static void enqueue_cold_start(BmWork<T> &W, const BmCoef &C, int n, cudaStream_
     for (DevBuf *b : {&W.s, &W.y, &W.z}) RUMB_CUDA(cudaMemsetAsync(b->ptr, 0, (size_t)m2 * sizeof(T), st));
 }
 
-// Picks the low-window size of the transform passes by timing a few iterations of each candidate
-// on the workspace (cached per context, n and dtype). The state is reset by the caller.
+// The iteration's autotuner: times a few iterations of each candidate on the workspace and keeps
+// the fastest, one knob at a time -- the transform passes' low-window size (10, 11 or 12 bits;
+// it sets the high-window split), then the prox kernel's form (the shared-memory tile, or 2, 4 or
+// 8 lanes per menu). Cached per context, n and dtype; the state is reset by the caller. The
+// environment variable RUMB_PROX_FORM (0 tile, 1..3 lanes 2/4/8) pins the prox form.
+static int forced_prox_form() {
+    const char *e = getenv("RUMB_PROX_FORM");
+    if (!e || !*e) return -1;
+    int v = atoi(e);
+    return (v >= 0 && v < PROX_FORMS) ? v : -1;
+}
+
 template <class T>
-static int tune_lo_bits(Ctx &c, BmWork<T> &W, BmCoef C, int n, cudaStream_t st) {
+static void tune_iteration(Ctx &c, BmWork<T> &W, BmCoef &C, int n, cudaStream_t st) {
     auto key = std::make_pair(n, (int)sizeof(T));
-    auto it = c.lo_bits.find(key);
-    if (it != c.lo_bits.end()) return it->second;
-    int best = 12;
-    if (n - 1 > 10) {
-        float best_ms = 1e30f;
+    auto it = c.tuned.find(key);
+    if (it == c.tuned.end()) {
+        BmCoef K = C;
         cudaEvent_t a, b;
         RUMB_CUDA(cudaEventCreate(&a));
         RUMB_CUDA(cudaEventCreate(&b));
-        for (int lb : {10, 11, 12}) {
-            if (lb > n - 1) continue;
-            C.lo_bits = lb;
-            for (int i = 0; i < 2; ++i) enqueue_iteration<T>(W, C, n, st);
+        auto time_it = [&]() -> float {
+            for (int i = 0; i < 2; ++i) enqueue_iteration<T>(W, K, n, st);
             RUMB_CUDA(cudaEventRecord(a, st));
-            for (int i = 0; i < 6; ++i) enqueue_iteration<T>(W, C, n, st);
+            for (int i = 0; i < 6; ++i) enqueue_iteration<T>(W, K, n, st);
             RUMB_CUDA(cudaEventRecord(b, st));
             RUMB_CUDA(cudaEventSynchronize(b));
             float ms = 0.f;
             RUMB_CUDA(cudaEventElapsedTime(&ms, a, b));
-            if (ms < best_ms) { best_ms = ms; best = lb; }
+            return ms;
+        };
+        int best_lo = 12, best_form = n <= PROX_LANES_MAX_N ? PROX_LANES4 : PROX_TILE;
+        if (n >= PT_M + 1) {
+            K.prox_form = best_form;
+            if (n - 1 > 10) {
+                float best_ms = 1e30f;
+                for (int lb : {10, 11, 12}) {
+                    if (lb > n - 1) continue;
+                    K.lo_bits = lb;
+                    float ms = time_it();
+                    if (ms < best_ms) { best_ms = ms; best_lo = lb; }
+                }
+            }
+            K.lo_bits = best_lo;
+            if (n <= PROX_LANES_MAX_N) {
+                float best_ms = 1e30f;
+                for (int f = 0; f < PROX_FORMS; ++f) {
+                    K.prox_form = f;
+                    float ms = time_it();
+                    if (ms < best_ms) { best_ms = ms; best_form = f; }
+                }
+            }
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
+        it = c.tuned.emplace(key, std::make_pair(best_lo, best_form)).first;
     }
-    c.lo_bits[key] = best;
-    return best;
+    C.lo_bits = it->second.first;
+    C.prox_form = it->second.second;
+    int f = forced_prox_form();
+    if (f >= 0) C.prox_form = f;
+}
+
+// The tuned schedule of (n, dtype) when it is known, else the defaults.
+template <class T>
+static void tuned_or_default(Ctx &c, BmCoef &C, int n) {
+    auto it = c.tuned.find(std::make_pair(n, (int)sizeof(T)));
+    if (it != c.tuned.end()) {
+        C.lo_bits = it->second.first;
+        C.prox_form = it->second.second;
+    }
+    int f = forced_prox_form();
+    if (f >= 0) C.prox_form = f;
 }
 
 // ----------------------------------------------------------------- problem upload
@@ -1128,6 +1172,25 @@ static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const r
     return true;
 }
 
+// Device bytes of one solve, counted from the buffers it ensures: BmWork (9 slabs, the snapshot
+// slab, observation bits, per-menu observed masks, diagonal, error word) per state dtype, the
+// float64 certificate (2 slabs, 3 node arrays, 4 row arrays, result words), the popcount-ordered
+// node ids and the uploaded rows.
+size_t bm_plan_bytes(int n, ll mp, int dtype) {
+    if (n < 2 || n > 30) fail(RUMB_E_INVAL, "bm_plan: 2 <= n <= 30");
+    if (mp < 1) fail(RUMB_E_INVAL, "bm_plan: mp >= 1");
+    if (dtype != RUMB_F64 && dtype != RUMB_F32 && dtype != RUMB_MIXED) fail(RUMB_E_INVAL, "bm_plan: dtype");
+    const size_t m2 = (size_t)n << (n - 1), N = (size_t)1 << n;
+    auto work = [&](size_t e) { return 10 * m2 * e + (m2 + 31) / 32 * 4 + 4 * N + 64 * e + 16; };
+    size_t b = 0;
+    if (dtype != RUMB_F64) b += work(4);
+    if (dtype != RUMB_F32) b += work(8);
+    b += 2 * m2 * 8 + 3 * N * 8 + 4 * (size_t)mp * 8 + R_SLOTS * 8;   // certificate
+    b += 4 * N;                                                        // node ids by popcount
+    b += 16 * (size_t)mp;                                              // rows: menu, alt, p
+    return b;
+}
+
 int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_bm_state *warm,
              rumb_bm_state **keep, rumb_bm_result *out, double *p_fit, rumb_trace_fn trace, void *user) {
     check_problem(pr);
@@ -1168,13 +1231,13 @@ int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const
     BmCoef C64 = C;
     if (W32) {
         enqueue_cold_start<float>(*W32, C, n, st);
-        C.lo_bits = tune_lo_bits<float>(c, *W32, C, n, st);
+        tune_iteration<float>(c, *W32, C, n, st);
     }
     if (W64) {
         enqueue_cold_start<double>(*W64, C64, n, st);
-        C64.lo_bits = tune_lo_bits<double>(c, *W64, C64, n, st);
+        tune_iteration<double>(c, *W64, C64, n, st);
     }
-    if (!W32) C.lo_bits = C64.lo_bits;
+    if (!W32) C = C64;
     if (use32) {
         if (warm) copy_state_in<float>(*W32, *warm, m2, st);
         else enqueue_cold_start<float>(*W32, C, n, st);
@@ -1258,6 +1321,7 @@ int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, voi
         std::vector<T> dg(C.diag.begin(), C.diag.end());
         RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
         size_t sb = (size_t)m2 * sizeof(T);
+        tuned_or_default<T>(c, C, n);
         if (cold) {
             enqueue_cold_start<T>(W, C, n, st);
         } else {
@@ -1310,22 +1374,36 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         std::vector<T> dg(C.diag.begin(), C.diag.end());
         RUMB_CUDA(cudaMemcpyAsync(W.diag.ptr, dg.data(), dg.size() * sizeof(T), cudaMemcpyHostToDevice, st));
         enqueue_cold_start<T>(W, C, n, st);
-        C.lo_bits = tune_lo_bits<T>(c, W, C, n, st);
+        tune_iteration<T>(c, W, C, n, st);
         enqueue_cold_start<T>(W, C, n, st);
         for (int i = 0; i < std::max(warmup, 3); ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
         RUMB_CUDA(cudaStreamSynchronize(st));
+        // the profiled iterations and one check captured as a CUDA graph, as a solve replays them,
+        // with an event recorded before and after every kernel; the graph runs twice and the
+        // second run's events are read
+        for (int i = 0; i < 64 * (iters + 4); ++i) {
+            cudaEvent_t e;
+            RUMB_CUDA(cudaEventCreate(&e));
+            prof.pool.push_back(e);
+        }
+        Graph gp;
         g_prof = &prof;
         try {
-            for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
-            if (par->lb_every > 0) {
-                enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
-                enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
-            }
+            gp.capture(st, [&] {
+                for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
+                if (par->lb_every > 0) {
+                    enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
+                    enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+                }
+            });
         } catch (...) {
             g_prof = nullptr;
             throw;
         }
         g_prof = nullptr;
+        gp.launch(st);
+        RUMB_CUDA(cudaStreamSynchronize(st));
+        gp.launch(st);
         RUMB_CUDA(cudaStreamSynchronize(st));
     };
     if (par->dtype == RUMB_F64) run(double());
@@ -1470,11 +1548,8 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
     I.slots = K;
     I.bstride = m2;
     I.active = W.active.template as<int>();
-    // the transform split tuned on slot 0's single-draw workspace when not known yet
-    {
-        auto key = std::make_pair(n, (int)sizeof(T));
-        if (c.lo_bits.count(key)) C.lo_bits = c.lo_bits[key];
-    }
+    // the schedule tuned on a single-draw workspace, when known
+    tuned_or_default<T>(c, C, n);
     DevBuf pbuf;                                    // the draws' rows, uploaded once
     pbuf.ensure((size_t)B * (size_t)mp * 8);
     RUMB_CUDA(cudaMemcpyAsync(pbuf.ptr, P, (size_t)B * (size_t)mp * 8, cudaMemcpyHostToDevice, st));

@@ -3,6 +3,7 @@
 #include "ctx.cuh"
 
 namespace rumb {
+size_t bm_plan_bytes(int n, ll mp, int dtype);
 int bm_solve(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, const rumb_bm_state *warm,
              rumb_bm_state **keep, rumb_bm_result *out, double *p_fit, rumb_trace_fn trace, void *user);
 int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, void *x2, void *s, void *y, void *z,

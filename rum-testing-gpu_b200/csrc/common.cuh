@@ -114,7 +114,8 @@ inline int num_sms(int dev) {
 // ---------------------------------------------------------------- launch profiler
 // When a profiler is installed on the calling thread (rumb_bm_profile), every kernel launch site
 // brackets its launch with CUDA events and reports its algorithmic bytes; otherwise these are
-// no-ops.
+// no-ops. Recorded while a stream is captured, the events become nodes of the CUDA graph and time
+// the kernels as the graph replays them.
 struct ProfRec {
     std::string name;
     cudaEvent_t a, b;
@@ -123,14 +124,26 @@ struct ProfRec {
 struct Prof {
     cudaStream_t st = nullptr;
     std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> pool;     // events made ahead (a profile captured into a CUDA graph)
+    cudaEvent_t event() {
+        cudaEvent_t e = nullptr;
+        if (!pool.empty()) {
+            e = pool.back();
+            pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    }
+    ~Prof() {
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
 };
 extern thread_local Prof *g_prof;
 
 inline void prof_begin(const std::string &name, double bytes, cudaStream_t st) {
     if (!g_prof || st != g_prof->st) return;
-    ProfRec r{name, nullptr, nullptr, bytes};
-    cudaEventCreate(&r.a);
-    cudaEventCreate(&r.b);
+    ProfRec r{name, g_prof->event(), g_prof->event(), bytes};
     cudaEventRecord(r.a, st);
     g_prof->recs.push_back(r);
 }

@@ -28,7 +28,8 @@ struct Ctx {
     std::unique_ptr<BmWorkBase> batch64, batch32;  // batched-draw workspaces
     std::unique_ptr<BmWorkBase> cert;           // float64 certificate workspace
     std::unique_ptr<BmWorkBase> scratch;        // primitive calls' scratch
-    std::map<std::pair<int, int>, int> lo_bits; // tuned low-window size per (n, state bytes)
+    // the iteration's tuned schedule per (n, state bytes): transform low-window size, prox form
+    std::map<std::pair<int, int>, std::pair<int, int>> tuned;
     // overlapped checks: a second stream, its two events and pinned result words (made on first use)
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_snap = nullptr, ev_done = nullptr;

@@ -188,6 +188,162 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T
     }
 }
 
+// ---------------------------------------------------------------- lane-group form
+// G consecutive lanes share one menu S (a warp holds 32 / G consecutive menus); lane gl of the
+// group owns the members i = gl, gl + G, gl + 2G, ... of S. Every member's x, x2 and z are read
+// straight from the slab into registers and x2', z' written back: for i >= log2(32 / G) bit i of S
+// is the same for all the warp's menus, so the active lanes read 32 / G consecutive rests of block
+// i (one contiguous segment per member slot and lane parity), and for lower i half of them do.
+// Nothing is staged, no barrier is taken, and the loads of all of a lane's members are in flight
+// together. The threshold's sums, the support and the optimality test are reduced over the group
+// with xor shuffles (every lane of a group ends with the same bits, so the group takes one path).
+template <int G>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+    return G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+}
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned m) {
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(m, v, o);
+    return v;
+}
+template <int G>
+__device__ __forceinline__ uint32_t group_or(uint32_t v, unsigned m) {
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) v |= __shfl_xor_sync(m, v, o);
+    return v;
+}
+
+template <class T, int N, int G>
+__global__ void __launch_bounds__(256, G >= 4 ? 4 : 2) prox_lanes_kernel(ProxTileArgs<T> P) {
+    if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
+    const ll boff = (ll)blockIdx.y * P.bstride;
+    const T *X = P.x + boff;
+    T *X2 = P.x2 + boff, *Z = P.z + boff;
+    const T *XH = P.xhat + boff;
+    const ll Nloc = P.Nloc;
+    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const unsigned gm = group_mask<G>(lane);
+    const uint32_t S = (uint32_t)(((ll)blockIdx.x * blockDim.x + threadIdx.x) / G);
+    constexpr int J = (N + G - 1) / G;                      // member slots per lane
+    const int k = __popc(S);
+    const uint32_t wb = P.menu_obs[S];
+    const bool mixed = wb != 0 && wb != S;
+    const T one = (T)1, two = (T)2;
+    const double cw = (double)P.b2 + 2.0, cu = (double)P.b2, icw = 1.0 / cw, icu = 1.0 / cu;
+    T val[J], q[J];
+    uint32_t A0 = 0;
+    double s1 = 0.0, s2 = 0.0, f1 = 0.0, f2 = 0.0;
+    // pass 1 (as the tile form): xo, v, q = z - b2 xo; val = the value the threshold works on
+    // (the equal-curvature value, or v for a menu with observed and unobserved members)
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const int i = j * G + gl;
+        val[j] = (T)0;
+        q[j] = (T)0;
+        if (i < N && ((S >> i) & 1u)) {
+            const ll g = (ll)i * Nloc + (ll)cb32(S, i);
+            const T x2o = X2[g];
+            const T xo = P.alpha * X[g] + (one - P.alpha) * x2o;
+            const T zz = Z[g];
+            const T v = xo - P.ib2 * zz;
+            q[j] = zz - P.b2 * xo;
+            const bool w = (wb >> i) & 1u;
+            const T xh = w ? XH[g] : (T)0;
+            double ti, ic = 1.0;
+            if (mixed) {
+                val[j] = v;
+                ti = (double)P.b2 * (double)v + (w ? 2.0 * (double)xh : 0.0);
+                ic = w ? icw : icu;
+            } else {
+                val[j] = (P.b2 * v + two * (w ? one : (T)0) * xh) * (w ? P.inv_c1 : P.inv_c0);
+                ti = (double)val[j];
+            }
+            f1 += mixed ? ti * ic : ti;
+            f2 += ic;
+            if (x2o > (T)0) {
+                A0 |= 1u << i;
+                s1 += mixed ? ti * ic : ti;
+                s2 += ic;
+            }
+        }
+    }
+    auto t_of = [&](int j, int i) -> double {
+        double ti = (double)val[j];
+        if (mixed) ti = (double)P.b2 * ti + (((wb >> i) & 1u) ? 2.0 * (double)XH[(ll)i * Nloc + (ll)cb32(S, i)] : 0.0);
+        return ti;
+    };
+    A0 = group_or<G>(A0, gm);
+    s1 = group_sum<G>(s1, gm);
+    s2 = group_sum<G>(s2, gm);
+    double tau = 0.0;
+    bool ok = false;
+    if (k > 1 && A0 != 0) {
+        tau = (s1 - 1.0) / s2;
+        uint32_t bad = 0;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const int i = j * G + gl;
+            if (i < N && ((S >> i) & 1u)) {
+                const bool in = (A0 >> i) & 1u;
+                if (in != (t_of(j, i) > tau)) bad = 1;
+            }
+        }
+        ok = group_or<G>(bad, gm) == 0;
+    }
+    if (k > 1 && !ok) {
+        // Michelot's iteration from the full set (the active set only shrinks)
+        f1 = group_sum<G>(f1, gm);
+        f2 = group_sum<G>(f2, gm);
+        uint32_t A = S;
+        tau = (f1 - 1.0) / f2;
+        for (int round = 0; round < 32; ++round) {
+            uint32_t A2 = 0;
+            double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int i = j * G + gl;
+                if (i < N && ((A >> i) & 1u)) {
+                    const double ti = t_of(j, i);
+                    const double ic = mixed ? (((wb >> i) & 1u) ? icw : icu) : 1.0;
+                    if (ti > tau) {
+                        A2 |= 1u << i;
+                        a1 += mixed ? ti * ic : ti;
+                        a2 += ic;
+                    }
+                }
+            }
+            A2 = group_or<G>(A2, gm);
+            a1 = group_sum<G>(a1, gm);
+            a2 = group_sum<G>(a2, gm);
+            if (A2 == A) break;
+            A = A2;
+            tau = (a1 - 1.0) / a2;
+        }
+    }
+    // pass 2: u = the projection, x2' = u, z' = q + b2 u
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const int i = j * G + gl;
+        if (i < N && ((S >> i) & 1u)) {
+            const ll g = (ll)i * Nloc + (ll)cb32(S, i);
+            T u;
+            if (k == 1) {
+                u = one;
+            } else if (mixed) {
+                const bool w = (wb >> i) & 1u;
+                const double yv = (t_of(j, i) - tau) / (w ? cw : cu);
+                u = yv > 0.0 ? (T)yv : (T)0;
+            } else {
+                const double yv = (double)val[j] - tau;
+                u = yv > 0.0 ? (T)yv : (T)0;
+            }
+            X2[g] = u;
+            Z[g] = q[j] + P.b2 * u;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 template <class T, int N>
 static void launch_tile_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
@@ -199,14 +355,36 @@ static void launch_tile_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) 
     RUMB_LAUNCH("prox_tile_kernel");
 }
 
+template <class T, int N, int G>
+static void launch_lanes_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
+    dim3 grid((unsigned)(((1LL << N) * G) / 256), (unsigned)slots);
+    prox_lanes_kernel<T, N, G><<<grid, 256, 0, st>>>(P);
+    RUMB_LAUNCH("prox_lanes_kernel");
+}
+
+template <class T, int N>
+static void launch_form_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots, int form) {
+    switch (form) {
+        case PROX_LANES2: launch_lanes_n<T, N, 2>(P, st, slots); return;
+        case PROX_LANES4: launch_lanes_n<T, N, 4>(P, st, slots); return;
+        case PROX_LANES8: launch_lanes_n<T, N, 8>(P, st, slots); return;
+        default: launch_tile_n<T, N>(P, st, slots); return;
+    }
+}
+
 template <class T>
-void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
+void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots, int form) {
+    if (P.n > PROX_LANES_MAX_N) form = PROX_TILE;
     switch (P.n) {
 #define RUMB_PT_CASE(NN) \
-    case NN: launch_tile_n<T, NN>(P, st, slots); return;
+    case NN: launch_form_n<T, NN>(P, st, slots, form); return;
         RUMB_PT_CASE(8) RUMB_PT_CASE(9) RUMB_PT_CASE(10) RUMB_PT_CASE(11) RUMB_PT_CASE(12) RUMB_PT_CASE(13)
         RUMB_PT_CASE(14) RUMB_PT_CASE(15) RUMB_PT_CASE(16) RUMB_PT_CASE(17) RUMB_PT_CASE(18) RUMB_PT_CASE(19)
-        RUMB_PT_CASE(20) RUMB_PT_CASE(21) RUMB_PT_CASE(22) RUMB_PT_CASE(23) RUMB_PT_CASE(24) RUMB_PT_CASE(25)
+        RUMB_PT_CASE(20) RUMB_PT_CASE(21) RUMB_PT_CASE(22)
+#undef RUMB_PT_CASE
+#define RUMB_PT_CASE(NN) \
+    case NN: launch_tile_n<T, NN>(P, st, slots); return;
+        RUMB_PT_CASE(23) RUMB_PT_CASE(24) RUMB_PT_CASE(25)
         RUMB_PT_CASE(26) RUMB_PT_CASE(27) RUMB_PT_CASE(28) RUMB_PT_CASE(29) RUMB_PT_CASE(30)
 #undef RUMB_PT_CASE
     default: break;
@@ -214,8 +392,8 @@ void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     fail(RUMB_E_INVAL, "prox: 8 <= n <= 30");
 }
 
-template void launch_prox_tile<float>(const ProxTileArgs<float> &, cudaStream_t, int);
-template void launch_prox_tile<double>(const ProxTileArgs<double> &, cudaStream_t, int);
+template void launch_prox_tile<float>(const ProxTileArgs<float> &, cudaStream_t, int, int);
+template void launch_prox_tile<double>(const ProxTileArgs<double> &, cudaStream_t, int, int);
 
 // per-menu mask of observed members, from the observation bits of the slab
 __global__ void menu_obs_kernel(const uint32_t *obsbits, int n, ll Nloc, uint32_t *menu_obs) {

@@ -106,9 +106,15 @@ __device__ __forceinline__ ll pt_rstart(uint32_t base, int i, ll Nloc) {
     return (ll)i * Nloc + rest0;
 }
 
+// The forms of the prox kernel (csrc/prox.cu): the shared-memory tile, or G lanes per menu
+// reading the slab straight into registers (n <= PROX_LANES_MAX_N); picked per GPU, n and dtype
+// by timing (the iteration's autotuner).
+constexpr int PROX_TILE = 0, PROX_LANES2 = 1, PROX_LANES4 = 2, PROX_LANES8 = 3, PROX_FORMS = 4;
+constexpr int PROX_LANES_MAX_N = 22;
+
 // The prox for one dtype (csrc/prox.cu; grid.y = batched draws' slots).
 template <class T>
-void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots = 1);
+void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots = 1, int form = PROX_TILE);
 
 // menu_obs[S] = the observed members of menu S, from the slab's observation bits.
 void launch_menu_obs(const uint32_t *obsbits, int n, ll Nloc, uint32_t *menu_obs, cudaStream_t st);

@@ -129,6 +129,8 @@ _SIGS = {
     "rumb_cg_pricer_max64": ([_vp, _vp, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "rumb_bm_iterate": ([_vp, ctypes.POINTER(BMProblem), ctypes.POINTER(BMParams), _vp, _vp, _vp, _vp,
                          ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "rumb_bm_plan": ([_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)],
+                     ctypes.c_int),
 }
 
 _lib = None
@@ -149,6 +151,14 @@ def load():
                 f.restype = res
             _lib = L
     return _lib
+
+
+def bm_plan(n, mp, dtype):
+    """Device bytes one rumb_bm_solve of (n, mp, dtype) allocates (rumb_bm_plan; no GPU needed).
+    dtype: "float64", "float32" or "mixed"."""
+    out = ctypes.c_size_t()
+    check(load().rumb_bm_plan(None, int(n), int(mp), DTYPES[dtype], ctypes.byref(out)))
+    return int(out.value)
 
 
 def exported_symbols():

@@ -420,12 +420,12 @@ def choose_method(n, mp):
     return "flow_cg", "; ".join(why)
 
 
-# Device bytes per slab entry of one BM-ADMM solve in this library: 9 state/scratch slabs in the
-# state dtype, 2 float64 certificate slabs, 1 bit of observation mask.
-def _bm_admm_bytes(n, dtype):
-    m2 = n << (n - 1)
-    item = {"float64": 8, "float32": 4, "mixed": 12}[dtype]
-    return int(1.1 * (9 * item * m2 + 16 * m2 + m2 / 8 + 24 * (1 << n)))
+# Device bytes of one BM-ADMM solve in this library (rumb_bm_plan: the buffers the solve allocates,
+# both state dtypes for "mixed"), plus 10 % as the reference's planner keeps
+# (solver/rum_solver.py:735-737).
+def _bm_admm_bytes(n, dtype, mp=1):
+    from . import _lib
+    return int(1.1 * _lib.bm_plan(n, mp, dtype))
 
 
 def _plan_bm_admm(n, mp, a):
@@ -438,7 +438,7 @@ def _plan_bm_admm(n, mp, a):
         raise ValueError("bm_admm dtype must be 'auto', 'float64', 'float32' or 'mixed'")
     dt = "float64" if a["dtype"] == "auto" else a["dtype"]
     budget = defaults.AUTO["gpu_memory_fraction"] * gpu_free_bytes()
-    need = _bm_admm_bytes(n, dt)
+    need = _bm_admm_bytes(n, dt, mp)
     if need > budget:
         raise RuntimeError("bm_admm at n = %d in %s needs %.1f GB of GPU memory; %.1f GB may be used. Use flow_cg"
                            % (n, dt, need / 2 ** 30, budget / 2 ** 30))

@@ -50,3 +50,19 @@ def test_context_without_gpu_reports_nodev_or_works():
         assert st == _lib.E_NODEV, _lib.last_error()
         with pytest.raises(_lib.RumbError):
             _lib.Context(0)
+
+
+def test_bm_plan_counts_the_solve_buffers_without_a_gpu():
+    """rumb_bm_plan sizes a solve from (n, mp, dtype) alone: the state and scratch slabs, the
+    snapshot slab, the float64 certificate, the masks and the rows; bad sizes are refused."""
+    from rumb import _lib
+    n, mp = 18, 23650
+    m2, N = n << (n - 1), 1 << n
+    cert = 16 * m2 + 24 * N + 32 * mp + 64 + 4 * N + 16 * mp
+    work = lambda e: 10 * m2 * e + (m2 + 31) // 32 * 4 + 4 * N + 64 * e + 16
+    assert _lib.bm_plan(n, mp, "float64") == work(8) + cert
+    assert _lib.bm_plan(n, mp, "float32") == work(4) + cert
+    assert _lib.bm_plan(n, mp, "mixed") == work(4) + work(8) + cert
+    for bad in ((1, mp, "float64"), (31, mp, "float64"), (n, 0, "float64")):
+        with pytest.raises(_lib.RumbError):
+            _lib.bm_plan(*bad)

@@ -134,6 +134,29 @@ def test_iterates_track_oracle(ctx, case, dtype):
             assert d <= tol[total] * max(1.0, float(np.max(np.abs(getattr(bm, name))))), (name, total, d)
 
 
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
+@pytest.mark.parametrize("case", ["n10_all_k20", "n16_mix"])
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_prox_forms_track_oracle(ctx, monkeypatch, case, form, dtype):
+    """Every form of the iteration's prox kernel (RUMB_PROX_FORM: 0 the shared-memory tile, 1..3
+    two, four or eight lanes per menu reading the slab into registers) keeps the iterates on the
+    oracle's: float64 to 1e-10 after 10 iterations, float32 at its rounding floor."""
+    monkeypatch.setenv("RUMB_PROX_FORM", str(form))
+    n, menu, alt, p = _instance(case)
+    beta = O.beta_default(p.size)
+    dt = np.float64 if dtype == "float64" else np.float32
+    bm = O.BMOracle(n, menu, alt, p, dtype=dt)
+    prob = ctx.bm_problem(n, menu, alt, p)
+    par = ctx.bm_params(beta, dtype=dtype)
+    st = ctx.bm_iterate(prob, par, None, 10, cold_start=True)
+    bm.iterate(10)
+    tol = 1e-10 if dt == np.float64 else (1e-4 if n < 14 else 1e-3)
+    for name in ("x2", "s", "y", "z"):
+        ref = getattr(bm, name).astype(np.float64)
+        d = np.max(np.abs(st[name].astype(np.float64) - ref))
+        assert d <= tol * max(1.0, float(np.max(np.abs(ref)))), (name, d)
+
+
 def test_certified_solve_matches_oracle(ctx):
     n, menu, alt, p = config_instance("n10_all_k20")
     beta = O.beta_default(p.size)

@@ -33,3 +33,29 @@ def test_noalloc_size_limit(ctx):
     w = np.arange(16 << 15, dtype=np.float64)
     np.testing.assert_array_equal(ctx.butterfly_noalloc(16, w, 1.0, 1.0, 0.0, 1.0),
                                   ctx.butterfly(16, w, 1.0, 1.0, 0.0, 1.0))
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The point of the entry point: after a warm-up call for each (n, dtype) used, further calls
+    leave the device's free memory unchanged. The same check on rumb_butterfly, whose context
+    scratch grows on first use, sees the free memory drop by the slab (4 MiB at n = 16 float64),
+    which shows the check can fail."""
+    c = _lib.Context(0)
+    try:
+        n = 16
+        v = np.random.default_rng(3).standard_normal(n << (n - 1))
+        ref = c.butterfly_noalloc(n, v, *COEFS[0])                # warm-up: symbol lookup, kernel loads
+        c.sync()
+        free0, _ = c.mem_info()
+        for k in COEFS:
+            c.butterfly_noalloc(n, v, *k)
+        c.sync()
+        free1, _ = c.mem_info()
+        assert free1 == free0, (free0, free1)
+        np.testing.assert_array_equal(c.butterfly_noalloc(n, v, *COEFS[0]), ref)
+        c.butterfly(n, v, *COEFS[0])                               # first use of the context scratch
+        c.sync()
+        free2, _ = c.mem_info()
+        assert free0 - free2 >= (n << (n - 1)) * 8, (free0, free2)
+    finally:
+        c.close()
