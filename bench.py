@@ -16,15 +16,21 @@ solve from the cold start: float64 upper and lower bound every 50 iterations unt
 
 value   solves/s with the instance already in HBM (device pointers), all ranks summed
 e2e     the same through the C ABI from host buffers: rows uploaded and p_fit read back per solve
-roofline, for the kernel with the largest time share in an eager profile of 20 iterations (after
-        2000 untimed ones): algorithmic bytes per launch / its CUDA-event launch time, against
-        MEASURED_PEAKS.json hbm_gbs
+roofline, for the kernel with the largest time share over 20 iterations and one check (after 2000
+        untimed iterations), captured as a CUDA graph with events around every kernel and
+        replayed: algorithmic bytes per launch / its launch time, against MEASURED_PEAKS.json
+        hbm_gbs; traffic = DRAM bytes per launch from the committed ncu summary of the same kernel
+        source (profiles/), null when there is none for the source built now
+reference_kernels   one certified solve of the same workload by the reference's own float64
+        kernels (its source strings compiled by NVRTC, replayed with its host sequence:
+        baseline/ref_replay.py), and value / its solves/s
 gpu_launches   the library's own count of the kernels the timed solves launched
 cpu_baseline   the oracle (C restatement of the reference's iteration and certificate) on the host,
-        a bounded sample of iterations scaled to solves/s by this run's iteration count
+        a bounded sample of iterations extrapolated to solves/s by this run's iteration count
 
---impl reference times the reference's CPU path -- the oracle port, all host threads -- on the
-same workload and prints its line with "impl": "reference".
+--impl reference times the reference's CPU path -- the oracle port, all host threads -- on a
+bounded sample per step, extrapolated by the iteration count of the reference's own kernels on the
+same workload, and prints its line with "impl": "reference" and "extrapolated": true.
 
 Multi-GPU: a single solve does not shard (the prox couples every alternative of a menu each
 iteration), so N GPUs run N replicas of the solve (weak scaling, no collective on the data path);
@@ -49,15 +55,9 @@ WORKLOAD = "n18_d1pct_k50"
 METRIC = "n=18 BM-ADMM certified solves/s at abs gap 1e-5"
 ABS_TOL = 1e-5
 CHECK = 50
-# Iterations of the float64 certified solve of this seeded workload (the float64 library path
-# and the oracle follow the same trajectory; checked at n = 10 by tests/test_gpu_bm.py); the
-# reference arm, which runs only a sample, scales by it.
-CERT_ITERS_F64 = 43800
 # iterations run before the profiled ones: the roofline kernel is timed mid-solve
 PROFILE_WARMUP = 2000
-# DRAM bytes (read + write) per launch of the dominant kernel, from the ncu capture summarised in
-# profiles/prox_tile_n18_f64.md (same workload, float64 state)
-NCU_TRAFFIC = {"prox_tile<f64>": 60.49e6 + 0.446e6}
+PROFILES = os.path.join(ROOT, "profiles")
 
 
 def _env_int(k, d):
@@ -73,6 +73,70 @@ def load_peaks():
         d = json.load(open(path))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+# the kernel sources whose digest a committed ncu summary must match for its DRAM figure to count
+KERNEL_SOURCES = {"prox": ("prox.cu", "prox.cuh"), "xform": ("xform.cuh",)}
+
+
+def source_digest(kernel):
+    import hashlib
+    files = next((v for k, v in KERNEL_SOURCES.items() if kernel.startswith(k)), None)
+    if files is None:
+        return None
+    h = hashlib.sha256()
+    for f in files:
+        h.update(open(os.path.join(ROOT, "rum-testing-gpu_b200", "csrc", f), "rb").read())
+    return h.hexdigest()[:16]
+
+
+def kernel_traffic(kernel):
+    """(DRAM bytes read + written per launch, summary file) of `kernel` from the committed ncu
+    summaries in profiles/: a summary names `kernel:`, `source_sha256:` and
+    `dram_bytes_per_launch:` on lines of their own, and counts only when its digest is the digest of
+    the kernel source built now; otherwise (None, None)."""
+    want = source_digest(kernel)
+    if want is None or not os.path.isdir(PROFILES):
+        return None, None
+    for f in sorted(os.listdir(PROFILES)):
+        if not f.endswith(".md"):
+            continue
+        kv = {}
+        for line in open(os.path.join(PROFILES, f)):
+            line = line.strip().strip("`")
+            for key in ("kernel:", "source_sha256:", "dram_bytes_per_launch:"):
+                if line.startswith(key):
+                    kv[key[:-1]] = line[len(key):].strip()
+        if kv.get("kernel") == kernel and kv.get("source_sha256") == want and "dram_bytes_per_launch" in kv:
+            return float(kv["dram_bytes_per_launch"]), f
+    return None, None
+
+
+def reference_kernels_leg(n, menu, alt, p, beta):
+    """One certified float64 solve of the workload by the reference's own kernels (its source
+    strings NVRTC-compiled into baseline/_ref and replayed with its host sequence: one_iter as a
+    CUDA graph with its calibrated butterfly plan, the float64 push and lower bound every `check`
+    iterations with the runner's hooks, solver/bm_admm/solver.py:148-377,
+    solver/rum_solver.py:879-905), timed on the wall clock with the device synchronized on both
+    sides; setup (compilation, calibration, cold start) excluded."""
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    import ref_replay
+    if not ref_replay.available():
+        return {"unavailable": "baseline/_ref not built: the reference's source tree was absent at build time"}
+    import torch
+    r = ref_replay.BMReplay(n, menu, alt, p, beta)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = r.solve(abs_tol=ABS_TOL, check=CHECK, lb_every=1)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    del r
+    torch.cuda.empty_cache()
+    return {"impl": "the reference's float64 solve_kadmm_v2 kernels, replayed on this GPU",
+            "s_per_solve": wall, "solves_per_s": 1.0 / wall, "iters": int(res["iters"]),
+            "checks": int(res["checks"]), "ms_per_iter": 1e3 * res["iter_s"] / max(1, res["iters"]),
+            "ms_per_check": 1e3 * res["check_s"] / max(1, res["checks"]), "ub": res["ub"], "lb": res["lb"],
+            "stop": res["stop_reason"]}
 
 
 class ClockSampler:
@@ -151,28 +215,51 @@ def cpu_sample(n, menu, alt, p, threads, iters_per_solve, checks_per_solve, samp
     t_chk = time.perf_counter() - t0
     per_solve = iters_per_solve * t_it + checks_per_solve * t_chk
     desc = ("%d float64 ADMM iterations + 1 float64 check (push + lower bound) of %s on %d thread(s): "
-            "%.1f ms/iteration, %.1f ms/check, scaled to %d iterations and %d checks per certified solve"
+            "%.1f ms/iteration, %.1f ms/check, extrapolated to %d iterations and %d checks per certified solve"
             % (sample_iters, WORKLOAD, used, 1e3 * t_it, 1e3 * t_chk, iters_per_solve, checks_per_solve))
     return 1.0 / per_solve, desc, used
 
 
 def run_reference(args, rank):
-    """The reference arm: the reference's CPU path (the oracle port) with every host thread."""
+    """The reference arm: the reference's CPU path (the oracle port of its iteration and float64
+    check) on every host thread, on a bounded sample of iterations per step, extrapolated to a
+    certified solve by the iteration and check counts of the reference's own float64 kernels on
+    this workload (one solve replayed on the GPU before the timed steps)."""
     if rank != 0:
         return
     n, menu, alt, p = instance()
-    iters = CERT_ITERS_F64 or 10000
-    checks = iters // CHECK
+    beta = beta_rule(p.size)
+    iters = checks = None
+    source = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            leg = reference_kernels_leg(n, menu, alt, p, beta)
+            if "iters" in leg:
+                iters, checks = leg["iters"], leg["checks"]
+                source = "counted by one certified solve of the reference's own float64 kernels (replayed on the GPU)"
+            else:
+                source = leg.get("unavailable")
+    except Exception as e:                                  # no GPU or no reference kernels: say so
+        source = "reference kernels unavailable (%s)" % str(e).splitlines()[0][:120]
+    if iters is None:
+        line = {"impl": "reference", "unavailable": "the iteration count of a certified solve needs the reference's "
+                "kernels on a GPU: " + (source or "no GPU")}
+        print(json.dumps(line), flush=True)
+        return
     vals = []
     desc, used = "", 0
+    sample = 10
     for i in range(args.warmup + args.steps):
-        v, desc, used = cpu_sample(n, menu, alt, p, 0, iters, checks, sample_iters=10)
+        v, desc, used = cpu_sample(n, menu, alt, p, 0, iters, checks, sample_iters=sample)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "extrapolated": True, "sample_iters": sample, "iters_per_solve": iters, "checks_per_solve": checks,
+            "iters_source": source,
             "config": {"workload": WORKLOAD, "n": n, "cells": int(p.size), "abs_tol": ABS_TOL, "check": CHECK,
                        "iters_per_solve": iters},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": used, "kind": "port", "sample": desc},
@@ -214,6 +301,17 @@ def pricing_sweeps(ctx, stream, sweeps=20):
             "subset_tests_per_s": out["subset_tests_per_sweep"] / (ms * 1e-3),
             "list_bytes_per_sweep": list_bytes, "list_gb_per_s": list_bytes / (ms * 1e-3) / 1e9}
         pr.close()
+    # the reference's own pricing kernels on the same scores (layer launches only: a lower bound)
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    import ref_replay
+    if ref_replay.available():
+        ref = ref_replay.time_pricing(menus, offsets, scores.cpu().numpy(), n)
+        out["reference_kernels"] = {"u24_ms_per_sweep": ref["u24_layers_ms"], "u16_ms_per_sweep": ref["u16_layers_ms"],
+                                    "mask_ms_per_sweep": ref["mask_layers_ms"],
+                                    "note": "the reference's layer kernels alone (no backtrace, no reads): a lower "
+                                            "bound of its sweep"}
+        for mode in ("u24", "u16", "mask"):
+            out["speedup_vs_reference_" + mode] = ref[mode + "_layers_ms"] / out[mode]["ms_per_sweep"]
     return out
 
 
@@ -446,14 +544,22 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step_ms, e2e_ms = float(t[0]), float(t[1])
 
-    # roofline of the dominant kernel: an eager profile (CUDA events around every launch on the
-    # library's stream) of 20 iterations and one check, after PROFILE_WARMUP iterations
+    # roofline of the dominant kernel: 20 iterations and one check after PROFILE_WARMUP iterations,
+    # captured as a CUDA graph with CUDA events around every kernel and replayed (rumb_bm_profile)
     prof = ctx.bm_profile((prob_dev, None), par, iters=20, warmup=PROFILE_WARMUP)
     top = max(prof, key=lambda k: k["total_ms"])
     tot = sum(k["total_ms"] for k in prof)
     per_launch_ms = top["total_ms"] / top["launches"]
     peak, peak_kind = load_peaks()
     achieved = top["bytes_per_launch"] / (per_launch_ms * 1e-3) / 1e9
+    traffic, traffic_src = kernel_traffic(top["name"])
+    # the reference's own float64 kernels on the same workload and GPU (rank 0, after the timing)
+    ref_leg = None
+    if rank == 0:
+        try:
+            ref_leg = reference_kernels_leg(n, menu, alt, p, beta)
+        except Exception as e:
+            ref_leg = {"unavailable": str(e).splitlines()[0][:200]}
 
     if world > 1:
         dist.barrier()
@@ -486,7 +592,14 @@ def main():
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "share": top["total_ms"] / tot if tot > 0 else None,
                      "bytes_per_launch": top["bytes_per_launch"], "launch_ms": per_launch_ms,
-                     "traffic": NCU_TRAFFIC.get(top["name"])},
+                     "timing": "CUDA events around each kernel inside the replayed CUDA graph",
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "source_sha256": source_digest(top["name"])},
+        # one iteration's kernels under graph replay (the check's plain transforms left out)
+        "iteration_ms": sum(k["total_ms"] for k in prof if ",plain>" not in k["name"]) / 20.0,
+        "reference_kernels": ref_leg,
+        "speedup_vs_reference_kernels": (value * ref_leg["s_per_solve"]
+                                         if ref_leg and "s_per_solve" in ref_leg else None),
         "kernels": [{"name": k["name"], "share": round(k["total_ms"] / tot, 4),
                      "us_per_launch": round(1e3 * k["total_ms"] / k["launches"], 2),
                      "gbs": round(k["bytes_per_launch"] / (k["total_ms"] / k["launches"] * 1e-3) / 1e9, 1)}
