@@ -283,7 +283,9 @@ def solve_cg(prob, p, **kw):
 
 def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi_ub_target=None, gap_rel_tol=None,
               gap_abs_tol=None, init_columns=None, init_lambda=None, early_ub_check=False, lb_stop=None,
-              record_columns=False):
+              record_columns=False, on_price=None):
+    """on_price(it, scores, vmax, rank_pos, margin), when given, sees every pricing call with the
+    float32 residual it priced (x-major rows; read back from the master, so it costs a copy)."""
     n = prob.n
     t_setup = time.perf_counter()
     p_obs = np.asarray(p, dtype=np.float64)[prob.perm].astype(np.float32).astype(np.float64)
@@ -343,6 +345,8 @@ def _solve_cg(prob, p, rc_tol=0.0, max_iters=4000, time_limit_s=0.0, seed=0, phi
         margins.append(margin)
         if record_columns:
             picked.append(rank_pos.copy())
+        if on_price is not None:
+            on_price(it, (p_obs - master.p_out()).astype(np.float32), vmax, rank_pos, margin)
         fw_gap = (vmax + margin) - inner
         rc_final = fw_gap
         UB = float(np.sqrt(max(0.0, err2)))

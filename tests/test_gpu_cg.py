@@ -296,3 +296,21 @@ def test_pricer_matches_recorded_reference_kernels(ctx):
                 np.testing.assert_array_equal(np.asarray(steps, np.float32), g["%s_%s_steps" % (key, mode)])
                 assert abs(mg - float(g["%s_%s_margin" % (key, mode)])) <= 1e-6 * max(1.0, mg)
             pr.close()
+
+
+_CG3 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cg_config3.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(_CG3), reason="config 3 column sequence not recorded")
+@pytest.mark.parametrize("mode", ["u24", "u16"])
+def test_config3_column_sequence_matches_recorded_reference(ctx, mode):
+    """Flow-CG at n = 18, 0.5 % menus to abs 1e-5: every CG iteration's column
+    is the recorded one, which the reference's own pricing kernels picked on the same residual
+    (tests/golden/make_cg_golden.py), and the bracket is the recorded bracket."""
+    from rumb import flow_cg
+    g = np.load(_CG3)
+    n, m, a, p = config_instance("n18_d05pct_k50")
+    prob = flow_cg.CGProblem(ctx, n, m, a, mode)
+    res = flow_cg.solve_cg(prob, p, max_iters=4000, gap_abs_tol=1e-5, record_columns=True)
+    np.testing.assert_array_equal(np.array(res["picked"]), g["picked_" + mode])
+    assert [res["lb"], res["distance"]] == g["bracket_" + mode].tolist()

@@ -2,6 +2,8 @@
 source strings and replayed (baseline/build_ref.py, baseline/ref_replay.py): Flow-CG pricing must
 agree bit for bit (values, rankings, per-layer steps). Skipped where baseline/_ref was not built
 (it needs the reference's source tree at build time)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -151,3 +153,42 @@ def test_certified_bracket_matches_reference_float64(ctx, case, dtype):
     assert abs(res["lb"] - ref["lb"]) <= 1e-6, (res["lb"], ref["lb"])
     if dtype == "float64":
         assert res["iters"] == ref["iters"], (res["iters"], ref["iters"])
+
+
+# ------------------------------------------------------------------ Flow-CG config 3, every column
+def _config3_run(ctx, mode, check_reference):
+    """The library's CG loop on n18_d05pct_k50 (n = 18, 0.5 % menus, K = 50, N = 500) to abs 1e-5
+    in `mode`; at every iteration the residual it priced is priced again by the reference's own
+    stream kernels (when check_reference) and by the library's pricer directly."""
+    from rumb import flow_cg
+    n, m, a, p = config_instance("n18_d05pct_k50")
+    prob = flow_cg.CGProblem(ctx, n, m, a, mode)
+    menus, alts, _, offsets, _ = O.cg_layout(n, m, a, p)
+    bad = []
+
+    def on_price(it, scores, vmax, rank_pos, margin):
+        v2, r2, m2 = prob.pricer.price(scores)           # the residual read back is the one priced
+        if not (v2 == vmax and np.array_equal(r2, rank_pos)):
+            bad.append(("library", it))
+        if check_reference:
+            v_ref, r_ref, m_ref, _ = ref_replay.price_stream(menus, alts, scores, offsets, n, mode=mode)
+            if not (v_ref == vmax and np.array_equal(r_ref, rank_pos)):
+                bad.append(("reference", it, v_ref, vmax))
+
+    res = flow_cg.solve_cg(prob, p, max_iters=4000, gap_abs_tol=1e-5, record_columns=True, on_price=on_price)
+    return res, bad
+
+
+@pytest.mark.parametrize("mode", ["u24", "u16"])
+def test_config3_columns_match_reference_kernels_every_iteration(ctx, mode):
+    """BASELINE config 3's check: Flow-CG at n = 18, 0.5 % density, run to abs 1e-5, and the column
+    (the ranking) the library prices at every CG iteration is the one the reference's own
+    bf_stream_u24 / bf_stream_u16 kernels and backtrace pick on the same residual
+    (solver/flow_cg/pricing_stream.py:61-181,302-412, solver/flow_cg/solver.py:131-243)."""
+    res, bad = _config3_run(ctx, mode, check_reference=True)
+    assert res["stop_reason"] == "gap_abs", res["stop_reason"]
+    assert not bad, bad[:5]
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cg_config3.npz")
+    if os.path.exists(gold):
+        g = np.load(gold)
+        np.testing.assert_array_equal(np.array(res["picked"]), g["picked_" + mode])
