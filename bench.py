@@ -550,6 +550,8 @@ def main():
     top = max(prof, key=lambda k: k["total_ms"])
     tot = sum(k["total_ms"] for k in prof)
     per_launch_ms = top["total_ms"] / top["launches"]
+    if not per_launch_ms > 0:
+        raise RuntimeError("the kernel profile timed nothing: %s" % prof)
     peak, peak_kind = load_peaks()
     achieved = top["bytes_per_launch"] / (per_launch_ms * 1e-3) / 1e9
     traffic, traffic_src = kernel_traffic(top["name"])
@@ -592,7 +594,8 @@ def main():
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "share": top["total_ms"] / tot if tot > 0 else None,
                      "bytes_per_launch": top["bytes_per_launch"], "launch_ms": per_launch_ms,
-                     "timing": "CUDA events around each kernel inside the replayed CUDA graph",
+                     "timing": ("CUDA events around each kernel inside the replayed CUDA graph" if top.get("graph")
+                                else "CUDA events around eager launches"),
                      "traffic": traffic, "traffic_source": traffic_src,
                      "source_sha256": source_digest(top["name"])},
         # one iteration's kernels under graph replay (the check's plain transforms left out)

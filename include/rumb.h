@@ -315,12 +315,14 @@ typedef struct {
     long long launches;
     double total_ms;          /* CUDA-event time summed over the launches */
     double bytes_per_launch;  /* algorithmic bytes one launch must move */
+    int graph;                /* 1: timed inside the replayed CUDA graph; 0: eager launches */
 } rumb_kernel_stat;
 
 /* Runs `warmup` untimed ADMM iterations from the cold start, then captures `iters` iterations
  * (plus one float64 check when par->lb_every > 0) as a CUDA graph with an event pair around every
  * kernel launch, replays it twice and reports per kernel of the second replay: launches, total
- * time and algorithmic bytes per launch -- the kernels timed as a solve's graph replays run them.
+ * time and algorithmic bytes per launch -- the kernels timed as a solve's graph replays run them
+ * (where the driver cannot time a graph's events, eager launches instead; `graph` says which).
  * Fills at most cap entries. This is the library's counterpart of the reference's per-phase
  * timers (solver/flow_cg/solver.py:174-188). */
 RUMB_API int rumb_bm_profile(rumb_ctx *ctx, const rumb_bm_problem *prob, const rumb_bm_params *par, int warmup,

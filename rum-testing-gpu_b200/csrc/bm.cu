@@ -1365,6 +1365,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
     BmCoef C = make_coef(n, par->beta, par->alpha, par->precond_p);
     Prof prof;
     prof.st = st;
+    bool prof_graph = true;
     auto run = [&](auto tag) {
         using T = decltype(tag);
         BmWork<T> &W = bm_work<T>(c);
@@ -1378,9 +1379,23 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         enqueue_cold_start<T>(W, C, n, st);
         for (int i = 0; i < std::max(warmup, 3); ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
         RUMB_CUDA(cudaStreamSynchronize(st));
+        // one check first, so that its cached tables exist before the capture (no allocation inside)
+        if (par->lb_every > 0) {
+            enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
+            enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+            RUMB_CUDA(cudaStreamSynchronize(st));
+        }
+        auto body = [&] {
+            for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
+            if (par->lb_every > 0) {
+                enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
+                enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
+            }
+        };
         // the profiled iterations and one check captured as a CUDA graph, as a solve replays them,
         // with an event recorded before and after every kernel; the graph runs twice and the
-        // second run's events are read
+        // second run's events are read. Where the driver cannot time events recorded by a graph,
+        // the same launches run eagerly instead.
         for (int i = 0; i < 64 * (iters + 4); ++i) {
             cudaEvent_t e;
             RUMB_CUDA(cudaEventCreate(&e));
@@ -1389,13 +1404,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         Graph gp;
         g_prof = &prof;
         try {
-            gp.capture(st, [&] {
-                for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
-                if (par->lb_every > 0) {
-                    enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
-                    enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
-                }
-            });
+            gp.capture(st, body);
         } catch (...) {
             g_prof = nullptr;
             throw;
@@ -1405,6 +1414,25 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         RUMB_CUDA(cudaStreamSynchronize(st));
         gp.launch(st);
         RUMB_CUDA(cudaStreamSynchronize(st));
+        float probe = 0.f;
+        if (!prof.recs.empty() && cudaEventElapsedTime(&probe, prof.recs[0].a, prof.recs[0].b) != cudaSuccess) {
+            cudaGetLastError();
+            for (auto &r : prof.recs) {
+                cudaEventDestroy(r.a);
+                cudaEventDestroy(r.b);
+            }
+            prof.recs.clear();
+            prof_graph = false;
+            g_prof = &prof;
+            try {
+                body();
+            } catch (...) {
+                g_prof = nullptr;
+                throw;
+            }
+            g_prof = nullptr;
+            RUMB_CUDA(cudaStreamSynchronize(st));
+        }
     };
     if (par->dtype == RUMB_F64) run(double());
     else run(float());
@@ -1412,7 +1440,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
     std::map<std::string, rumb_kernel_stat> agg;
     for (auto &r : prof.recs) {
         float ms = 0.f;
-        if (r.b) cudaEventElapsedTime(&ms, r.a, r.b);
+        if (r.b) RUMB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
         cudaEventDestroy(r.a);
         if (r.b) cudaEventDestroy(r.b);
         auto it = agg.find(r.name);
@@ -1425,6 +1453,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         }
         it->second.launches += 1;
         it->second.total_ms += ms;
+        it->second.graph = prof_graph ? 1 : 0;
     }
     int k = 0;
     for (auto &nm : names) {

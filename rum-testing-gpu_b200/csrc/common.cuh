@@ -141,15 +141,23 @@ struct Prof {
 };
 extern thread_local Prof *g_prof;
 
+// An event recorded on st; while st is being captured the record becomes a node of the graph
+// (cudaEventRecordExternal), so each replay records it.
+inline void prof_record(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else cudaEventRecord(e, st);
+}
 inline void prof_begin(const std::string &name, double bytes, cudaStream_t st) {
     if (!g_prof || st != g_prof->st) return;
     ProfRec r{name, g_prof->event(), g_prof->event(), bytes};
-    cudaEventRecord(r.a, st);
+    prof_record(r.a, st);
     g_prof->recs.push_back(r);
 }
 inline void prof_end(cudaStream_t st) {
     if (!g_prof || st != g_prof->st || g_prof->recs.empty()) return;
-    cudaEventRecord(g_prof->recs.back().b, st);
+    prof_record(g_prof->recs.back().b, st);
 }
 
 inline unsigned grid_for(ll n, int block) {

@@ -67,7 +67,7 @@ class BatchInfo(ctypes.Structure):
 
 class KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 64), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
-                ("bytes_per_launch", ctypes.c_double)]
+                ("bytes_per_launch", ctypes.c_double), ("graph", ctypes.c_int)]
 
 
 TRACE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
@@ -359,7 +359,7 @@ class Context:
         check(load().rumb_bm_profile(self.h, ctypes.byref(pr), ctypes.byref(params), int(warmup), int(iters), arr, cap,
                                      ctypes.byref(cnt)))
         return [dict(name=arr[i].name.decode(), launches=arr[i].launches, total_ms=arr[i].total_ms,
-                     bytes_per_launch=arr[i].bytes_per_launch) for i in range(cnt.value)]
+                     bytes_per_launch=arr[i].bytes_per_launch, graph=bool(arr[i].graph)) for i in range(cnt.value)]
 
     def bm_iterate(self, problem, params, state, iters, cold_start=False):
         pr, _alive = problem if isinstance(problem, tuple) else (problem, None)
