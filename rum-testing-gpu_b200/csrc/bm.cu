@@ -562,6 +562,7 @@ struct BmCoef {
     std::vector<double> diag;   // by popcount, nb + 1 entries
     int lo_bits = 12;           // transform window split (tuned)
     int prox_form = PROX_TILE;  // prox kernel form (tuned)
+    int fuse = 1;               // two windows: P4 carries the next A' (three passes an iteration; tuned)
 };
 
 static BmCoef make_coef(int n, double beta, double alpha, double p) {
@@ -626,10 +627,14 @@ static IterPtrs<T> iter_ptrs(BmWork<T> &W) {
     return P;
 }
 
-// One ADMM iteration: 4 register-tiled transform passes (or 1 for n <= 13, more for n >= 21)
-// and the fused prox, for every slot of I (n >= 8).
+// One ADMM iteration: register-tiled transform passes (1 for n <= 13; with two windows 3, or 4
+// unfused; more for n >= 21) and the fused prox, for every slot of I (n >= 8). seq_i / seq_n place
+// the iteration in a sequence: with C.fuse and two windows, the first iteration of a sequence
+// starts with P1 on the low window, iteration i applies P2 and P4A on window Y (high for even i,
+// low for odd i) and P3 on the other, and the last one ends with a plain P4.
 template <class T>
-static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n, cudaStream_t st) {
+static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n, cudaStream_t st, int seq_i = 0,
+                                   int seq_n = 1) {
     T *x2 = I.x2, *s = I.s, *y = I.y, *z = I.z, *x = I.x, *Ax = I.Ax, *t1 = I.t1, *t2 = I.t2;
     const int K = I.slots;
     {
@@ -653,6 +658,26 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
             A.y = y; A.s = s; A.z = z; A.x2 = x2; A.out = x; A.s_io = s; A.y_io = y;
             A.k1 = kA; A.k2 = kQt; A.k3 = kQ; A.k4 = kAQ;
             xf_launch<T, T, K_FULL>(A, plan[0], n, st, K);
+        } else if (m == 1 && C.fuse) {
+            if (seq_i == 0) {
+                XfArgs<T, T> A = at(plan[0]); A.y = y; A.s = s; A.out = t1; A.k1 = kA;
+                xf_launch<T, T, K_P1>(A, plan[0], n, st, K);
+            }
+            const XfShape &Y = (seq_i % 2 == 0) ? plan[1] : plan[0], &Xw = (seq_i % 2 == 0) ? plan[0] : plan[1];
+            { XfArgs<T, T> A = at(Y); A.in = t1; A.out = t2; A.z = z; A.x2 = x2; A.k1 = kA; A.k2 = kQt;
+              xf_launch<T, T, K_P2>(A, Y, n, st, K); }
+            { XfArgs<T, T> A = at(Xw); A.in = t2; A.out = x; A.out2 = Ax; A.k1 = kQt; A.k2 = kQ; A.k3 = kAQ;
+              A.k4 = kAr;
+              xf_launch<T, T, K_P3>(A, Xw, n, st, K); }
+            { XfArgs<T, T> A = at(Y); A.in = x; A.in2 = Ax; A.out = x; A.s_io = s; A.y_io = y; A.k1 = kQ;
+              A.k3 = kAQ;
+              if (seq_i + 1 < seq_n) {
+                  A.out2 = t1; A.k4 = kA;
+                  xf_launch<T, T, K_P4A>(A, Y, n, st, K);
+              } else {
+                  xf_launch<T, T, K_P4>(A, Y, n, st, K);
+              }
+            }
         } else {
             { XfArgs<T, T> A = at(plan[0]); A.y = y; A.s = s; A.out = t1; A.k1 = kA;
               xf_launch<T, T, K_P1>(A, plan[0], n, st, K); }
@@ -698,10 +723,16 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
     prof_end(st);
 }
 
+// `count` iterations as one sequence (see enqueue_iteration_ptrs) for every slot of I.
 template <class T>
-static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st) {
+static void enqueue_iterations_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n, cudaStream_t st, int count) {
+    for (int i = 0; i < count; ++i) enqueue_iteration_ptrs<T>(I, C, n, st, i, count);
+}
+
+template <class T>
+static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st, int seq_i = 0, int seq_n = 1) {
     if (n >= PT_M + 1) {
-        enqueue_iteration_ptrs<T>(iter_ptrs<T>(W), C, n, st);
+        enqueue_iteration_ptrs<T>(iter_ptrs<T>(W), C, n, st, seq_i, seq_n);
         return;
     }
     // small lattices: separate butterflies and the thread-per-menu prox
@@ -716,6 +747,11 @@ static void enqueue_iteration(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t
     P.obsbits = W.obsbits.template as<uint32_t>();
     P.alpha = (T)C.alpha; P.b1 = (T)C.b1; P.b2 = (T)C.b2; P.ib1 = (T)C.ib1; P.ib2 = (T)C.ib2;
     launch_prox_n<T, PROX_ITER>(P, st);
+}
+
+template <class T>
+static void enqueue_iterations(BmWork<T> &W, const BmCoef &C, int n, cudaStream_t st, int count) {
+    for (int i = 0; i < count; ++i) enqueue_iteration<T>(W, C, n, st, i, count);
 }
 
 template <class T>
@@ -737,13 +773,20 @@ static void enqueue_cold_start(BmWork<T> &W, const BmCoef &C, int n, cudaStream_
 // The iteration's autotuner: times a few iterations of each candidate on the workspace and keeps
 // the fastest, one knob at a time -- the transform passes' low-window size (10, 11 or 12 bits;
 // it sets the high-window split), then the prox kernel's form (the shared-memory tile, or 2, 4 or
-// 8 lanes per menu). Cached per context, n and dtype; the state is reset by the caller. The
-// environment variable RUMB_PROX_FORM (0 tile, 1..3 lanes 2/4/8) pins the prox form.
-static int forced_prox_form() {
-    const char *e = getenv("RUMB_PROX_FORM");
+// 8 lanes per menu), then with two windows the fused three-pass sequence against four passes.
+// Cached per context, n and dtype; the state is reset by the caller. The environment variables
+// RUMB_PROX_FORM (0 tile, 1..3 lanes 2/4/8) and RUMB_FUSE (0 / 1) pin those knobs.
+static int forced_knob(const char *name, int count) {
+    const char *e = getenv(name);
     if (!e || !*e) return -1;
     int v = atoi(e);
-    return (v >= 0 && v < PROX_FORMS) ? v : -1;
+    return (v >= 0 && v < count) ? v : -1;
+}
+static void apply_forced(BmCoef &C) {
+    int f = forced_knob("RUMB_PROX_FORM", PROX_FORMS);
+    if (f >= 0) C.prox_form = f;
+    f = forced_knob("RUMB_FUSE", 2);
+    if (f >= 0) C.fuse = f;
 }
 
 template <class T>
@@ -756,18 +799,19 @@ static void tune_iteration(Ctx &c, BmWork<T> &W, BmCoef &C, int n, cudaStream_t 
         RUMB_CUDA(cudaEventCreate(&a));
         RUMB_CUDA(cudaEventCreate(&b));
         auto time_it = [&]() -> float {
-            for (int i = 0; i < 2; ++i) enqueue_iteration<T>(W, K, n, st);
+            enqueue_iterations<T>(W, K, n, st, 2);
             RUMB_CUDA(cudaEventRecord(a, st));
-            for (int i = 0; i < 6; ++i) enqueue_iteration<T>(W, K, n, st);
+            enqueue_iterations<T>(W, K, n, st, 6);
             RUMB_CUDA(cudaEventRecord(b, st));
             RUMB_CUDA(cudaEventSynchronize(b));
             float ms = 0.f;
             RUMB_CUDA(cudaEventElapsedTime(&ms, a, b));
             return ms;
         };
-        int best_lo = 12, best_form = n <= PROX_LANES_MAX_N ? PROX_LANES4 : PROX_TILE;
+        int best_lo = 12, best_form = n <= PROX_LANES_MAX_N ? PROX_LANES4 : PROX_TILE, best_fuse = 1;
         if (n >= PT_M + 1) {
             K.prox_form = best_form;
+            K.fuse = best_fuse;
             if (n - 1 > 10) {
                 float best_ms = 1e30f;
                 for (int lb : {10, 11, 12}) {
@@ -786,15 +830,24 @@ static void tune_iteration(Ctx &c, BmWork<T> &W, BmCoef &C, int n, cudaStream_t 
                     if (ms < best_ms) { best_ms = ms; best_form = f; }
                 }
             }
+            K.prox_form = best_form;
+            if (xf_plan(n - 1, best_lo).size() == 2) {
+                float best_ms = 1e30f;
+                for (int f = 0; f < 2; ++f) {
+                    K.fuse = f;
+                    float ms = time_it();
+                    if (ms < best_ms) { best_ms = ms; best_fuse = f; }
+                }
+            }
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
-        it = c.tuned.emplace(key, std::make_pair(best_lo, best_form)).first;
+        it = c.tuned.emplace(key, std::array<int, 3>{best_lo, best_form, best_fuse}).first;
     }
-    C.lo_bits = it->second.first;
-    C.prox_form = it->second.second;
-    int f = forced_prox_form();
-    if (f >= 0) C.prox_form = f;
+    C.lo_bits = it->second[0];
+    C.prox_form = it->second[1];
+    C.fuse = it->second[2];
+    apply_forced(C);
 }
 
 // The tuned schedule of (n, dtype) when it is known, else the defaults.
@@ -802,11 +855,11 @@ template <class T>
 static void tuned_or_default(Ctx &c, BmCoef &C, int n) {
     auto it = c.tuned.find(std::make_pair(n, (int)sizeof(T)));
     if (it != c.tuned.end()) {
-        C.lo_bits = it->second.first;
-        C.prox_form = it->second.second;
+        C.lo_bits = it->second[0];
+        C.prox_form = it->second[1];
+        C.fuse = it->second[2];
     }
-    int f = forced_prox_form();
-    if (f >= 0) C.prox_form = f;
+    apply_forced(C);
 }
 
 // ----------------------------------------------------------------- problem upload
@@ -1101,7 +1154,7 @@ static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const r
     Graph g_iter, g_ub, g_ublb;
     bool graphs = par.use_graph != 0;
     if (graphs) {
-        g_iter.capture(st, [&] { for (int i = 0; i < chunk; ++i) enqueue_iteration<T>(W, C, n, st); });
+        g_iter.capture(st, [&] { enqueue_iterations<T>(W, C, n, st, chunk); });
         g_ub.capture(st, [&] {
             enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), false, st);
             enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
@@ -1118,7 +1171,7 @@ static bool run_leg(Ctx &c, CertWork &CW, BmWork<T> &W, const BmCoef &C, const r
         if (graphs) {
             for (int i = 0; i < par.check / chunk; ++i) g_iter.launch(st);
         } else {
-            for (int i = 0; i < par.check; ++i) enqueue_iteration<T>(W, C, n, st);
+            enqueue_iterations<T>(W, C, n, st, par.check);
         }
         L.it += par.check;
         if (sizeof(T) == 4) L.it32 += par.check;
@@ -1330,7 +1383,7 @@ int bm_iterate(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, voi
             RUMB_CUDA(cudaMemcpyAsync(W.y.ptr, y, sb, cudaMemcpyHostToDevice, st));
             RUMB_CUDA(cudaMemcpyAsync(W.z.ptr, z, sb, cudaMemcpyHostToDevice, st));
         }
-        for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
+        enqueue_iterations<T>(W, C, n, st, iters);
         RUMB_CUDA(cudaMemcpyAsync(x2, W.x2.ptr, sb, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaMemcpyAsync(s, W.s.ptr, sb, cudaMemcpyDeviceToHost, st));
         RUMB_CUDA(cudaMemcpyAsync(y, W.y.ptr, sb, cudaMemcpyDeviceToHost, st));
@@ -1377,7 +1430,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
         enqueue_cold_start<T>(W, C, n, st);
         tune_iteration<T>(c, W, C, n, st);
         enqueue_cold_start<T>(W, C, n, st);
-        for (int i = 0; i < std::max(warmup, 3); ++i) enqueue_iteration<T>(W, C, n, st);      // warm-up
+        enqueue_iterations<T>(W, C, n, st, std::max(warmup, 3));      // warm-up
         RUMB_CUDA(cudaStreamSynchronize(st));
         // one check first, so that its cached tables exist before the capture (no allocation inside)
         if (par->lb_every > 0) {
@@ -1386,7 +1439,7 @@ int bm_profile(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_params *par, int
             RUMB_CUDA(cudaStreamSynchronize(st));
         }
         auto body = [&] {
-            for (int i = 0; i < iters; ++i) enqueue_iteration<T>(W, C, n, st);
+            enqueue_iterations<T>(W, C, n, st, iters);
             if (par->lb_every > 0) {
                 enqueue_stats_lb<T>(c, CW, n, W.x2.template as<T>(), true, st);
                 enqueue_push<T>(c, CW, n, W.x2.template as<T>(), st);
@@ -1656,7 +1709,7 @@ static int bm_solve_batch_t(Ctx &c, const rumb_bm_problem *pr, const rumb_bm_par
     auto t_setup = Clock::now();
     const int chunk = graph_chunk(par->check);
     Graph g_iter;
-    g_iter.capture(st, [&] { for (int i = 0; i < chunk; ++i) enqueue_iteration_ptrs<T>(I, C, n, st); });
+    g_iter.capture(st, [&] { enqueue_iterations_ptrs<T>(I, C, n, st, chunk); });
     std::vector<double> res((size_t)K * R_SLOTS);
     cudaEvent_t e0, e1;
     RUMB_CUDA(cudaEventCreate(&e0));

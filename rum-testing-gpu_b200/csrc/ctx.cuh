@@ -1,6 +1,7 @@
 // The library context: one device, one stream, cached lattice tables and workspaces.
 #pragma once
 #include <atomic>
+#include <array>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -28,8 +29,9 @@ struct Ctx {
     std::unique_ptr<BmWorkBase> batch64, batch32;  // batched-draw workspaces
     std::unique_ptr<BmWorkBase> cert;           // float64 certificate workspace
     std::unique_ptr<BmWorkBase> scratch;        // primitive calls' scratch
-    // the iteration's tuned schedule per (n, state bytes): transform low-window size, prox form
-    std::map<std::pair<int, int>, std::pair<int, int>> tuned;
+    // the iteration's tuned schedule per (n, state bytes): transform low-window size, prox form,
+    // fused passes (0 / 1)
+    std::map<std::pair<int, int>, std::array<int, 3>> tuned;
     // overlapped checks: a second stream, its two events and pinned result words (made on first use)
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_snap = nullptr, ev_done = nullptr;

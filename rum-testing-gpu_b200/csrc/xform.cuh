@@ -24,6 +24,11 @@
 //                      a = -alpha Ax - (1-alpha) s; s' = max(y/b1 - a, 0); y -= b1 (a + s')
 //   K_FULL (all bits, n <= 13) P1..P4 in one pass
 //   K_DUAL (middle high bits, n >= 21) Q and (A Q) forward on two streams, in place
+//   K_P4A  K_P4, then the next iteration's w = y - b1 s and its A' on the same window -> T1
+// With two windows an iteration sequence alternates the windows: iteration i runs P2 on window Y,
+// P3 on the other window and P4A on Y, where Y is the high window for even i and the low window
+// for odd i; the sequence starts with P1 on the low window and ends with a plain P4, so an
+// iteration costs three passes instead of four (every pass is written window-agnostic).
 // The tensor factors of a transform act on different bits and commute, so applying a
 // transform's high bits before its low bits (P2 / P3) changes only the rounding.
 #pragma once
@@ -143,7 +148,7 @@ __device__ __forceinline__ void xf_backward(T (&v)[1 << RB], T *sm, int w, int l
     if (L) xf_lanes<T, 1 << RB, AP>(v, lane, k);
 }
 
-enum XfKind { K_PLAIN = 0, K_P1 = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_FULL = 5, K_DUAL = 6 };
+enum XfKind { K_PLAIN = 0, K_P1 = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_FULL = 5, K_DUAL = 6, K_P4A = 7 };
 
 template <class T, class TI>
 struct XfArgs {
@@ -181,7 +186,7 @@ __device__ __forceinline__ ll xf_index(int s0, int B, ll Nloc, ll tile, int row,
 // Streams a kind reads for each tile (staged ahead; stream 0 has element type TI).
 template <int KIND>
 struct XfStreams {
-    static constexpr int n = (KIND == K_P4 || KIND == K_FULL) ? 4 : (KIND == K_P2) ? 3
+    static constexpr int n = (KIND == K_P4 || KIND == K_P4A || KIND == K_FULL) ? 4 : (KIND == K_P2) ? 3
                              : (KIND == K_P1 || KIND == K_DUAL) ? 2 : 1;
 };
 
@@ -224,13 +229,13 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
             } else {
                 xf_cp_async(st_in + spos(ra), A.in + ga);
             }
-            if (KIND == K_P4 || KIND == K_DUAL) xf_cp_async(st_x + spos(ra), A.in2 + ga);
+            if (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) xf_cp_async(st_x + spos(ra), A.in2 + ga);
             if (KIND == K_P2 || KIND == K_FULL) {
                 const ll gb = gidx(tile, rb);
                 xf_cp_async(st_x + (KIND == K_FULL ? 1 : 0) * TILE + spos(rb), A.z + gb);
                 xf_cp_async(st_x + (KIND == K_FULL ? 2 : 1) * TILE + spos(rb), A.x2 + gb);
             }
-            if (KIND == K_P4) {
+            if (KIND == K_P4 || KIND == K_P4A) {
                 const ll gb = gidx(tile, rb);
                 xf_cp_async(st_x + TILE + spos(rb), A.s_io + gb);
                 xf_cp_async(st_x + 2 * TILE + spos(rb), A.y_io + gb);
@@ -248,11 +253,11 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
             const int ra = row_A<RB, WB>(w, j), rb = rowB(j);
             if (KIND == K_P1 || KIND == K_FULL) v[j] = reinterpret_cast<T *>(st_in)[spos(ra)] - A.b1 * st_x[spos(ra)];
             else v[j] = (T)st_in[spos(ra)];
-            if (KIND == K_P4 || KIND == K_DUAL) u[j] = st_x[spos(ra)];
+            if (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) u[j] = st_x[spos(ra)];
             if (KIND == K_P2 || KIND == K_FULL)        // z + b2 x2, kept as one value
                 zz[j] = st_x[(KIND == K_FULL ? 1 : 0) * TILE + spos(rb)] +
                         A.b2 * st_x[(KIND == K_FULL ? 2 : 1) * TILE + spos(rb)];
-            if (KIND == K_P4) {
+            if (KIND == K_P4 || KIND == K_P4A) {
                 ss[j] = st_x[TILE + spos(rb)];
                 yy[j] = st_x[2 * TILE + spos(rb)];
             }
@@ -260,7 +265,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
         // every thread has read its staged values: the stage can take the next tile
         __syncthreads();
         if (tile + gridDim.x < tiles) prefetch(tile + gridDim.x);
-        if constexpr (KIND == K_P4 || KIND == K_DUAL) {
+        if constexpr (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) {
             xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k1);
             xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k3);
 #pragma unroll
@@ -275,9 +280,17 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
                     T axor = -A.alpha * ax - (one - A.alpha) * sv;
                     T sn = A.ib1 * yv - axor;
                     sn = sn > (T)0 ? sn : (T)0;
-                    A.y_io[g] = yv - A.b1 * (axor + sn);
+                    const T yn = yv - A.b1 * (axor + sn);
+                    A.y_io[g] = yn;
                     A.s_io[g] = sn;
+                    ss[j] = yn - A.b1 * sn;                  // K_P4A: the next iteration's w
                 }
+            }
+            if constexpr (KIND == K_P4A) {
+                // the next iteration's A' on this window, from layout B back to layout A
+                xf_backward<T, L, RB, WB, XF_APRIME>(ss, sm, w, lane, A.k4);
+#pragma unroll
+                for (int j = 0; j < R; ++j) A.out2[gidx(tile, row_A<RB, WB>(w, j))] = ss[j];
             }
             continue;
         }
@@ -411,9 +424,10 @@ inline void xf_launch_one(const XfArgs<T, TI> &A0, int n, cudaStream_t st, int s
             case K_P3: bytes += 2 * S * e; break;
             case K_DUAL: bytes += 3 * S * e; break;
             case K_P4: bytes += 6 * S * e; break;
+            case K_P4A: bytes += 7 * S * e; break;
             case K_FULL: bytes += 7 * S * e; break;
         }
-        const char *kn[] = {"plain", "P1", "P2", "P3", "P4", "full", "dual"};
+        const char *kn[] = {"plain", "P1", "P2", "P3", "P4", "full", "dual", "P4A"};
         char nm[64];
         snprintf(nm, sizeof nm, "xform<%s,%s>[s=%d,B=%d]", sizeof(T) == 8 ? "f64" : "f32", kn[KIND], A.s0, A.B);
         prof_begin(nm, bytes, st);

@@ -157,6 +157,29 @@ def test_prox_forms_track_oracle(ctx, monkeypatch, case, form, dtype):
         assert d <= tol * max(1.0, float(np.max(np.abs(ref)))), (name, d)
 
 
+@pytest.mark.parametrize("fuse", [0, 1])
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_fused_and_unfused_sequences_track_oracle(ctx, monkeypatch, fuse, dtype):
+    """With two transform windows (n = 16) an iteration sequence runs three passes per iteration
+    (RUMB_FUSE=1: P4 carries the next iteration's A', windows alternating) or four (RUMB_FUSE=0);
+    both keep the iterates on the oracle's over sequences of odd and even length."""
+    monkeypatch.setenv("RUMB_FUSE", str(fuse))
+    n, menu, alt, p = _instance("n16_mix")
+    beta = O.beta_default(p.size)
+    dt = np.float64 if dtype == "float64" else np.float32
+    bm = O.BMOracle(n, menu, alt, p, dtype=dt)
+    prob = ctx.bm_problem(n, menu, alt, p)
+    par = ctx.bm_params(beta, dtype=dtype)
+    st = ctx.bm_iterate(prob, par, None, 7, cold_start=True)
+    st = ctx.bm_iterate(prob, par, st, 4)
+    bm.iterate(11)
+    tol = 1e-10 if dt == np.float64 else 1e-3
+    for name in ("x2", "s", "y", "z"):
+        ref = getattr(bm, name).astype(np.float64)
+        d = np.max(np.abs(st[name].astype(np.float64) - ref))
+        assert d <= tol * max(1.0, float(np.max(np.abs(ref)))), (name, d)
+
+
 def test_certified_solve_matches_oracle(ctx):
     n, menu, alt, p = config_instance("n10_all_k20")
     beta = O.beta_default(p.size)
