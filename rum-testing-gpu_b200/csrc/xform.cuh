@@ -11,8 +11,8 @@
 // A "forward" phase runs lane stages, the layout-A register stages, one shared-memory transpose
 // and the layout-B register stages (ending in layout B); a "backward" phase runs them in the
 // opposite order (ending in layout A). Loads and stores are coalesced rows of 32 lanes in either
-// layout. A pass is persistent (a few CTAs per SM loop over the tiles) and stages the next tile's
-// inputs in shared memory with cp.async while the current tile is transformed and stored.
+// layout, and every load of a pass is issued before the first stage, so each warp keeps 2^RB
+// (times the number of input streams) loads in flight.
 //
 // The four iteration passes fuse the elementwise ADMM steps of the reference's one_iter
 // (solver/bm_admm/solver.py:240-254) into the transforms:
@@ -162,7 +162,6 @@ struct XfArgs {
     Co<T> k1, k2, k3, k4;  // phase coefficients: see each kind (K_FULL: A', Q^T, Q, A Q)
     T b1, b2, ib1, alpha;
     ll Nloc;
-    int nalt;           // alternatives (blocks per slab)
     int s0, B;          // window
     ll bstride;         // batched draws: elements between consecutive draws' slabs (grid.y = draw slot)
     const int *active;  // batched draws: slot flags (nullptr: every slot runs)
@@ -183,177 +182,153 @@ __device__ __forceinline__ ll xf_index(int s0, int B, ll Nloc, ll tile, int row,
     return x * Nloc + (hi << (s0 + B)) + ((ll)row << s0) + (lowblk << 5) + lane;
 }
 
-// Streams a kind reads for each tile (staged ahead; stream 0 has element type TI).
-template <int KIND>
-struct XfStreams {
-    static constexpr int n = (KIND == K_P4 || KIND == K_P4A || KIND == K_FULL) ? 4 : (KIND == K_P2) ? 3
-                             : (KIND == K_P1 || KIND == K_DUAL) ? 2 : 1;
-};
-
-template <class E>
-__device__ __forceinline__ void xf_cp_async(E *dst, const E *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-                 "l"(src), "n"((int)sizeof(E))
-                 : "memory");
-}
-
-// A persistent pass: CTA b of a slot takes tiles b, b + gridDim.x, ... While a tile is computed
-// and stored, the next tile's inputs are already on their way into a shared-memory stage
-// (cp.async, each thread fetching exactly the elements it will read), so the loads of one tile
-// overlap the arithmetic and stores of the previous one.
 template <class T, class TI, int L, int RB, int WB, int KIND>
 __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
     extern __shared__ __align__(16) unsigned char xf_smem[];
+    T *sm = reinterpret_cast<T *>(xf_smem);
     constexpr int R = 1 << RB;
-    constexpr int TILE = 1 << (RB + WB + 5);
-    T *sm = reinterpret_cast<T *>(xf_smem);                                  // layout transposes
-    TI *st_in = reinterpret_cast<TI *>(xf_smem + (size_t)TILE * sizeof(T));  // stream 0 (TI)
-    T *st_x = reinterpret_cast<T *>(xf_smem + (size_t)TILE * (sizeof(T) + sizeof(TI)));  // streams 1..
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const ll tile = blockIdx.x;
     const int s0 = A.s0, B = A.B;
     const ll Nloc = A.Nloc;
     if (A.active && !A.active[blockIdx.y]) return;          // a retired slot (uniform per CTA)
     const ll boff = (ll)blockIdx.y * A.bstride;
-    const ll tiles = (Nloc >> (L ? B : B + 5)) * (ll)A.nalt;
-    auto gidx = [&](ll tile, int row) -> ll { return boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane); };
-    auto rowB = [&](int j) -> int { return WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j); };
-    auto spos = [&](int row) -> int { return (row << 5) + lane; };
-    auto prefetch = [&](ll tile) {
+    T v[R];
+    if constexpr (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) {
+        constexpr bool SY = KIND == K_P4 || KIND == K_P4A;
+        T u[R], ss[SY ? R : 1], yy[SY ? R : 1];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            const int ra = row_A<RB, WB>(w, j), rb = rowB(j);
-            const ll ga = gidx(tile, ra);
-            if (KIND == K_P1 || KIND == K_FULL) {
-                xf_cp_async(reinterpret_cast<T *>(st_in) + spos(ra), A.y + ga);
-                xf_cp_async(st_x + spos(ra), A.s + ga);
-            } else {
-                xf_cp_async(st_in + spos(ra), A.in + ga);
-            }
-            if (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) xf_cp_async(st_x + spos(ra), A.in2 + ga);
-            if (KIND == K_P2 || KIND == K_FULL) {
-                const ll gb = gidx(tile, rb);
-                xf_cp_async(st_x + (KIND == K_FULL ? 1 : 0) * TILE + spos(rb), A.z + gb);
-                xf_cp_async(st_x + (KIND == K_FULL ? 2 : 1) * TILE + spos(rb), A.x2 + gb);
-            }
-            if (KIND == K_P4 || KIND == K_P4A) {
-                const ll gb = gidx(tile, rb);
-                xf_cp_async(st_x + TILE + spos(rb), A.s_io + gb);
-                xf_cp_async(st_x + 2 * TILE + spos(rb), A.y_io + gb);
-            }
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+            v[j] = (T)A.in[g];
+            u[j] = A.in2[g];
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-    ll tile = blockIdx.x;
-    if (tile < tiles) prefetch(tile);
-    for (; tile < tiles; tile += gridDim.x) {
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        T v[R], u[R], zz[R], ss[R], yy[R];             // the kind's streams (unused ones vanish)
-#pragma unroll
-        for (int j = 0; j < R; ++j) {
-            const int ra = row_A<RB, WB>(w, j), rb = rowB(j);
-            if (KIND == K_P1 || KIND == K_FULL) v[j] = reinterpret_cast<T *>(st_in)[spos(ra)] - A.b1 * st_x[spos(ra)];
-            else v[j] = (T)st_in[spos(ra)];
-            if (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) u[j] = st_x[spos(ra)];
-            if (KIND == K_P2 || KIND == K_FULL)        // z + b2 x2, kept as one value
-                zz[j] = st_x[(KIND == K_FULL ? 1 : 0) * TILE + spos(rb)] +
-                        A.b2 * st_x[(KIND == K_FULL ? 2 : 1) * TILE + spos(rb)];
-            if (KIND == K_P4 || KIND == K_P4A) {
-                ss[j] = st_x[TILE + spos(rb)];
-                yy[j] = st_x[2 * TILE + spos(rb)];
-            }
-        }
-        // every thread has read its staged values: the stage can take the next tile
-        __syncthreads();
-        if (tile + gridDim.x < tiles) prefetch(tile + gridDim.x);
-        if constexpr (KIND == K_P4 || KIND == K_P4A || KIND == K_DUAL) {
-            xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k1);
-            xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k3);
+        if constexpr (SY) {
 #pragma unroll
             for (int j = 0; j < R; ++j) {
-                const ll g = gidx(tile, rowB(j));
-                A.out[g] = v[j];
-                if (KIND == K_DUAL) {
-                    A.out2[g] = u[j];
-                } else {
-                    T ax = u[j], sv = ss[j], yv = yy[j];
-                    T one = (T)1;
-                    T axor = -A.alpha * ax - (one - A.alpha) * sv;
-                    T sn = A.ib1 * yv - axor;
-                    sn = sn > (T)0 ? sn : (T)0;
-                    const T yn = yv - A.b1 * (axor + sn);
-                    A.y_io[g] = yn;
-                    A.s_io[g] = sn;
-                    ss[j] = yn - A.b1 * sn;                  // K_P4A: the next iteration's w
-                }
+                int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+                ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+                ss[j] = A.s_io[g];
+                yy[j] = A.y_io[g];
             }
-            if constexpr (KIND == K_P4A) {
-                // the next iteration's A' on this window, from layout B back to layout A
-                xf_backward<T, L, RB, WB, XF_APRIME>(ss, sm, w, lane, A.k4);
+        }
+        xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k1);
+        xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k3);
 #pragma unroll
-                for (int j = 0; j < R; ++j) A.out2[gidx(tile, row_A<RB, WB>(w, j))] = ss[j];
+        for (int j = 0; j < R; ++j) {
+            int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+            A.out[g] = v[j];
+            if constexpr (!SY) {
+                A.out2[g] = u[j];
+            } else {
+                T ax = u[j], sv = ss[j], yv = yy[j];
+                T one = (T)1;
+                T axor = -A.alpha * ax - (one - A.alpha) * sv;
+                T sn = A.ib1 * yv - axor;
+                sn = sn > (T)0 ? sn : (T)0;
+                const T yn = yv - A.b1 * (axor + sn);
+                A.y_io[g] = yn;
+                A.s_io[g] = sn;
+                ss[j] = yn - A.b1 * sn;                  // K_P4A: the next iteration's w
             }
-            continue;
+        }
+        if constexpr (KIND == K_P4A) {
+            // the next iteration's A' on this window, from layout B back to layout A
+            xf_backward<T, L, RB, WB, XF_APRIME>(ss, sm, w, lane, A.k4);
+#pragma unroll
+            for (int j = 0; j < R; ++j)
+                A.out2[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane)] = ss[j];
+        }
+        return;
+    } else {
+        // single input stream; the layout-B side inputs (z, x2) are loaded up front as well
+        T zz[(KIND == K_P2 || KIND == K_FULL) ? R : 1], xx[(KIND == K_P2 || KIND == K_FULL) ? R : 1];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+            if (KIND == K_P1 || KIND == K_FULL) v[j] = A.y[g] - A.b1 * A.s[g];
+            else v[j] = (T)A.in[g];
+        }
+        if (KIND == K_P2 || KIND == K_FULL) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+                ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+                zz[j] = A.z[g];
+                xx[j] = A.x2[g];
+            }
         }
         if (KIND == K_P1 || KIND == K_P2 || KIND == K_FULL) xf_forward<T, L, RB, WB, XF_APRIME>(v, sm, w, lane, A.k1);
         else xf_forward<T, L, RB, WB, XF_GEN>(v, sm, w, lane, A.k1);
         // now in layout B (layout A when WB == 0)
         if constexpr (KIND == K_PLAIN || KIND == K_P1) {
 #pragma unroll
-            for (int j = 0; j < R; ++j) A.out[gidx(tile, rowB(j))] = v[j];
-            continue;
+            for (int j = 0; j < R; ++j) {
+                int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+                A.out[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane)] = v[j];
+            }
+            return;
         }
         if constexpr (KIND == K_P2 || KIND == K_FULL) {
 #pragma unroll
-            for (int j = 0; j < R; ++j) v[j] = (zz[j] - v[j]) * A.ib1;
+            for (int j = 0; j < R; ++j) v[j] = (zz[j] + A.b2 * xx[j] - v[j]) * A.ib1;
             xf_backward<T, L, RB, WB>(v, sm, w, lane, A.k2);
-            if constexpr (KIND == K_P2) {
+            if (KIND == K_P2) {
 #pragma unroll
-                for (int j = 0; j < R; ++j) A.out[gidx(tile, row_A<RB, WB>(w, j))] = v[j];
-                continue;
-            } else {
-                // K_FULL: diag, then Q and (A Q) forward, x and the s/y update (layout A -> B)
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    const ll g = gidx(tile, row_A<RB, WB>(w, j));
-                    v[j] = v[j] * A.diag[__popcll((ull)((g - boff) & (Nloc - 1)))];
-                    u[j] = v[j];
-                }
-                xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k3);
-                xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k4);
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    const ll g = gidx(tile, rowB(j));
-                    A.out[g] = v[j];
-                    T ax = u[j], sv = A.s_io[g], yv = A.y_io[g];
-                    T one = (T)1;
-                    T axor = -A.alpha * ax - (one - A.alpha) * sv;
-                    T sn = A.ib1 * yv - axor;
-                    sn = sn > (T)0 ? sn : (T)0;
-                    A.y_io[g] = yv - A.b1 * (axor + sn);
-                    A.s_io[g] = sn;
-                }
-                continue;
+                for (int j = 0; j < R; ++j)
+                    A.out[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane)] = v[j];
+                return;
             }
+            // K_FULL: diag, then Q and (A Q) forward, x and the s/y update (layout A -> B)
+            T u[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane);
+                v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
+                u[j] = v[j];
+            }
+            xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k3);
+            xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k4);
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+                ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+                A.out[g] = v[j];
+                T ax = u[j], sv = A.s_io[g], yv = A.y_io[g];
+                T one = (T)1;
+                T axor = -A.alpha * ax - (one - A.alpha) * sv;
+                T sn = A.ib1 * yv - axor;
+                sn = sn > (T)0 ? sn : (T)0;
+                A.y_io[g] = yv - A.b1 * (axor + sn);
+                A.s_io[g] = sn;
+            }
+            return;
         }
         if constexpr (KIND == K_P3) {
             // (A Q) on the low window is A applied after Q: the fork copies Q's result (layout A) and
             // runs the two-operation A form (k4 = (1, -1, 0, p)) forward from layout A to layout B
             // instead of a second general transform; the factors of A commute, so the stage order
             // does not matter
+            T u[R];
 #pragma unroll
             for (int j = 0; j < R; ++j) {
-                const ll g = gidx(tile, rowB(j));
-                v[j] = v[j] * A.diag[__popcll((ull)((g - boff) & (Nloc - 1)))];
+                int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+                ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
+                v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
             }
             xf_backward<T, L, RB, WB>(v, sm, w, lane, A.k2);
 #pragma unroll
             for (int j = 0; j < R; ++j) {
                 u[j] = v[j];
-                A.out[gidx(tile, row_A<RB, WB>(w, j))] = v[j];
+                A.out[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row_A<RB, WB>(w, j), lane)] = v[j];
             }
             xf_forward<T, L, RB, WB, XF_A>(u, sm, w, lane, A.k4);
 #pragma unroll
-            for (int j = 0; j < R; ++j) A.out2[gidx(tile, rowB(j))] = u[j];
+            for (int j = 0; j < R; ++j) {
+                int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
+                A.out2[boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane)] = u[j];
+            }
         }
     }
 }
@@ -387,33 +362,12 @@ inline std::vector<XfShape> xf_plan(int nb, int lo_bits = 12) {
     return plan;
 }
 
-// Dynamic shared memory of a pass: the transpose buffer and the stages of its streams.
-template <class T, class TI, int RB, int WB, int KIND>
-constexpr size_t xf_smem_bytes() {
-    return ((size_t)1 << (RB + WB + 5)) * (sizeof(T) + sizeof(TI) + (XfStreams<KIND>::n - 1) * sizeof(T));
-}
-
 template <class T, class TI, int L, int RB, int WB, int KIND>
-inline void xf_launch_one(const XfArgs<T, TI> &A0, int n, cudaStream_t st, int slots = 1) {
+inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st, int slots = 1) {
     static std::atomic<unsigned long long> optin{0};
-    static std::atomic<int> resident[64];               // CTAs per SM, per device (0: not known)
-    constexpr size_t smem = xf_smem_bytes<T, TI, RB, WB, KIND>();
-    auto kern = xform_pass<T, TI, L, RB, WB, KIND>;
-    smem_optin(kern, (int)smem, optin);
-    XfArgs<T, TI> A = A0;
-    A.nalt = n;
-    int dev = 0;
-    RUMB_CUDA(cudaGetDevice(&dev));
-    int occ = resident[dev & 63].load(std::memory_order_relaxed);
-    if (occ <= 0) {
-        RUMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 << WB, smem));
-        if (occ < 1) occ = 1;
-        resident[dev & 63].store(occ, std::memory_order_relaxed);
-    }
-    const ll tiles = (A.Nloc >> (L ? A.B : A.B + 5)) * n;
-    ll grid = ((ll)occ * num_sms(dev) + slots - 1) / slots;    // persistent CTAs per slot
-    if (grid > tiles) grid = tiles;
-    if (grid < 1) grid = 1;
+    size_t smem = (size_t)sizeof(T) << (RB + WB + 5);
+    smem_optin(xform_pass<T, TI, L, RB, WB, KIND>, (int)smem, optin);
+    ll tiles = (A.Nloc >> (L ? A.B : A.B + 5)) * n;
     if (g_prof) {
         double S = (double)A.Nloc * n * slots, e = sizeof(T), ei = sizeof(TI);
         double bytes = S * e;                                          // one output
@@ -432,7 +386,7 @@ inline void xf_launch_one(const XfArgs<T, TI> &A0, int n, cudaStream_t st, int s
         snprintf(nm, sizeof nm, "xform<%s,%s>[s=%d,B=%d]", sizeof(T) == 8 ? "f64" : "f32", kn[KIND], A.s0, A.B);
         prof_begin(nm, bytes, st);
     }
-    kern<<<dim3((unsigned)grid, (unsigned)slots), 32 << WB, smem, st>>>(A);
+    xform_pass<T, TI, L, RB, WB, KIND><<<dim3((unsigned)tiles, (unsigned)slots), 32 << WB, smem, st>>>(A);
     RUMB_LAUNCH("xform_pass");
     prof_end(st);
 }
