@@ -3,7 +3,8 @@
     python tests/golden/make_cg_golden.py          # on a GPU host, after build()
 
 The library's CG loop runs n18_d05pct_k50 (n = 18, 0.5 % menus, K = 50, N = 500) to abs 1e-5 in
-uint24 and uint16 storage; at every iteration the residual it priced is priced again by the
+uint24 storage and for 1,000 columns in uint16 storage (whose quantization margin keeps its bound
+above abs 1e-5 at this density); at every iteration the residual it priced is priced again by the
 reference's own stream kernels (baseline/ref_replay.py, NVRTC-compiled from the reference's
 source) and the run is kept only if every ranking is the reference kernels' ranking. The file
 holds the rankings (rank positions, one row per CG iteration) and the final bracket per storage;
@@ -33,7 +34,7 @@ def main():
     out = {}
     for mode in ("u24", "u16"):
         res, bad = T._config3_run(ctx, mode, check_reference=True)
-        if bad or res["stop_reason"] != "gap_abs":
+        if bad or res["stop_reason"] != ("gap_abs" if mode == "u24" else "max_iters"):
             raise SystemExit("%s: not recorded (%s, %d mismatches: %s)" % (mode, res["stop_reason"], len(bad), bad[:3]))
         out["picked_" + mode] = np.array(res["picked"], dtype=np.int32)
         out["bracket_" + mode] = np.array([res["lb"], res["distance"]])
