@@ -134,7 +134,7 @@ def test_iterates_track_oracle(ctx, case, dtype):
             assert d <= tol[total] * max(1.0, float(np.max(np.abs(getattr(bm, name))))), (name, total, d)
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("case", ["n10_all_k20", "n16_mix"])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
 def test_prox_forms_track_oracle(ctx, monkeypatch, case, form, dtype):
