@@ -559,7 +559,10 @@ static Eigen eigen2(double p) {
 struct BmCoef {
     double b1, b2, ib1, ib2, alpha, p;
     double Qt[4], Q[4], AQ[4];
-    std::vector<double> diag;   // by popcount, nb + 1 entries
+    // the register-tiled passes (n >= 8): Q and Q^T as q00 (1, t, t, -1) applied in unit form and
+    // A Q divided by q00; the scales q00^(n-1) of Q and of Q^T move into the diagonal
+    double Qu[4], AQu[4];
+    std::vector<double> diag;   // by popcount: entries 0..nb as is, 32..32+nb times q00^(2 nb)
     int lo_bits = 12;           // transform window split (tuned)
     int prox_form = PROX_TILE;  // prox kernel form (tuned)
     int fuse = 1;               // two windows: P4 carries the next A' (three passes an iteration; tuned)
@@ -576,12 +579,21 @@ static BmCoef make_coef(int n, double beta, double alpha, double p) {
     C.Q[0] = E.Q[0][0]; C.Q[1] = E.Q[0][1]; C.Q[2] = E.Q[1][0]; C.Q[3] = E.Q[1][1];
     // A Q with A = [[1, -1], [0, p]] (the raw A butterfly, solver/bm_admm/solver.py:247)
     C.AQ[0] = C.Q[0] - C.Q[2]; C.AQ[1] = C.Q[1] - C.Q[3]; C.AQ[2] = p * C.Q[2]; C.AQ[3] = p * C.Q[3];
+    // Q is a reflection (det < 0): [[q00, q01], [q01, -q00]], symmetric, so Q^T = Q
+    for (int i = 0; i < 4; ++i) {
+        C.Qu[i] = C.Q[i] / C.Q[0];
+        C.AQu[i] = C.AQ[i] / C.Q[0];
+    }
+    C.Qu[3] = -1.0;
     int nb = n - 1;
     double gamma = 1.0;                                  // beta2 / beta1
+    C.diag.assign(64, 0.0);
+    const double scale = std::pow(C.Q[0], 2.0 * nb);
     for (int pc = 0; pc <= nb; ++pc) {
         double lam = 1.0;
         for (int bit = 0; bit < nb; ++bit) lam *= (bit < pc) ? E.ev[1] : E.ev[0];
-        C.diag.push_back(1.0 / (gamma + lam));
+        C.diag[pc] = 1.0 / (gamma + lam);
+        C.diag[32 + pc] = C.diag[pc] * scale;
     }
     return C;
 }
@@ -640,15 +652,15 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
     {
         T p = (T)C.p;
         Co<T> kA{(T)1, (T)0, (T)-1, p};                                    // A' (sign folded)
-        Co<T> kQt{(T)C.Qt[0], (T)C.Qt[1], (T)C.Qt[2], (T)C.Qt[3]};
-        Co<T> kQ{(T)C.Q[0], (T)C.Q[1], (T)C.Q[2], (T)C.Q[3]};
-        Co<T> kAQ{(T)C.AQ[0], (T)C.AQ[1], (T)C.AQ[2], (T)C.AQ[3]};      // A Q, A = [[1,-1],[0,p]]
+        Co<T> kQt{(T)C.Qu[0], (T)C.Qu[1], (T)C.Qu[2], (T)C.Qu[3]};      // Q^T = Q, unit form
+        Co<T> kQ = kQt;
+        Co<T> kAQ{(T)C.AQu[0], (T)C.AQu[1], (T)C.AQu[2], (T)C.AQu[3]};  // A Q / q00, A = [[1,-1],[0,p]]
         Co<T> kAr{(T)1, (T)-1, (T)0, p};                                   // A itself
         std::vector<XfShape> plan = xf_plan(n - 1, C.lo_bits);
         XfArgs<T, T> base{};
         base.Nloc = 1LL << (n - 1);
         base.b1 = (T)C.b1; base.b2 = (T)C.b2; base.ib1 = (T)C.ib1; base.alpha = (T)C.alpha;
-        base.diag = I.diag;
+        base.diag = I.diag + 32;                                           // with the folded scales
         base.bstride = I.bstride;
         base.active = I.active;
         auto at = [&](const XfShape &sh) { XfArgs<T, T> A = base; A.s0 = sh.s0; A.B = sh.B; return A; };

@@ -42,8 +42,11 @@ struct Co {
 };
 
 // Pair forms (MODE): 0 general (a, b, c, d); 1 A' = (1, 0, -1, p): lo' = lo, hi' = p hi - lo
-// (one operation per pair); 2 A = (1, -1, 0, p): lo' = lo - hi, hi' = p hi (two operations)
-constexpr int XF_GEN = 0, XF_APRIME = 1, XF_A = 2;
+// (one operation per pair); 2 A = (1, -1, 0, p): lo' = lo - hi, hi' = p hi (two operations);
+// 3 a reflection scaled to unit diagonal, (1, b, c, -1): lo' = lo + b hi, hi' = c lo - hi (two
+// fused multiply-adds per pair; the eigenvector matrix Q = q00 (1, t, t, -1) is applied this way and
+// its scale q00 per stage is folded into the eigen-space diagonal)
+constexpr int XF_GEN = 0, XF_APRIME = 1, XF_A = 2, XF_UNIT = 3;
 
 template <class T, int MODE>
 __device__ __forceinline__ void xf_pair(T &X, T &Y, const Co<T> &k) {
@@ -54,6 +57,13 @@ __device__ __forceinline__ void xf_pair(T &X, T &Y, const Co<T> &k) {
     if (MODE == XF_A) {
         X = X - Y;
         Y = k.d * Y;
+        return;
+    }
+    if (MODE == XF_UNIT) {
+        T lo = X + k.b * Y;
+        T hi = k.c * X - Y;
+        X = lo;
+        Y = hi;
         return;
     }
     T lo = k.a * X + k.b * Y;
@@ -86,6 +96,8 @@ __device__ __forceinline__ void xf_lanes(T (&v)[R], int lane, const Co<T> &k) {
             T o = __shfl_xor_sync(0xffffffffu, v[i], 1 << j);
             if (AP == XF_APRIME) {
                 if (hi) v[i] = k.d * v[i] - o;
+            } else if (AP == XF_UNIT) {
+                v[i] = c1 * o + (hi ? -v[i] : v[i]);
             } else if (AP == XF_A) {
                 v[i] = hi ? k.d * v[i] : v[i] - o;
             } else {
@@ -182,8 +194,15 @@ __device__ __forceinline__ ll xf_index(int s0, int B, ll Nloc, ll tile, int row,
     return x * Nloc + (hi << (s0 + B)) + ((ll)row << s0) + (lowblk << 5) + lane;
 }
 
+// CTAs kept resident per SM: the four-stream kinds with 8 values a thread and 256 threads are held
+// to 128 registers so that two CTAs fit an SM
+template <int RB, int WB, int KIND>
+constexpr int xf_min_blocks() {
+    return ((KIND == K_P4 || KIND == K_P4A) && RB <= 3 && WB == 3) ? 2 : 1;
+}
+
 template <class T, class TI, int L, int RB, int WB, int KIND>
-__global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
+__global__ void __launch_bounds__(32 << WB, xf_min_blocks<RB, WB, KIND>()) xform_pass(XfArgs<T, TI> A) {
     extern __shared__ __align__(16) unsigned char xf_smem[];
     T *sm = reinterpret_cast<T *>(xf_smem);
     constexpr int R = 1 << RB;
@@ -212,8 +231,8 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
                 yy[j] = A.y_io[g];
             }
         }
-        xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k1);
-        xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k3);
+        xf_forward<T, L, RB, WB, XF_UNIT>(v, sm, w, lane, A.k1);          // Q (unit form)
+        xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k3);                   // A Q (scaled)
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
@@ -260,6 +279,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
             }
         }
         if (KIND == K_P1 || KIND == K_P2 || KIND == K_FULL) xf_forward<T, L, RB, WB, XF_APRIME>(v, sm, w, lane, A.k1);
+        else if (KIND == K_P3) xf_forward<T, L, RB, WB, XF_UNIT>(v, sm, w, lane, A.k1);   // Q^T (unit form)
         else xf_forward<T, L, RB, WB, XF_GEN>(v, sm, w, lane, A.k1);
         // now in layout B (layout A when WB == 0)
         if constexpr (KIND == K_PLAIN || KIND == K_P1) {
@@ -273,7 +293,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
         if constexpr (KIND == K_P2 || KIND == K_FULL) {
 #pragma unroll
             for (int j = 0; j < R; ++j) v[j] = (zz[j] + A.b2 * xx[j] - v[j]) * A.ib1;
-            xf_backward<T, L, RB, WB>(v, sm, w, lane, A.k2);
+            xf_backward<T, L, RB, WB, XF_UNIT>(v, sm, w, lane, A.k2);        // Q^T (unit form)
             if (KIND == K_P2) {
 #pragma unroll
                 for (int j = 0; j < R; ++j)
@@ -288,8 +308,8 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
                 v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
                 u[j] = v[j];
             }
-            xf_forward<T, L, RB, WB>(v, sm, w, lane, A.k3);
-            xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k4);
+            xf_forward<T, L, RB, WB, XF_UNIT>(v, sm, w, lane, A.k3);      // Q (unit form)
+            xf_forward<T, L, RB, WB>(u, sm, w, lane, A.k4);               // A Q (scaled)
 #pragma unroll
             for (int j = 0; j < R; ++j) {
                 int row = WB ? row_B<RB, WB>(w, j) : row_A<RB, WB>(w, j);
@@ -317,7 +337,7 @@ __global__ void __launch_bounds__(32 << WB) xform_pass(XfArgs<T, TI> A) {
                 ll g = boff + xf_index<T, L, RB, WB>(s0, B, Nloc, tile, row, lane);
                 v[j] = v[j] * A.diag[__popcll((ull)(g & (Nloc - 1)))];
             }
-            xf_backward<T, L, RB, WB>(v, sm, w, lane, A.k2);
+            xf_backward<T, L, RB, WB, XF_UNIT>(v, sm, w, lane, A.k2);         // Q (unit form)
 #pragma unroll
             for (int j = 0; j < R; ++j) {
                 u[j] = v[j];
