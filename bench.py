@@ -25,6 +25,8 @@ reference_kernels   one certified solve of the same workload by the reference's 
         kernels (its source strings compiled by NVRTC, replayed with its host sequence:
         baseline/ref_replay.py), and value / its solves/s
 gpu_launches   the library's own count of the kernels the timed solves launched
+mixed_state    the same certified solve with a float32 state until its bracket stalls, then float64
+        (rumb_bm_params dtype RUMB_MIXED; the bounds are float64 throughout)
 cpu_baseline   the oracle (C restatement of the reference's iteration and certificate) on the host,
         a bounded sample of iterations extrapolated to solves/s by this run's iteration count
 
@@ -544,6 +546,28 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step_ms, e2e_ms = float(t[0]), float(t[1])
 
+    # the same solve with a float32 state until its bracket stalls, float64 to the end (informative;
+    # `value` stays the float64 state), timed the same way on rank 0
+    mixed = None
+    if rank == 0 and args.dtype == "float64":
+        par_m = ctx.bm_params(beta, check=CHECK, abs_tol=ABS_TOL, rel_tol=None, dtype="mixed", max_iter=10 ** 7,
+                              time_limit=600, overlap_check=True)
+        for _ in range(2):
+            ctx.bm_solve((prob_dev, None), par_m, want_fit=False)
+        ms_m, res_m = [], None
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res_m, _, _ = ctx.bm_solve((prob_dev, None), par_m, want_fit=False)
+            e1.record(stream)
+            e1.synchronize()
+            ms_m.append(e0.elapsed_time(e1))
+        mixed = {"solves_per_s": 1e3 / (sum(ms_m) / len(ms_m)), "ms_per_step": sum(ms_m) / len(ms_m),
+                 "iters_per_solve": int(res_m["iters"]), "iters_float32": int(res_m["iters_f32"]),
+                 "ub": res_m["ub"], "lb": res_m["lb"], "stop": res_m["stop_reason"]}
+
     # roofline of the dominant kernel: 20 iterations and one check after PROFILE_WARMUP iterations,
     # captured as a CUDA graph with CUDA events around every kernel and replayed (rumb_bm_profile)
     prof = ctx.bm_profile((prob_dev, None), par, iters=20, warmup=PROFILE_WARMUP)
@@ -601,6 +625,9 @@ def main():
         # one iteration's kernels under graph replay (the check's plain transforms left out)
         "iteration_ms": sum(k["total_ms"] for k in prof if ",plain>" not in k["name"]) / 20.0,
         "reference_kernels": ref_leg,
+        "mixed_state": dict(mixed, speedup_vs_reference_kernels=(mixed["solves_per_s"] * ref_leg["s_per_solve"]
+                                                                 if ref_leg and "s_per_solve" in ref_leg else None))
+        if mixed else None,
         "speedup_vs_reference_kernels": (value * ref_leg["s_per_solve"]
                                          if ref_leg and "s_per_solve" in ref_leg else None),
         "kernels": [{"name": k["name"], "share": round(k["total_ms"] / tot, 4),
