@@ -7,6 +7,8 @@
     python bench.py --workload bootstrap_n20             # batched bootstrap draws vs one at a time
     python bench.py --workload paper                     # paper instances beside the reference's times
     python bench.py --workload pricing --steps 20        # Flow-CG pricing sweeps alone
+    python bench.py --workload dsr_n25                   # p_hat's solve at the learned warm start's
+                                                          # shape (n = 25), time-boxed
 
 Workload "n18_d1pct_k50": every menu of 18 alternatives with >= 2 members kept with probability
 0.01 (2,627 menus, 23,650 observed cells), p_hat from a Dirichlet(1) mixture of 50 random linear
@@ -409,6 +411,41 @@ PAPER = {
 }
 
 
+def run_dsr_n25(args, rank, seconds=90.0):
+    """Workload dsr_n25 (n25_dsr301_panel520: n = 25, alternative 0 observed on 301 menus, a
+    520-respondent panel, K = 40; the learned warm start's configuration): p_hat's own certified
+    solve to abs 5e-4, bounded by `seconds` per state dtype, from the cold start. It measures what a
+    bootstrap at this shape must first do once -- certify p_hat -- and what one iteration costs
+    (8 slabs of 2^24 x 25 values), the reference's record being that its bm_admm did not certify
+    this shape in 4 hours (replication/empirical_dsr_n25/README.md:57-58)."""
+    if rank != 0:
+        return
+    import torch
+    from rumb import _lib
+    from rumb.instances import config_instance
+    n, m, a, p, _panel = config_instance("n25_dsr301_panel520")
+    ctx = _lib.Context(0)
+    beta = beta_rule(p.size)
+    prob = ctx.bm_problem(n, m.astype(np.uint32), a.astype(np.int32), p)
+    out = {}
+    for dt in ("float32", "float64"):
+        par = ctx.bm_params(beta, check=CHECK, abs_tol=5e-4, rel_tol=None, dtype=dt, max_iter=10 ** 7,
+                            time_limit=seconds, stall_checks=0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r, _, _ = ctx.bm_solve(prob, par, want_fit=False)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        out[dt] = {"seconds": wall, "iters": int(r["iters"]), "ms_per_iter": 1e3 * r["solve_s"] / max(1, r["iters"]),
+                   "lb": r["lb"], "ub": r["ub"], "gap": r["ub"] - r["lb"], "stop": r["stop_reason"],
+                   "setup_s": r["setup_s"]}
+    ctx.close()
+    print(json.dumps({"metric": "n=25 DSR p_hat certified solve, bounded (abs 5e-4)", "unit": "s", "n_gpus": 1,
+                      "data": "synthetic", "config": {"workload": "n25_dsr301_panel520", "cells": int(p.size),
+                                                      "time_box_s": seconds, "abs_tol": 5e-4},
+                      "runs": out}), flush=True)
+
+
 def run_paper(args, rank):
     """Workload paper: the reference's certified runs on two of its paper instances, regenerated
     from its generator (sha256 fingerprints checked): BM-ADMM on n20_d1pct (104,885 cells) in
@@ -448,7 +485,7 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing"],
+    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing", "dsr_n25"],
                     help="bootstrap_n20: the batched-draw comparison; paper: the reference's certified runs on "
                          "its paper instances beside its published times (each prints its own line)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
@@ -467,6 +504,9 @@ def main():
         return
     if args.workload == "pricing":
         run_pricing(args, rank)
+        return
+    if args.workload == "dsr_n25":
+        run_dsr_n25(args, rank)
         return
 
     import torch

@@ -181,6 +181,28 @@ def test_fused_and_unfused_sequences_track_oracle(ctx, monkeypatch, fuse, dtype)
         assert d <= tol * max(1.0, float(np.max(np.abs(ref)))), (name, d)
 
 
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_three_window_iteration_tracks_oracle(ctx, dtype):
+    """n = 21 splits the rest bits into three windows (the middle ones run as plain and dual
+    passes, the eigenvectors in unit form there too): 3 iterations against the oracle."""
+    from rumb.instances import mixture_instance
+    n = 21
+    menu, alt, p = mixture_instance(n, 0.0005, K=10, N=200, seed=21)
+    beta = O.beta_default(p.size)
+    dt = np.float64 if dtype == "float64" else np.float32
+    O.set_threads(0)
+    bm = O.BMOracle(n, menu, alt, p, dtype=dt)
+    prob = ctx.bm_problem(n, menu, alt, p)
+    par = ctx.bm_params(beta, dtype=dtype)
+    st = ctx.bm_iterate(prob, par, None, 3, cold_start=True)
+    bm.iterate(3)
+    tol = 1e-11 if dt == np.float64 else 1e-4
+    for name in ("x2", "s", "y", "z"):
+        ref = getattr(bm, name).astype(np.float64)
+        d = np.max(np.abs(st[name].astype(np.float64) - ref))
+        assert d <= tol * max(1.0, float(np.max(np.abs(ref)))), (name, d)
+
+
 def test_certified_solve_matches_oracle(ctx):
     n, menu, alt, p = config_instance("n10_all_k20")
     beta = O.beta_default(p.size)
