@@ -366,6 +366,187 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tau_kernel(ProxTileArgs<T>
     }
 }
 
+// The one-walk form with two staged arrays (more CTAs per SM): xo formed while staging, the
+// previous support kept as one bit per element.
+template <class T, int N>
+__global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T> P) {
+    extern __shared__ __align__(128) unsigned char pt_smem[];
+    if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
+    {
+        const ll boff = (ll)blockIdx.y * P.bstride;
+        P.x += boff;
+        P.x2 += boff;
+        P.z += boff;
+        P.xhat += boff;
+    }
+    const int tid = threadIdx.x;
+    const ll Nloc = P.Nloc;
+    constexpr int E_max = (int)prox_tile_elems(N);
+    T *sx = reinterpret_cast<T *>(pt_smem + 256);        // xo, then the threshold's value
+    T *sz = sx + E_max;                                    // z, then q
+    uint32_t *sbit = reinterpret_cast<uint32_t *>(sz + E_max);   // x2 > 0, a bit per element
+    const uint32_t base = (uint32_t)blockIdx.x << PT_M;
+    int *roff = reinterpret_cast<int *>(pt_smem + 16);
+    __shared__ long long rg[32];     // global start of each alternative's run
+    __shared__ int hi_alt[32];       // the j-th present high run's alternative
+    __shared__ double stau[PT_THREADS];
+    __shared__ uint32_t sobs[PT_THREADS];
+    __shared__ unsigned char sflag[PT_THREADS];
+    if (tid < N) {
+        roff[tid] = pt_roff(base, tid);
+        rg[tid] = pt_rstart(base, tid, Nloc);
+        if (tid >= PT_M && ((base >> tid) & 1u)) hi_alt[__popc(base & ((1u << tid) - 1u) & ~((1u << PT_M) - 1u))] = tid;
+    }
+    __syncthreads();
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int Et = PT_M * (1 << (PT_M - 1)) + __popc(base >> PT_M) * (1 << PT_M);
+    auto run_of = [&](int e) -> int {
+        return e < PT_M * (1 << (PT_M - 1)) ? (e >> (PT_M - 1)) : hi_alt[(e - PT_M * (1 << (PT_M - 1))) >> PT_M];
+    };
+    const T one = (T)1, two = (T)2;
+    // z staged as it is; the relaxed point xo = alpha x + (1 - alpha) x2 formed on the way in, with
+    // one bit per element for x2 > 0 (the previous support): two staged arrays instead of three
+    for (int c = tid; c < Et / VEC; c += PT_THREADS) {
+        const int e = c * VEC;
+        const int i = run_of(e);
+        const ll g = rg[i] + (e - roff[i]);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sz + e)), "l"(P.z + g) : "memory");
+        T xv[VEC], x2v[VEC];
+        *reinterpret_cast<uint4 *>(xv) = *reinterpret_cast<const uint4 *>(P.x + g);
+        *reinterpret_cast<uint4 *>(x2v) = *reinterpret_cast<const uint4 *>(P.x2 + g);
+        const unsigned am = __activemask();
+#pragma unroll
+        for (int t = 0; t < VEC; ++t) {
+            sx[e + t] = P.alpha * xv[t] + (one - P.alpha) * x2v[t];
+            const unsigned b = __ballot_sync(am, x2v[t] > (T)0);
+            if ((threadIdx.x & 31) == __ffs(am) - 1) sbit[(c >> 5) * VEC + t] = b;
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const uint32_t low = (uint32_t)tid;
+    const uint32_t S = base | low;
+    const uint32_t wb = P.menu_obs[S];
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const int k = __popc(S);
+    const bool mixed = wb != 0 && wb != S;
+    const double cw = (double)P.b2 + 2.0, cu = (double)P.b2, icw = 1.0 / cw, icu = 1.0 / cu;
+    auto xhat_of = [&](int i) -> T { return P.xhat[(ll)i * Nloc + (ll)cb32(S, i)]; };
+    uint32_t A0 = 0;
+    double s1 = 0.0, s2 = 0.0, f1 = 0.0, f2 = 0.0;
+    double min_on = INFINITY, max_off = -INFINITY;
+    for (uint32_t SS = S; SS; SS &= SS - 1) {
+        const int i = __ffs(SS) - 1;
+        const int e = roff[i] + (int)(i < PT_M ? cb32(low, i) : low);
+        const int ce = e / VEC;
+        const bool on = (sbit[(ce >> 5) * VEC + (e % VEC)] >> (ce & 31)) & 1u;
+        T xo = sx[e];
+        T zz = sz[e];
+        T v = xo - P.ib2 * zz;
+        sz[e] = zz - P.b2 * xo;
+        const bool w = (wb >> i) & 1u;
+        T xh = (T)0;
+        if (w) xh = xhat_of(i);
+        double ti, ic = 1.0;
+        if (mixed) {
+            sx[e] = v;
+            ti = (double)P.b2 * (double)v + (w ? 2.0 * (double)xh : 0.0);
+            ic = w ? icw : icu;
+        } else {
+            T val = (P.b2 * v + two * (w ? one : (T)0) * xh) * (w ? P.inv_c1 : P.inv_c0);
+            sx[e] = val;
+            ti = (double)val;
+        }
+        f1 += mixed ? ti * ic : ti;
+        f2 += ic;
+        if (on) {
+            A0 |= 1u << i;
+            s1 += mixed ? ti * ic : ti;
+            s2 += ic;
+            min_on = ti < min_on ? ti : min_on;
+        } else {
+            max_off = ti > max_off ? ti : max_off;
+        }
+    }
+    auto t_of = [&](int i, int e) -> double {
+        double ti = (double)sx[e];
+        if (mixed) ti = (double)P.b2 * ti + (((wb >> i) & 1u) ? 2.0 * (double)xhat_of(i) : 0.0);
+        return ti;
+    };
+    double tau = 0.0;
+    bool ok = false;
+    if (k > 1 && A0 != 0) {
+        tau = (s1 - 1.0) / s2;
+        ok = (min_on > tau) && !(max_off > tau);
+    }
+    if (k > 1 && !ok) {
+        uint32_t A = S;
+        s1 = f1;
+        s2 = f2;
+        tau = (s1 - 1.0) / s2;
+        for (int round = 0; round < 32; ++round) {
+            uint32_t A2 = 0;
+            s1 = 0.0;
+            s2 = 0.0;
+            for (uint32_t AA = A; AA; AA &= AA - 1) {
+                const int i = __ffs(AA) - 1;
+                const double ti = t_of(i, roff[i] + (int)(i < PT_M ? cb32(low, i) : low));
+                const double ic = mixed ? (((wb >> i) & 1u) ? icw : icu) : 1.0;
+                if (ti > tau) {
+                    A2 |= 1u << i;
+                    s1 += mixed ? ti * ic : ti;
+                    s2 += ic;
+                }
+            }
+            if (A2 == A) break;
+            A = A2;
+            tau = (s1 - 1.0) / s2;
+        }
+    }
+    stau[low] = tau;
+    sobs[low] = wb;
+    sflag[low] = (unsigned char)(k == 1 ? PT_SINGLE : (mixed ? PT_MIXED : PT_PLAIN));
+    __syncthreads();
+    // the projection and the write-back, element by element: element e of run i belongs to the
+    // menu base | low, low = e - roff[i] for a high run, the lows containing i in order for a low run
+    for (int c = tid; c < Et / VEC; c += PT_THREADS) {
+        const int e = c * VEC;
+        const int i = run_of(e);
+        const int pos = e - roff[i];
+        const ll g = rg[i] + pos;
+        T u2[VEC], z2[VEC];
+#pragma unroll
+        for (int t = 0; t < VEC; ++t) {
+            const int ps = pos + t;
+            const uint32_t lw = i >= PT_M ? (uint32_t)ps
+                                          : ((((uint32_t)ps >> i) << (i + 1)) | ((uint32_t)ps & ((1u << i) - 1u)) | (1u << i));
+            const double tau_m = stau[lw];
+            const int fl = sflag[lw];
+            T u;
+            if (fl == PT_SINGLE) {
+                u = one;
+            } else if (fl == PT_MIXED) {
+                const bool w = (sobs[lw] >> i) & 1u;
+                const double ti = (double)P.b2 * (double)sx[e + t] + (w ? 2.0 * (double)P.xhat[g + t] : 0.0);
+                const double yv = (ti - tau_m) / (w ? cw : cu);
+                u = yv > 0.0 ? (T)yv : (T)0;
+            } else {
+                const double yv = (double)sx[e + t] - tau_m;
+                u = yv > 0.0 ? (T)yv : (T)0;
+            }
+            u2[t] = u;
+            z2[t] = sz[e + t] + P.b2 * u;
+        }
+        if constexpr (sizeof(T) == 8) {
+            *reinterpret_cast<double2 *>(P.x2 + g) = make_double2(u2[0], u2[1]);
+            *reinterpret_cast<double2 *>(P.z + g) = make_double2(z2[0], z2[1]);
+        } else {
+            *reinterpret_cast<float4 *>(P.x2 + g) = make_float4(u2[0], u2[1], u2[2], u2[3]);
+            *reinterpret_cast<float4 *>(P.z + g) = make_float4(z2[0], z2[1], z2[2], z2[3]);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- lane-group form
 // G consecutive lanes share one menu S (a warp holds 32 / G consecutive menus); lane gl of the
 // group owns the members i = gl, gl + G, gl + 2G, ... of S. Every member's x, x2 and z are read
@@ -543,6 +724,17 @@ static void launch_tau_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     RUMB_LAUNCH("prox_tau_kernel");
 }
 
+template <class T, int N>
+static void launch_tau2_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
+    static std::atomic<unsigned long long> optin{0};   // the opt-in above 48 KB, per device
+    constexpr int E_max = (int)prox_tile_elems(N), VEC = 16 / (int)sizeof(T);
+    const size_t smem = 256 + 2 * (size_t)E_max * sizeof(T) + (size_t)((E_max / VEC + 31) / 32) * VEC * 4;
+    smem_optin(prox_tau2_kernel<T, N>, (int)smem, optin);
+    dim3 grid((unsigned)(1LL << (N - PT_M)), (unsigned)slots);
+    prox_tau2_kernel<T, N><<<grid, PT_THREADS, smem, st>>>(P);
+    RUMB_LAUNCH("prox_tau2_kernel");
+}
+
 template <class T, int N, int G>
 static void launch_lanes_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     dim3 grid((unsigned)(((1LL << N) * G) / 256), (unsigned)slots);
@@ -557,13 +749,14 @@ static void launch_form_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots, 
         case PROX_LANES4: launch_lanes_n<T, N, 4>(P, st, slots); return;
         case PROX_LANES8: launch_lanes_n<T, N, 8>(P, st, slots); return;
         case PROX_TAU: launch_tau_n<T, N>(P, st, slots); return;
+        case PROX_TAU2: launch_tau2_n<T, N>(P, st, slots); return;
         default: launch_tile_n<T, N>(P, st, slots); return;
     }
 }
 
 template <class T>
 void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots, int form) {
-    if (P.n > PROX_LANES_MAX_N && form != PROX_TAU) form = PROX_TILE;
+    if (P.n > PROX_LANES_MAX_N && form != PROX_TAU && form != PROX_TAU2) form = PROX_TILE;
     switch (P.n) {
 #define RUMB_PT_CASE(NN) \
     case NN: launch_form_n<T, NN>(P, st, slots, form); return;
@@ -572,7 +765,11 @@ void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots, int 
         RUMB_PT_CASE(20) RUMB_PT_CASE(21) RUMB_PT_CASE(22)
 #undef RUMB_PT_CASE
 #define RUMB_PT_CASE(NN) \
-    case NN: if (form == PROX_TAU) launch_tau_n<T, NN>(P, st, slots); else launch_tile_n<T, NN>(P, st, slots); return;
+    case NN:                                                                                                      \
+        if (form == PROX_TAU) launch_tau_n<T, NN>(P, st, slots);                                                  \
+        else if (form == PROX_TAU2) launch_tau2_n<T, NN>(P, st, slots);                                           \
+        else launch_tile_n<T, NN>(P, st, slots);                                                                  \
+        return;
         RUMB_PT_CASE(23) RUMB_PT_CASE(24) RUMB_PT_CASE(25)
         RUMB_PT_CASE(26) RUMB_PT_CASE(27) RUMB_PT_CASE(28) RUMB_PT_CASE(29) RUMB_PT_CASE(30)
 #undef RUMB_PT_CASE

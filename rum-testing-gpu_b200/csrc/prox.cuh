@@ -108,9 +108,11 @@ __device__ __forceinline__ ll pt_rstart(uint32_t base, int i, ll Nloc) {
 
 // The forms of the prox kernel (csrc/prox.cu): the shared-memory tile; the tile with one pass over
 // each menu's members (the menu's threshold kept in shared memory, the projection and the write-back
-// done element by element); or G lanes per menu reading the slab straight into registers
+// done element by element; x, x2, z staged, or the relaxed point and z with a support bit); or G
+// lanes per menu reading the slab straight into registers
 // (n <= PROX_LANES_MAX_N). Picked per GPU, n and dtype by timing (the iteration's autotuner).
-constexpr int PROX_TILE = 0, PROX_LANES2 = 1, PROX_LANES4 = 2, PROX_LANES8 = 3, PROX_TAU = 4, PROX_FORMS = 5;
+constexpr int PROX_TILE = 0, PROX_LANES2 = 1, PROX_LANES4 = 2, PROX_LANES8 = 3, PROX_TAU = 4, PROX_TAU2 = 5,
+              PROX_FORMS = 6;
 constexpr int PROX_LANES_MAX_N = 22;
 
 // The prox for one dtype (csrc/prox.cu; grid.y = batched draws' slots).
