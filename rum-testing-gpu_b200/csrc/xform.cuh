@@ -195,14 +195,14 @@ __device__ __forceinline__ ll xf_index(int s0, int B, ll Nloc, ll tile, int row,
 }
 
 // CTAs kept resident per SM: the four-stream kinds with 8 values a thread and 256 threads are held
-// to 128 registers so that two CTAs fit an SM
-template <int RB, int WB, int KIND>
+// to 128 registers so that two CTAs fit an SM (85, three CTAs, on the low window)
+template <int L, int RB, int WB, int KIND>
 constexpr int xf_min_blocks() {
-    return ((KIND == K_P4 || KIND == K_P4A) && RB <= 3 && WB == 3) ? 2 : 1;
+    return ((KIND == K_P4 || KIND == K_P4A) && RB <= 3 && WB == 3) ? (L ? 3 : 2) : 1;
 }
 
 template <class T, class TI, int L, int RB, int WB, int KIND>
-__global__ void __launch_bounds__(32 << WB, xf_min_blocks<RB, WB, KIND>()) xform_pass(XfArgs<T, TI> A) {
+__global__ void __launch_bounds__(32 << WB, xf_min_blocks<L, RB, WB, KIND>()) xform_pass(XfArgs<T, TI> A) {
     extern __shared__ __align__(16) unsigned char xf_smem[];
     T *sm = reinterpret_cast<T *>(xf_smem);
     constexpr int R = 1 << RB;
