@@ -196,7 +196,9 @@ def test_three_window_iteration_tracks_oracle(ctx, dtype):
     par = ctx.bm_params(beta, dtype=dtype)
     st = ctx.bm_iterate(prob, par, None, 3, cold_start=True)
     bm.iterate(3)
-    tol = 1e-11 if dt == np.float64 else 1e-4
+    # float32: the rounding of 4 (n - 1) butterfly stages per iteration in another order, as in
+    # test_iterates_track_oracle at n >= 14
+    tol = 1e-11 if dt == np.float64 else 1e-3
     for name in ("x2", "s", "y", "z"):
         ref = getattr(bm, name).astype(np.float64)
         d = np.max(np.abs(st[name].astype(np.float64) - ref))
