@@ -7,6 +7,7 @@
     python bench.py --workload bootstrap_n20             # batched bootstrap draws vs one at a time
     python bench.py --workload paper                     # paper instances beside the reference's times
     python bench.py --workload pricing --steps 20        # Flow-CG pricing sweeps alone
+    python bench.py --workload pricing_large             # pricing calls at n = 28, 30, 32 (pairwise)
     python bench.py --workload dsr_n25                   # p_hat's solve at the learned warm start's
                                                           # shape (n = 25), time-boxed
 
@@ -411,6 +412,47 @@ PAPER = {
 }
 
 
+# the reference's published large-n pricing times (RTX 5090, pairwise instances):
+# solver/flow_cg/MEMORY.md:61 (mask sweep) and :67-69 (one column at n = 32)
+LARGE_N_PUBLISHED = {"mask_sweep_ms": {20: 0.4, 28: 39.0, 30: 170.0},
+                     "column_s_n32": {"mask": 0.70, "f32": 0.70, "u16": 0.72}}
+
+
+def run_pricing_large(args, rank, sweeps=3):
+    """Workload pricing_large: one pricing call (sweep, backtrace, read-back) on the reference's
+    pairwise instances at n = 28, 30 and 32, in mask storage (n <= 30) and float32 / uint16 stream
+    storage (rows scanned per subset: the lists are not built above n = 26), seeded float32
+    scores; beside the reference's published RTX 5090 times for the same instances."""
+    if rank != 0:
+        return
+    import torch
+    from rumb import _lib, flow_cg
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import paper_instances as PI
+    ctx = _lib.Context(0)
+    out = {}
+    for n in (28, 30, 32):
+        cd, _ = PI.gen_pairwise(n)
+        menus, alts, p32, offsets, _ = flow_cg.prepare_choice_data(cd[:, 0], cd[:, 1], cd[:, 2], n)
+        scores = np.random.default_rng(n).standard_normal(menus.size).astype(np.float32)
+        row = {}
+        for mode in (("mask", "f32", "u16") if n <= 30 else ("f32", "u16")):
+            pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+            pr.price(scores)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(sweeps):
+                pr.price(scores)
+            torch.cuda.synchronize()
+            row[mode + "_ms"] = 1e3 * (time.perf_counter() - t0) / sweeps
+            pr.close()
+        out["n%d" % n] = row
+    ctx.close()
+    print(json.dumps({"metric": "Flow-CG pricing call at large n (pairwise), ms", "unit": "ms", "n_gpus": 1,
+                      "higher_is_better": False, "data": "the reference's pairwise instances (regenerated)",
+                      "runs": out, "reference_rtx5090": LARGE_N_PUBLISHED}), flush=True)
+
+
 def run_dsr_n25(args, rank, seconds=90.0):
     """Workload dsr_n25 (n25_dsr301_panel520: n = 25, alternative 0 observed on 301 menus, a
     520-respondent panel, K = 40; the learned warm start's configuration): p_hat's own certified
@@ -485,7 +527,7 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing", "dsr_n25"],
+    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing", "pricing_large", "dsr_n25"],
                     help="bootstrap_n20: the batched-draw comparison; paper: the reference's certified runs on "
                          "its paper instances beside its published times (each prints its own line)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
@@ -507,6 +549,9 @@ def main():
         return
     if args.workload == "dsr_n25":
         run_dsr_n25(args, rank)
+        return
+    if args.workload == "pricing_large":
+        run_pricing_large(args, rank)
         return
 
     import torch

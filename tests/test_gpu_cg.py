@@ -316,3 +316,20 @@ def test_config3_column_sequence_matches_recorded_reference(ctx, mode):
                            record_columns=True)
     np.testing.assert_array_equal(np.array(res["picked"]), g["picked_" + mode])
     assert [res["lb"], res["distance"]] == g["bracket_" + mode].tolist()
+
+
+def test_mask_pricer_at_n28_equals_float32_stream(ctx):
+    """The mask pricer at n = 28 (2^28 float32 values, 1 GiB) gives the float32 stream pricer's
+    value and ranking bit for bit (the reference's own check, validation/feasibility/
+    test_stream_pricer.py:56-84, at the large-n end)."""
+    n = 28
+    cd, _ = PI.gen_pairwise(n)
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    scores = (np.random.RandomState(29).randn(menus.size)).astype(np.float32)
+    pm = _lib.Pricer(ctx, n, menus, offsets, mode="mask")
+    ps = _lib.Pricer(ctx, n, menus, offsets, mode="f32")
+    vm, rm, _ = pm.price(scores)
+    vs, rs, _ = ps.price(scores)
+    assert vm == vs and np.array_equal(rm, rs)
+    pm.close()
+    ps.close()

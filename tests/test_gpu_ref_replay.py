@@ -208,3 +208,24 @@ def test_config3_columns_match_reference_kernels_every_iteration(ctx, mode):
     if os.path.exists(gold):
         g = np.load(gold)
         np.testing.assert_array_equal(np.array(res["picked"]), g["picked_" + mode])
+
+
+# ------------------------------------------------------------------ large lattices
+@pytest.mark.parametrize("mode", ["f32", "u16", "u24"])
+def test_stream_pricer_at_n28_matches_reference_kernels(ctx, mode):
+    """The stream pricer at n = 28 (pairwise menus, 756 rows; 2^28 subsets, rows scanned per
+    subset as the lists are not built above n = 26) against the reference's own stream kernels:
+    the same Vmax, ranking, per-layer steps and margin (solver/flow_cg/pricing_stream.py:61-181,
+    302-412; the reference's large-n pricing path, solver/flow_cg/MEMORY.md:59-74)."""
+    n = 28
+    cd, _ = PI.gen_pairwise(n)
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+    scores = (np.random.RandomState(28).randn(menus.size)).astype(np.float32)
+    v_ref, r_ref, m_ref, steps_ref = ref_replay.price_stream(menus, alts, scores, offsets, n, mode=mode)
+    v, r, m, steps = pr.price(scores, want_steps=True)
+    assert v == v_ref, (v, v_ref)
+    np.testing.assert_array_equal(r, r_ref)
+    np.testing.assert_array_equal(steps, steps_ref)
+    assert abs(m - m_ref) <= 1e-6 * max(1.0, m_ref)
+    pr.close()
