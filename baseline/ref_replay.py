@@ -145,8 +145,18 @@ def _colex_rank(mask):
     return r
 
 
-def _gosper(n, k):
-    return np.array([m for m in range(1 << n) if bin(m).count("1") == k], dtype=np.int32)
+def _layers(n):
+    """The masks of popcount k in ascending order, k = 0 .. n (the reference's layer tables)."""
+    m = np.arange(1 << n, dtype=np.uint32)
+    x = m - ((m >> np.uint32(1)) & np.uint32(0x55555555))
+    x = (x & np.uint32(0x33333333)) + ((x >> np.uint32(2)) & np.uint32(0x33333333))
+    x = (x + (x >> np.uint32(4))) & np.uint32(0x0F0F0F0F)
+    pc = ((x * np.uint32(0x01010101)) >> np.uint32(24)).astype(np.uint8)
+    del x
+    order = np.argsort(pc, kind="stable").astype(np.int32)
+    bounds = np.concatenate(([0], np.cumsum(np.bincount(pc, minlength=n + 1))))
+    return [order[bounds[k]:bounds[k + 1]] for k in range(n + 1)]
+
 
 
 def price_mask_sub(L, masks_u32, scores_f32, offs_u64, K):
@@ -157,8 +167,9 @@ def price_mask_sub(L, masks_u32, scores_f32, offs_u64, K):
     gm = torch.from_numpy(np.ascontiguousarray(masks_u32).view(np.int32)).cuda()
     gs = torch.from_numpy(np.ascontiguousarray(scores_f32)).cuda()
     go = torch.from_numpy(np.ascontiguousarray(offs_u64).view(np.int64)).cuda()
+    lay = _layers(K)
     for c in range(1, K + 1):
-        st = torch.from_numpy(_gosper(K, c)).cuda()
+        st = torch.from_numpy(np.ascontiguousarray(lay[c])).cuda()
         ns = st.numel()
         L.launch("bf_update", (ns + 255) // 256, 256, [V, pred, gm, gs, go, st, (_I, ns)])
     torch.cuda.synchronize()
@@ -324,7 +335,7 @@ class BMReplay:
             lam *= np.where(b1s > 0, evals[1], evals[0])
         self.inv_gl = torch.from_numpy(1.0 / (1.0 + lam)).cuda()
         self.Q, self.Qt, self.p_ = Q, Q.T, pp
-        masks = np.concatenate([_gosper(n, k) for k in range(1, n + 1)])
+        masks = np.concatenate(_layers(n)[1:])
         self.all_masks = torch.from_numpy(masks).cuda()
         self.n_menus = masks.size
         self.b1 = self.b2 = float(beta)
@@ -681,7 +692,7 @@ def time_pricing(menus, offsets, scores, n, reps=10):
     V = torch.zeros(1 << n, dtype=torch.float32, device="cuda")
     P = torch.zeros(1 << n, dtype=torch.uint8, device="cuda")
     gm32 = torch.from_numpy(np.asarray(menus, dtype=np.uint64).astype(np.uint32).view(np.int32)).cuda()
-    states = [torch.from_numpy(_gosper(n, c)).cuda() for c in range(n + 1)]
+    states = [torch.from_numpy(np.ascontiguousarray(t)).cuda() for t in _layers(n)]
 
     def mask_sweep():
         for c in range(1, n + 1):

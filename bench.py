@@ -415,29 +415,46 @@ PAPER = {
 # the reference's published large-n pricing times (RTX 5090, pairwise instances):
 # solver/flow_cg/MEMORY.md:61 (mask sweep) and :67-69 (one column at n = 32)
 LARGE_N_PUBLISHED = {"mask_sweep_ms": {20: 0.4, 28: 39.0, 30: 170.0},
-                     "column_s_n32": {"mask": 0.70, "f32": 0.70, "u16": 0.72}}
+                     "column_s_n32": {"mask": 0.70, "f32": 0.70, "u16": 0.72},
+                     "column_s_n33": {"f32": 1.62, "u16": 1.72}}
+
+
+PRICING_LARGE = ((20, ("mask", "f32", "f32_stream", "u16")), (28, ("mask", "f32", "f32_stream", "u16")),
+                 (30, ("mask", "f32", "f32_stream", "u16")), (32, ("mask", "f32", "f32_stream", "u16")),
+                 (33, ("mask", "f32")))
 
 
 def run_pricing_large(args, rank, sweeps=3):
-    """Workload pricing_large: one pricing call (sweep, backtrace, read-back) on the reference's
-    pairwise instances at n = 28, 30 and 32, in mask storage (n <= 30) and float32 / uint16 stream
-    storage (rows scanned per subset: the lists are not built above n = 26), seeded float32
-    scores; beside the reference's published RTX 5090 times for the same instances."""
+    """Workload pricing_large: one pricing call (sweep, backtrace or readout, read-back) on the
+    reference's pairwise instances at n = 20 to 33, in mask storage (the tile sweep: 5 * 2^n bytes,
+    20 GiB at n = 32, 40 GiB at n = 33), float32 storage (by mask where it fits, the same bits),
+    float32 forced to two rank-indexed layers (f32_stream) and uint16 storage (rows scanned per
+    subset above n = 26, where the cover lists are not built), seeded float32 scores; beside the
+    reference's published RTX 5090 times for the same instances. --pricing-n / --pricing-modes
+    restrict the list (one small case for a profiler)."""
     if rank != 0:
         return
     import torch
     from rumb import _lib, flow_cg
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import paper_instances as PI
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    import ref_replay
     ctx = _lib.Context(0)
     out = {}
-    for n in (28, 30, 32):
+    only_n = {int(v) for v in args.pricing_n.split(",")} if args.pricing_n else None
+    only_modes = set(args.pricing_modes.split(",")) if args.pricing_modes else None
+    for n, modes in PRICING_LARGE:
+        if only_n is not None and n not in only_n:
+            continue
+        modes = [m for m in modes if only_modes is None or m in only_modes]
         cd, _ = PI.gen_pairwise(n)
         menus, alts, p32, offsets, _ = flow_cg.prepare_choice_data(cd[:, 0], cd[:, 1], cd[:, 2], n)
         scores = np.random.default_rng(n).standard_normal(menus.size).astype(np.float32)
         row = {}
-        for mode in (("mask", "f32", "u16") if n <= 30 else ("f32", "u16")):
-            pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+        for mode in modes:
+            pr = _lib.Pricer(ctx, n, menus, offsets, mode="f32" if mode == "f32_stream" else mode,
+                             stream=mode == "f32_stream")
             pr.price(scores)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -446,6 +463,11 @@ def run_pricing_large(args, rank, sweeps=3):
             torch.cuda.synchronize()
             row[mode + "_ms"] = 1e3 * (time.perf_counter() - t0) / sweeps
             pr.close()
+        if n <= 28 and ref_replay.available():
+            # the reference's own layer kernels on the same B200 and scores (launches only)
+            ref = ref_replay.time_pricing(menus, offsets, scores, n, reps=2)
+            row["reference_kernels_ms"] = {"u24": ref["u24_layers_ms"], "u16": ref["u16_layers_ms"],
+                                           "mask": ref["mask_layers_ms"]}
         out["n%d" % n] = row
     ctx.close()
     print(json.dumps({"metric": "Flow-CG pricing call at large n (pairwise), ms", "unit": "ms", "n_gpus": 1,
@@ -527,6 +549,8 @@ def main():
     ap.add_argument("--dtype", default="float64", choices=["float64", "mixed", "float32"])
     ap.add_argument("--impl", default="rumb", choices=["rumb", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--pricing-n", default="", help="pricing_large: comma-separated n to run (default all)")
+    ap.add_argument("--pricing-modes", default="", help="pricing_large: comma-separated storages to run")
     ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing", "pricing_large", "dsr_n25"],
                     help="bootstrap_n20: the batched-draw comparison; paper: the reference's certified runs on "
                          "its paper instances beside its published times (each prints its own line)")

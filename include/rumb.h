@@ -222,8 +222,10 @@ RUMB_API int rumb_bm_solve_batch(rumb_ctx *ctx, const rumb_bm_problem *prob, con
 
 /* ---------------------------------------------------------------- Flow-CG pricing */
 /* pricing storage of the lattice values */
-#define RUMB_PRICE_MASK 0 /* float32 per subset (2^n values, n <= 30) */
-#define RUMB_PRICE_F32 1  /* rank-indexed, two live layers, float32 */
+#define RUMB_PRICE_MASK 0 /* float32 per subset (2^n values and 2^n predecessor bytes, n <= 34) */
+#define RUMB_PRICE_F32 1  /* float32 values: stored by mask when 5 * 2^n bytes fit half the free device
+                           * memory (the same bits as two live rank-indexed layers, and the mask's
+                           * speed), else rank-indexed with two live layers */
 #define RUMB_PRICE_U16 2  /* rank-indexed, 16-bit mantissa per rank + float32 (offset, step) per 1024 ranks */
 #define RUMB_PRICE_U24 3  /* rank-indexed, 24-bit mantissa per rank + float32 (offset, step) per 1024 ranks */
 /* OR-ed into mode: evaluate w(x, D) by scanning x's rows in every sweep. Without it the pricer
@@ -231,6 +233,8 @@ RUMB_API int rumb_bm_solve_batch(rumb_ctx *ctx, const rumb_bm_problem *prob, con
  * row order (when n <= 26, the lists have < 2^32 entries and fit a quarter of the free device
  * memory), and a sweep adds exactly those rows' scores: the same float32 sums, far fewer tests. */
 #define RUMB_PRICE_SCAN 16
+/* OR-ed into RUMB_PRICE_F32: keep the rank-indexed two-layer storage whatever the free memory. */
+#define RUMB_PRICE_STREAM 32
 
 /* A pricer over the rows (menu bitmask, alternative) in x-major order: offsets[x]..offsets[x+1]
  * are alternative x's rows (offsets has n+1 entries, offsets[n] = mp). k_pred: predecessors are

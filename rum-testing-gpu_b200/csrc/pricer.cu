@@ -439,16 +439,19 @@ struct PriceOut {
     unsigned int qtop;     // u16 / u24: quantized top value
     int rank_pos[MAXN_PR];
     int error;
+    int pos;               // descent only: elements placed by the descent
+    ull node;              // descent only: the node reached at layer k_pred
 };
 
 // Descent through the stored predecessor layers (stream modes), then the mask DP on the
 // sub-lattice of the node reached; one CTA. V/pred scratch: 2^K entries (K = k_pred); Ws: the
-// 2^K K sub-lattice sums.
+// 2^K K sub-lattice sums. descend_only: stop after the descent and leave the node and the number
+// of placed elements in *out (the larger sub-lattices run as a tile sweep of their own).
 __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *const *preds, const ull *menus,
                                  const float *scores, const ll *offsets, float *Vs, uint8_t *Ps, PriceOut *out,
                                  const float *vtop_f, const uint16_t *vtop_h, const uint8_t *ltop, const float *mtop,
                                  const float *etop, int mode, int wmode, const unsigned *loffs, const void *lent,
-                                 const ull *layer_base, float *Ws) {
+                                 const ull *layer_base, float *Ws, int descend_only) {
     __shared__ ull sD;
     __shared__ int elems[MAXN_PR];
     __shared__ int spos;
@@ -479,6 +482,14 @@ __global__ void backtrace_kernel(int n, int k_pred, const ull *binom, uint8_t *c
         }
     }
     __syncthreads();
+    if (descend_only) {                 // the sub-lattice is solved by the tile sweep
+        if (threadIdx.x == 0) {
+            out->node = sD;
+            out->pos = spos;
+            out->error = 0;
+        }
+        return;
+    }
     const ull D = sD;
     const int K = __popcll(D);
     const ull Nsub = 1ULL << K;
@@ -551,6 +562,366 @@ __global__ void mask_readout_kernel(int n, const float *V, const uint8_t *pred, 
     out->error = 0;
 }
 
+// Mask storage by tiles. The lattice V[D] (D < 2^n, float32, indexed by the mask) splits into tiles
+// of MT_TILE = 256 consecutive masks: tile H holds D = H * 256 + L, L < 256 (alternatives 0..7 are
+// the tile's low bits, L = lane + 32 j: bits 0-4 the lane, bits 5-7 the thread's register j). One
+// warp computes one tile; one launch covers the tiles whose high part H has popcount t, for
+// t = 0 .. n - 8, so every tile H ^ {x} a tile reads was written by the launch before. Per tile:
+//   w(x, D) for every x in D: one pass over x's rows for the whole tile. A row whose menu's high
+//     part is not a subset of H fails for all 256 masks (a warp-uniform skip); otherwise the lane
+//     test (menu bits 0-4 within the lane's) gives the lane's addend (the score or +0, which leaves
+//     a sum unchanged: a sum that starts at +0 is never -0) and a warp-uniform switch on the menu's
+//     bits 5-7 adds it to the registers j that contain them, in row order;
+//   high x in H: V[D \ {x}] is the same L of tile H ^ {x} (coalesced loads), merged at once;
+//   low x in L: V[D \ {x}] is a mask of the same tile, so the tile's values and w(x, D) go to
+//     shared memory and the low candidates are merged by popcount rounds of L (the masks of
+//     popcount q are final once round q ends; a round's masks read only rounds before it).
+// Sums add x's qualifying rows in row order, one float32 add at a time (the row scan's and the
+// cover lists' sums), and candidates merge with the larger value winning and, on equal values,
+// the lower x: V and the predecessor bytes are the layer kernels' bit for bit. The lattice is read
+// once per (D, x in D) at 4 bytes over coalesced lines and written once, with no layer table.
+// Scores are finite (a +0 addend and a skipped row are then the same).
+constexpr int MT_LOW = 8, MT_TILE = 1 << MT_LOW, MT_WARPS = 4, MT_REGS = MT_TILE / 32;
+constexpr int MASK_MIN_N_TILE = MT_LOW + 1;
+constexpr int MASK_MAX_N = 34;
+
+struct MaskTileArgs {
+    int n, h, t;
+    ull count;                 // tiles in this launch: C(h, t)
+    const ull *binom;          // C(b, k) at b*bstride+k
+    int bstride;
+    const int4 *rows;          // x-major rows {menu >> 8, menu & 31, score bits, (menu >> 5) & 7}
+    const ll *offsets;
+    float *V;
+    uint8_t *P;
+};
+
+// Row records for the tile and group sweeps, rebuilt with each call's scores:
+// {menu >> shift, menu & ymask, score bits, (menu >> 5) & 7}; idx (may be NULL) maps record i to the
+// row whose score it carries (the restricted rows of a sub-lattice).
+__global__ void rows_kernel(ll mp, const ull *menus, const float *scores, const int *idx, int shift, unsigned ymask,
+                            int4 *rows) {
+    const ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (i >= mp) return;
+    const ull m = menus[i];
+    const float sc = scores[idx ? (ll)idx[i] : i];
+    rows[i] = make_int4((int)(unsigned)(m >> shift), (int)((unsigned)m & ymask), __float_as_int(sc),
+                        (int)(unsigned)((m >> 5) & 7ULL));
+}
+
+// Row records are read ROW_PF at a time ahead of their use; ROW_NONE pads the last batch (its high
+// part has every bit set, so no tile or group takes it: their high parts have at most 29 bits).
+constexpr int ROW_PF = 8;
+#define ROW_NONE make_int4(-1, 0, 0, 0)
+
+__device__ __forceinline__ void mt_merge(float &v, int &b, float c, int x) {
+    if (b < 0 || c > v || (c == v && x < b)) {
+        v = c;
+        b = x;
+    }
+}
+
+// acc[j] += s for the registers j that contain mr (j's bits 5-7 of L; mr warp-uniform).
+__device__ __forceinline__ void mt_add(float (&acc)[MT_REGS], int mr, float s) {
+#define MT_A(j) acc[j] = __fadd_rn(acc[j], s)
+    switch (mr) {
+        case 0: MT_A(0); MT_A(1); MT_A(2); MT_A(3); MT_A(4); MT_A(5); MT_A(6); MT_A(7); break;
+        case 1: MT_A(1); MT_A(3); MT_A(5); MT_A(7); break;
+        case 2: MT_A(2); MT_A(3); MT_A(6); MT_A(7); break;
+        case 3: MT_A(3); MT_A(7); break;
+        case 4: MT_A(4); MT_A(5); MT_A(6); MT_A(7); break;
+        case 5: MT_A(5); MT_A(7); break;
+        case 6: MT_A(6); MT_A(7); break;
+        default: MT_A(7); break;
+    }
+#undef MT_A
+}
+
+// The 256 low masks ordered by popcount (ascending masks within one popcount), and where each
+// popcount starts.
+struct MtOrder {
+    uint8_t order[MT_TILE];
+    int qoff[MT_LOW + 2];
+};
+static MtOrder mt_order_host() {
+    MtOrder o{};
+    int k = 0;
+    for (int q = 0; q <= MT_LOW; ++q) {
+        o.qoff[q] = k;
+        for (int L = 0; L < MT_TILE; ++L)
+            if (__builtin_popcount(L) == q) o.order[k++] = (uint8_t)L;
+    }
+    o.qoff[MT_LOW + 1] = k;
+    return o;
+}
+
+// Index of a low mask L that contains x among the 128 that do: L without bit x.
+__device__ __forceinline__ int mt_half(int L, int x) { return ((L >> (x + 1)) << x) | (L & ((1 << x) - 1)); }
+
+__global__ void __launch_bounds__(32 * MT_WARPS) mask_tile_kernel(MaskTileArgs A, MtOrder ord) {
+    __shared__ float wl[MT_WARPS][MT_LOW][MT_TILE / 2];   // w(x, D) for low x, at mt_half(L, x) (x in L)
+    __shared__ float vt[MT_WARPS][MT_TILE];
+    __shared__ uint8_t bt[MT_WARPS][MT_TILE];
+    __shared__ unsigned sbin[(MASK_MAX_N - MT_LOW + 1) * (MASK_MAX_N - MT_LOW + 1)];   // C(b, k), b, k <= h
+    __shared__ uint8_t sord[MT_TILE];
+    const int n = A.n, h = A.h;
+    for (int i = threadIdx.x; i < (h + 1) * (h + 1); i += blockDim.x)
+        sbin[i] = (unsigned)A.binom[(i / (h + 1)) * A.bstride + i % (h + 1)];
+    for (int i = threadIdx.x; i < MT_TILE; i += blockDim.x) sord[i] = ord.order[i];
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const ull tile = (ull)blockIdx.x * MT_WARPS + w;
+    if (tile >= A.count) return;                          // whole warps leave
+    unsigned H = 0;                                       // colex unranking of the tile in [0, h)
+    {
+        unsigned r = (unsigned)tile;
+        int b = h - 1;
+        for (int k = A.t; k >= 1; --k) {
+            while (sbin[b * (h + 1) + k] > r) --b;
+            H |= 1u << b;
+            r -= sbin[b * (h + 1) + k];
+            --b;
+        }
+    }
+    const unsigned nH = ~H, nlane = ~(unsigned)lane;
+    const ull base = (ull)H << MT_LOW;
+    float best[MT_REGS];
+    int bx[MT_REGS];
+#pragma unroll
+    for (int j = 0; j < MT_REGS; ++j) {
+        best[j] = 0.0f;
+        bx[j] = -1;
+    }
+    for (int x = 0; x < n; ++x) {
+        const bool high = x >= MT_LOW;
+        if (high && !((H >> (x - MT_LOW)) & 1u)) continue;      // uniform per warp
+        float prev[MT_REGS];
+        if (high) {
+            const float *pv = A.V + (base ^ (1ULL << x)) + lane;
+#pragma unroll
+            for (int j = 0; j < MT_REGS; ++j) prev[j] = pv[32 * j];
+        }
+        float acc[MT_REGS];
+#pragma unroll
+        for (int j = 0; j < MT_REGS; ++j) acc[j] = 0.0f;
+        const int lo = (int)A.offsets[x], hi = (int)A.offsets[x + 1];
+        for (int i0 = lo; i0 < hi; i0 += ROW_PF) {
+            int4 R[ROW_PF];                                     // loaded ahead: the skips depend on them
+#pragma unroll
+            for (int u = 0; u < ROW_PF; ++u) R[u] = i0 + u < hi ? __ldg(A.rows + i0 + u) : ROW_NONE;
+#pragma unroll
+            for (int u = 0; u < ROW_PF; ++u) {
+                if ((unsigned)R[u].x & nH) continue;            // uniform: fails for the whole tile
+                const float s = ((unsigned)R[u].y & nlane) ? 0.0f : __int_as_float(R[u].z);
+                mt_add(acc, R[u].w, s);
+            }
+        }
+        if (high) {
+#pragma unroll
+            for (int j = 0; j < MT_REGS; ++j) mt_merge(best[j], bx[j], __fadd_rn(prev[j], acc[j]), x);
+        } else {
+#pragma unroll
+            for (int j = 0; j < MT_REGS; ++j) {
+                const int L = lane + 32 * j;
+                if ((L >> x) & 1) wl[w][x][mt_half(L, x)] = acc[j];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < MT_REGS; ++j) {
+        vt[w][lane + 32 * j] = best[j];
+        bt[w][lane + 32 * j] = (uint8_t)(bx[j] < 0 ? 255 : bx[j]);
+    }
+    __syncwarp();
+    // low candidates, popcount round by popcount round (the round's masks share their popcount q,
+    // so every lane walks q bits)
+    for (int q = 1; q <= MT_LOW; ++q) {
+        for (int idx = ord.qoff[q] + lane; idx < ord.qoff[q + 1]; idx += 32) {
+            const int L = sord[idx];
+            float v = vt[w][L];
+            int b = bt[w][L] == 255 ? -1 : (int)bt[w][L];
+            for (unsigned m = (unsigned)L; m; m &= m - 1u) {
+                const int x = __ffs((int)m) - 1;
+                mt_merge(v, b, __fadd_rn(vt[w][L ^ (1 << x)], wl[w][x][mt_half(L, x)]), x);
+            }
+            vt[w][L] = v;
+            bt[w][L] = (uint8_t)(b < 0 ? 255 : b);
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int j = 0; j < MT_REGS; ++j) {
+        const int L = lane + 32 * j;
+        A.V[base + L] = vt[w][L];
+        A.P[base + L] = bt[w][L] == 255 ? (uint8_t)0 : bt[w][L];
+    }
+}
+
+// The sub-lattice ranking after a tile sweep over the K elements left by the descent: positions
+// pos .. pos + K - 1 in the order the sub-lattice's predecessors give (element j of the sub-problem
+// is alternative elems[j]).
+struct SubElems {
+    int e[MAXN_PR];
+};
+__global__ void sub_readout_kernel(int K, const float *V, const uint8_t *pred, SubElems el, int mode, PriceOut *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ull D = (1ULL << K) - 1ULL;
+    const int pos = out->pos;
+    if (mode == 0) out->vtop = V[D];
+    for (int i = 0; i < K; ++i) {
+        const int j = pred[D];
+        out->rank_pos[el.e[j]] = pos + i;
+        D ^= 1ULL << j;
+    }
+    out->error = 0;
+}
+
+// Stream storage by groups (layers whose w(x, D) scans rows). The subsets of layer k whose elements
+// >= SG_LOW agree (the high part H, t = |H| elements) and whose low part L has l = k - t elements
+// take consecutive colex ranks: with H's elements a_0 < a_1 < ..., rank(L u H) = rank_l(L) +
+// base(H, l), base(H, l) = sum_i C(a_i, l + i + 1), rank_l(L) = L's rank among the l-subsets of
+// [0, SG_LOW) (ascending masks). One warp computes one group: slot s = lane + 32 j holds the l-subset
+// of rank s (C(SG_LOW, l) <= 252 slots). Per group and alternative x in D:
+//   x in H: D \ {x} is (L, H \ {x}) in layer k - 1, rank base(H \ {x}, l) + s (coalesced);
+//   x in L: D \ {x} is (L \ {x}, H), rank base(H, l - 1) + rank_{l-1}(L \ {x});
+//   w(x, D): one pass over x's rows for the group; a row whose menu's high part is not within H
+//   fails for every slot (a warp-uniform skip), the others are tested on the low part per slot.
+// Values are decoded from the previous layer's storage and candidates merge with the larger value
+// winning and, on equal values, the lower x (the row scan's x descending with `>=`): the layer is
+// the layer kernels' bit for bit, and stream_quant_kernel quantizes it as before.
+constexpr int SG_LOW = 10, SG_REGS = 8, SG_WARPS = 4, SG_PF = 4;   // SG_PF: rows read ahead
+constexpr int SG_MIN_N = SG_LOW + 2;
+
+struct StreamGroupArgs {
+    int lmin, lmax;
+    ull cum[SG_LOW + 2];       // groups before low popcount lmin + i
+    int loff[SG_LOW + 2];      // first index of popcount l in the low-mask order
+    const int4 *rows;          // {menu >> SG_LOW, menu & (2^SG_LOW - 1), score bits, -}
+    const uint16_t *lowtab;    // [0, 2^SG_LOW): low masks by (popcount, value); then each mask's rank
+};
+
+// One group's slots, NR registers per lane (NR * 32 >= the group's C(SG_LOW, l) slots).
+template <int NR>
+__device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupArgs &G, float *vals, const ull *sbin,
+                                         const uint16_t *sord, const uint16_t *srk, int lane, int l, unsigned H,
+                                         ull base, ull tsum, int nsl) {
+    const int n = A.n;
+    unsigned Lj[NR], nLj[NR];
+    float best[NR];
+    int bx[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        const int sl = lane + 32 * j;
+        Lj[j] = sl < nsl ? (unsigned)sord[G.loff[l] + sl] : 0u;
+        nLj[j] = ~Lj[j];
+        best[j] = 0.0f;
+        bx[j] = -1;
+    }
+    const unsigned nH = ~H;
+    ull pre = 0, cle = 0;                                 // sums over the elements of H below x
+    int ih = 0;
+    for (int x = 0; x < n; ++x) {
+        const bool high = x >= SG_LOW;
+        ull hbase = 0;
+        if (high) {
+            if (!((H >> (x - SG_LOW)) & 1u)) continue;    // uniform per warp
+            const ull c1 = sbin[x * (n + 1) + l + ih + 1], c0 = sbin[x * (n + 1) + l + ih];
+            hbase = pre + (tsum - cle - c0);              // base(H \ {x}, l)
+            pre += c1;
+            cle += c0;
+            ++ih;
+        }
+        float prev[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            const int sl = lane + 32 * j;
+            const bool use = sl < nsl && (high || ((Lj[j] >> x) & 1u));
+            const ull rp = high ? hbase + (ull)sl : tsum + (ull)srk[Lj[j] ^ (1u << x)];
+            prev[j] = use ? decode_prev(A, rp) : 0.0f;
+        }
+        float acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = 0.0f;
+        const int lo = (int)A.offsets[x], hi = (int)A.offsets[x + 1];
+        for (int i0 = lo; i0 < hi; i0 += SG_PF) {
+            int4 R[SG_PF];
+#pragma unroll
+            for (int u = 0; u < SG_PF; ++u) R[u] = i0 + u < hi ? __ldg(G.rows + i0 + u) : ROW_NONE;
+#pragma unroll
+            for (int u = 0; u < SG_PF; ++u) {
+                if ((unsigned)R[u].x & nH) continue;            // uniform: fails for the whole group
+                const unsigned ml = (unsigned)R[u].y;
+                const float sc = __int_as_float(R[u].z);
+                if (ml == 0u) {                                 // uniform: a menu within H fits every slot
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) acc[j] = __fadd_rn(acc[j], sc);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NR; ++j)
+                        if (!(ml & nLj[j])) acc[j] = __fadd_rn(acc[j], sc);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            const int sl = lane + 32 * j;
+            if (sl < nsl && (high || ((Lj[j] >> x) & 1u))) mt_merge(best[j], bx[j], __fadd_rn(prev[j], acc[j]), x);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        const int sl = lane + 32 * j;
+        if (sl >= nsl) continue;
+        const ull r = base + (ull)sl;
+        if (A.pred) A.pred[r] = (uint8_t)bx[j];
+        if (A.mode == 1) A.vcur_f[r] = best[j];
+        else vals[r] = best[j];
+    }
+}
+
+__global__ void __launch_bounds__(32 * SG_WARPS) stream_group_kernel(PricerArgs A, StreamGroupArgs G, float *vals) {
+    __shared__ ull sbin[BIN_MAX];
+    __shared__ uint16_t sord[1 << SG_LOW], srk[1 << SG_LOW];
+    const int n = A.n, k = A.k, hb = n - SG_LOW;
+    stage_binom(sbin, A.binom, n);
+    for (int i = threadIdx.x; i < (1 << SG_LOW); i += blockDim.x) {
+        sord[i] = G.lowtab[i];
+        srk[i] = G.lowtab[(1 << SG_LOW) + i];
+    }
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const ull g = (ull)blockIdx.x * SG_WARPS + w;
+    if (g >= G.cum[G.lmax - G.lmin + 1]) return;          // whole warps leave
+    int l = G.lmin;
+    while (g >= G.cum[l - G.lmin + 1]) ++l;
+    const int t = k - l;
+    unsigned H = 0;                                       // colex unranking among the t-subsets of [0, hb)
+    {
+        ull r = g - G.cum[l - G.lmin];
+        int b = hb - 1;
+        for (int kk = t; kk >= 1; --kk) {
+            while (sbin[b * (n + 1) + kk] > r) --b;
+            H |= 1u << b;
+            r -= sbin[b * (n + 1) + kk];
+            --b;
+        }
+    }
+    ull base = 0, tsum = 0;                               // base(H, l) and base(H, l - 1)
+    {
+        int i = 0;
+        for (unsigned m = H; m; m &= m - 1u, ++i) {
+            const int a = SG_LOW + __ffs((int)m) - 1;
+            base += sbin[a * (n + 1) + l + i + 1];
+            tsum += sbin[a * (n + 1) + l + i];
+        }
+    }
+    const int nsl = (int)sbin[SG_LOW * (n + 1) + l];
+    if (nsl <= 32) sg_group<1>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    else if (nsl <= 64) sg_group<2>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    else if (nsl <= 128) sg_group<4>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    else sg_group<SG_REGS>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+}
+
 // ----------------------------------------------------------------- host object
 struct Pricer {
     Ctx *c = nullptr;
@@ -575,7 +946,21 @@ struct Pricer {
     DevBuf lbase_dev, loffs, lent;
     std::vector<char> wide;                 // per layer: layer_wide_kernel (1) or layer_eval_kernel (0)
     DevBuf d64[2], s64;                     // the float64 max sweep's two layers and scores (on first use)
+    // mask storage: the tile sweep (mask_tile_kernel) or the layer kernels over the layer table
+    bool by_mask = false;                   // the lattice is stored by mask (mask storage, or float32 routed)
+    bool mask_tile = false;
+    DevBuf rows;                            // row records of the tile and group sweeps (int4 per row)
+    // stream storage: the group sweep (stream_group_kernel) or the layer kernels
+    bool stream_group = false;
+    DevBuf lowtab;                          // the group sweep's low-mask order and ranks (uint16)
+    // sub-lattices solved by the tile sweep (k_pred >= SUB_TILE_MIN)
+    std::vector<ull> host_menus;
+    DevBuf sub_menus, sub_idx, sub_offsets, sub_rows;
 };
+
+// The sub-lattice left by the descent is solved by the tile sweep from this many elements on (one
+// CTA below it).
+constexpr int SUB_TILE_MIN = 12;
 
 // Mean cover-list length from which a layer runs layer_wide_kernel (measured at n = 18: a mean of
 // 82 entries takes 68 us with a thread per pair and 13 us with a warp per pair; 41 entries, 41 and
@@ -655,13 +1040,165 @@ static void build_cover_lists(Pricer &P, const uint64_t *menus_host) {
     }
 }
 
+static void run_sweep(Pricer *P, const float *scores);
+
+// One tile sweep over an n-element lattice whose x-major rows are menus[0..mp) (offsets[n+1] on the
+// device, idx: each record's score index or NULL), into V and pred (2^n entries each).
+static void tile_sweep(cudaStream_t st, int n, ll mp, const ull *menus, const float *scores, const int *idx,
+                       const ll *offsets, const ull *binom, int bstride, int4 *rows, float *V, uint8_t *pred) {
+    static const MtOrder order = mt_order_host();
+    if (mp) {
+        rows_kernel<<<grid_for(mp, 256), 256, 0, st>>>(mp, menus, scores, idx, MT_LOW, 31u, rows);
+        RUMB_LAUNCH("rows_kernel");
+    }
+    const int h = n - MT_LOW;
+    std::vector<ull> bt = binom_host(h);
+    for (int t = 0; t <= h; ++t) {
+        MaskTileArgs A{};
+        A.n = n;
+        A.h = h;
+        A.t = t;
+        A.count = bt[h * (h + 1) + t];
+        A.binom = binom;
+        A.bstride = bstride;
+        A.rows = rows;
+        A.offsets = offsets;
+        A.V = V;
+        A.P = pred;
+        mask_tile_kernel<<<(unsigned)((A.count + MT_WARPS - 1) / MT_WARPS), 32 * MT_WARPS, 0, st>>>(A, order);
+        RUMB_LAUNCH("mask_tile_kernel");
+    }
+}
+
+// After a descend-only backtrace: the rows of the K elements left whose menus lie within the node
+// (in their order, relabelled to the node's elements, as the reference's sub-problem builds them),
+// solved by a tile sweep, and the ranking completed from its predecessors.
+static void sublattice_tile(Pricer &P, const float *scores) {
+    cudaStream_t st = P.c->own;
+    PriceOut h;
+    RUMB_CUDA(cudaMemcpyAsync(&h, P.out.ptr, sizeof(PriceOut), cudaMemcpyDeviceToHost, st));
+    RUMB_CUDA(cudaStreamSynchronize(st));
+    const ull node = h.node;
+    SubElems el{};
+    int K = 0;
+    for (int b = 0; b < P.n; ++b)
+        if ((node >> b) & 1ULL) el.e[K++] = b;
+    std::vector<ull> sm;
+    std::vector<int> si;
+    std::vector<ll> so(K + 1, 0);
+    for (int j = 0; j < K; ++j) {
+        const int x = el.e[j];
+        for (ll i = P.host_offsets[x]; i < P.host_offsets[x + 1]; ++i) {
+            const ull m = P.host_menus[i];
+            if (m & ~node) continue;
+            ull c = 0;
+            for (int q = 0; q < K; ++q) c |= ((m >> el.e[q]) & 1ULL) << q;
+            sm.push_back(c);
+            si.push_back((int)i);
+        }
+        so[j + 1] = (ll)sm.size();
+    }
+    const ll smp = (ll)sm.size();
+    P.sub_menus.ensure((size_t)std::max<ll>(smp, 1) * 8);
+    P.sub_idx.ensure((size_t)std::max<ll>(smp, 1) * 4);
+    P.sub_offsets.ensure((size_t)(K + 1) * 8);
+    P.sub_rows.ensure((size_t)std::max<ll>(smp, 1) * sizeof(int4));
+    if (smp) {
+        RUMB_CUDA(cudaMemcpyAsync(P.sub_menus.ptr, sm.data(), (size_t)smp * 8, cudaMemcpyHostToDevice, st));
+        RUMB_CUDA(cudaMemcpyAsync(P.sub_idx.ptr, si.data(), (size_t)smp * 4, cudaMemcpyHostToDevice, st));
+    }
+    RUMB_CUDA(cudaMemcpyAsync(P.sub_offsets.ptr, so.data(), (size_t)(K + 1) * 8, cudaMemcpyHostToDevice, st));
+    tile_sweep(st, K, smp, P.sub_menus.as<ull>(), scores, P.sub_idx.as<int>(), P.sub_offsets.as<ll>(),
+               P.binom.as<ull>(), P.n + 1, P.sub_rows.as<int4>(), P.Vs.as<float>(), P.Ps.as<uint8_t>());
+    sub_readout_kernel<<<1, 32, 0, st>>>(K, P.Vs.as<float>(), P.Ps.as<uint8_t>(), el, P.mode, P.out.as<PriceOut>());
+    RUMB_LAUNCH("sub_readout_kernel");
+    // the sub-problem's buffers go back to the stream before the host vectors above are freed
+    RUMB_CUDA(cudaStreamSynchronize(st));
+}
+
+// Times one sweep in each of two forms (the form flag set by `set`) and keeps the faster; both give
+// the same bits.
+template <class F>
+static bool faster_second(Pricer &P, F set) {
+    cudaStream_t st = P.c->own;
+    if (P.mp) RUMB_CUDA(cudaMemsetAsync(P.scores.ptr, 0, (size_t)P.mp * 4, st));
+    cudaEvent_t e[2];
+    for (auto &ev : e) RUMB_CUDA(cudaEventCreate(&ev));
+    float ms[2] = {0.0f, 0.0f};
+    for (int f = 0; f < 2; ++f) {
+        set(f == 1);
+        run_sweep(&P, P.scores.as<float>());                 // warm (the layer table is built once)
+        RUMB_CUDA(cudaEventRecord(e[0], st));
+        run_sweep(&P, P.scores.as<float>());
+        RUMB_CUDA(cudaEventRecord(e[1], st));
+        RUMB_CUDA(cudaEventSynchronize(e[1]));
+        RUMB_CUDA(cudaEventElapsedTime(&ms[f], e[0], e[1]));
+    }
+    for (auto &ev : e) cudaEventDestroy(ev);
+    return ms[1] <= ms[0];
+}
+
+// Mask storage: the tile sweep from n = 9 on (the layer kernels below that, and above n = 30 the
+// layer table would not fit). Where both run and the cover lists were built (n <= 26), one sweep of
+// each on zero scores picks the faster (both give the same bits); without the lists the tile sweep
+// is taken. RUMB_MASK_FORM = "tile" or "layer" pins the form where it can run.
+static void choose_mask_form(Pricer &P) {
+    const int n = P.n;
+    const bool tile_ok = n >= MASK_MIN_N_TILE, layer_ok = n <= 30;
+    if (tile_ok) P.rows.ensure((size_t)std::max<ll>(P.mp, 1) * sizeof(int4));
+    const char *env = getenv("RUMB_MASK_FORM");
+    if (env && std::strcmp(env, "tile") == 0 && tile_ok) { P.mask_tile = true; return; }
+    if (env && std::strcmp(env, "layer") == 0 && layer_ok) { P.mask_tile = false; return; }
+    if (!tile_ok || !layer_ok) { P.mask_tile = tile_ok; return; }
+    if (P.wmode == W_SCAN) { P.mask_tile = true; return; }
+    P.mask_tile = faster_second(P, [&](bool second) { P.mask_tile = second; });
+}
+
+// Stream storage: the group sweep from n = 12 on. Without cover lists it is taken; with them one
+// sweep of each form on zero scores picks the faster. RUMB_STREAM_FORM = "group" or "layer" pins
+// the form where it can run.
+static void choose_stream_form(Pricer &P) {
+    const int n = P.n;
+    const bool group_ok = n >= SG_MIN_N;
+    if (group_ok) {
+        P.rows.ensure((size_t)std::max<ll>(P.mp, 1) * sizeof(int4));
+        std::vector<uint16_t> tab(2 << SG_LOW);
+        int k = 0;
+        std::vector<int> rk(SG_LOW + 1, 0);
+        for (int q = 0; q <= SG_LOW; ++q)
+            for (int L = 0; L < (1 << SG_LOW); ++L)
+                if (__builtin_popcount(L) == q) {
+                    tab[k++] = (uint16_t)L;
+                    tab[(1 << SG_LOW) + L] = (uint16_t)rk[q]++;
+                }
+        P.lowtab.ensure(tab.size() * 2);
+        RUMB_CUDA(cudaMemcpy(P.lowtab.ptr, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
+    }
+    const char *env = getenv("RUMB_STREAM_FORM");
+    if (env && std::strcmp(env, "group") == 0 && group_ok) { P.stream_group = true; return; }
+    if (env && std::strcmp(env, "layer") == 0) { P.stream_group = false; return; }
+    if (!group_ok) { P.stream_group = false; return; }
+    if (P.wmode == W_SCAN) { P.stream_group = true; return; }
+    P.stream_group = faster_second(P, [&](bool second) { P.stream_group = second; });
+}
+
+// Float32 storage keeps the same float32 value for every subset whether it is stored by colex rank
+// (two live layers) or by mask, and the readout from the full set walks the same predecessors as
+// the layer descent and sub-lattice DP, so the priced value and ranking are the same bits. The
+// float32 pricer therefore stores the lattice by mask and runs the tile sweep when 5 * 2^n bytes
+// are at most half the free device memory (n <= 34), unless RUMB_PRICE_STREAM asks for the
+// two-layer storage.
+static bool f32_by_mask(int n, size_t free_b) {
+    return n >= MASK_MIN_N_TILE && n <= MASK_MAX_N && std::ldexp(5.0, n) <= 0.5 * (double)free_b;
+}
+
 Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t *offsets, int mode, int k_pred,
                       int fma_decode) {
-    const bool scan = (mode & RUMB_PRICE_SCAN) != 0;
-    mode &= ~RUMB_PRICE_SCAN;
+    const bool scan = (mode & RUMB_PRICE_SCAN) != 0, keep_stream = (mode & RUMB_PRICE_STREAM) != 0;
+    mode &= ~(RUMB_PRICE_SCAN | RUMB_PRICE_STREAM);
     if (mode < 0 || mode > 3) fail(RUMB_E_INVAL, "pricer mode must be 0 (mask), 1 (f32), 2 (u16) or 3 (u24)");
     if (n < 1 || n > 39) fail(RUMB_E_INVAL, "pricing handles 1 <= n <= 39");
-    if (mode == 0 && n > 30) fail(RUMB_E_INVAL, "mask pricing handles n <= 30");
+    if (mode == 0 && n > MASK_MAX_N) fail(RUMB_E_INVAL, "mask pricing handles n <= 34");
     if (mp < 0 || (mp > 0 && !menus) || !offsets) fail(RUMB_E_INVAL, "menus / offsets must not be NULL");
     std::vector<ll> off(offsets, offsets + n + 1);
     if (off[0] != 0 || off[n] != mp) fail(RUMB_E_INVAL, "offsets must run from 0 to mp");
@@ -679,7 +1216,6 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
     P->fma_decode = fma_decode ? 1 : 0;
     int kp = k_pred > 0 ? k_pred : n - 10;
     P->k_pred = kp < 1 ? 1 : (kp > n ? n : kp);
-    if (mode != 0 && P->k_pred > 22) fail(RUMB_E_INVAL, "k_pred > 22 needs a sub-lattice larger than this pricer keeps");
     P->host_offsets = off;
     std::vector<ull> bt = binom_host(n);
     for (int k = 0; k <= n; ++k) P->counts.push_back(bt[n * (n + 1) + k]);
@@ -693,11 +1229,17 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
     RUMB_CUDA(cudaMemcpyAsync(P->binom.ptr, bt.data(), bt.size() * 8, cudaMemcpyHostToDevice, st));
     P->out.ensure(sizeof(PriceOut));
     P->layer_step.ensure((size_t)(n + 1) * 4);
-    if (mode == 0) {
+    size_t free_b = 0, total_b = 0;
+    RUMB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    P->by_mask = mode == 0 || (mode == 1 && !keep_stream && f32_by_mask(n, free_b));
+    if (P->by_mask) {
         ull N = 1ULL << n;
+        if ((double)N * 5.0 > 0.9 * (double)free_b)
+            fail(RUMB_E_OOM, "mask pricing needs 5 * 2^n bytes of device memory");
         P->Vs.ensure((size_t)N * 4);
         P->Ps.ensure((size_t)N);
     } else {
+        if (P->k_pred > MASK_MAX_N) fail(RUMB_E_INVAL, "k_pred must be <= 34");
         ull cap = 0;
         for (ull v : P->counts) cap = v > cap ? v : cap;
         ull nblk = (cap + PB - 1) / PB;
@@ -721,11 +1263,14 @@ Pricer *pricer_create(Ctx &c, int n, ll mp, const uint64_t *menus, const int64_t
         ull Nsub = 1ULL << P->k_pred;
         P->Vs.ensure((size_t)Nsub * 4);
         P->Ps.ensure((size_t)Nsub);
-        P->Ws.ensure((size_t)Nsub * P->k_pred * 4);
+        if (P->k_pred < SUB_TILE_MIN) P->Ws.ensure((size_t)Nsub * P->k_pred * 4);
+        else P->host_menus.assign(menus, menus + mp);
     }
     RUMB_CUDA(cudaStreamSynchronize(st));
     P->wide.assign(n + 1, 0);
     if (!scan) build_cover_lists(*P, menus);
+    if (P->by_mask) choose_mask_form(*P);
+    else choose_stream_form(*P);
     return P.release();
 }
 
@@ -834,7 +1379,12 @@ static void run_sweep(Pricer *P, const float *scores) {
     };
     const unsigned *loffs = P->loffs.as<unsigned>();
     const ull *lbase = P->lbase_dev.as<ull>();
-    if (P->mode == 0) {
+    if (P->by_mask && P->mask_tile) {
+        tile_sweep(st, n, P->mp, menus, scores, nullptr, offs, P->binom.as<ull>(), n + 1, P->rows.as<int4>(),
+                   P->Vs.as<float>(), P->Ps.as<uint8_t>());
+        mask_readout_kernel<<<1, 32, 0, st>>>(n, P->Vs.as<float>(), P->Ps.as<uint8_t>(), P->out.as<PriceOut>());
+        RUMB_LAUNCH("mask_readout_kernel");
+    } else if (P->by_mask) {
         RUMB_CUDA(cudaMemsetAsync(P->Vs.ptr, 0, ((size_t)1 << n) * 4, st));
         RUMB_CUDA(cudaMemsetAsync(P->Ps.ptr, 0, (size_t)1 << n, st));
         std::vector<ll> bounds;
@@ -855,6 +1405,16 @@ static void run_sweep(Pricer *P, const float *scores) {
         if (P->mode == 3) RUMB_CUDA(cudaMemsetAsync(P->l[prev].ptr, 0, 1, st));
         RUMB_CUDA(cudaMemsetAsync(P->m[prev].ptr, 0, 4, st));
         RUMB_CUDA(cudaMemsetAsync(P->e[prev].ptr, 0, 4, st));
+        std::vector<ull> bh, b10;
+        if (P->stream_group) {
+            b10 = binom_host(SG_LOW);
+            if (P->mp) {
+                rows_kernel<<<grid_for(P->mp, 256), 256, 0, st>>>(P->mp, menus, scores, nullptr, SG_LOW,
+                                                                  (1u << SG_LOW) - 1u, P->rows.as<int4>());
+                RUMB_LAUNCH("rows_kernel");
+            }
+            bh = binom_host(n - SG_LOW);
+        }
         for (int k = 1; k <= n; ++k) {
             PricerArgs A = args(k);
             A.vprev_f = P->v[prev].as<float>();
@@ -869,7 +1429,25 @@ static void run_sweep(Pricer *P, const float *scores) {
             A.ecur = P->e[cur].as<float>();
             A.pred = k >= P->k_pred ? P->pred[k]->as<uint8_t>() : nullptr;
             A.layer_step = P->layer_step.as<unsigned int>() + k;
-            layer(A, false, P->vals.as<float>());
+            if (P->stream_group) {
+                const int hb = n - SG_LOW;
+                StreamGroupArgs G{};
+                G.lmin = std::max(0, k - hb);
+                G.lmax = std::min(SG_LOW, k);
+                for (int l = G.lmin; l <= G.lmax; ++l) G.cum[l - G.lmin + 1] = G.cum[l - G.lmin] + bh[hb * (hb + 1) + (k - l)];
+                for (int l = 0, o = 0; l <= SG_LOW; ++l) {
+                    G.loff[l] = o;
+                    o += (int)b10[SG_LOW * (SG_LOW + 1) + l];
+                }
+                G.rows = P->rows.as<int4>();
+                G.lowtab = P->lowtab.as<uint16_t>();
+                const ull groups = G.cum[G.lmax - G.lmin + 1];
+                stream_group_kernel<<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
+                    A, G, P->vals.as<float>());
+                RUMB_LAUNCH("stream_group_kernel");
+            } else {
+                layer(A, false, P->vals.as<float>());
+            }
             if (A.mode != 1) {
                 stream_quant_kernel<<<(unsigned)((A.count + PB - 1) / PB), PB, 0, st>>>(A, P->vals.as<float>());
                 RUMB_LAUNCH("stream_quant_kernel");
@@ -880,8 +1458,10 @@ static void run_sweep(Pricer *P, const float *scores) {
                                              scores, offs, P->Vs.as<float>(), P->Ps.as<uint8_t>(),
                                              P->out.as<PriceOut>(), P->v[prev].as<float>(), P->v[prev].as<uint16_t>(),
                                              P->l[prev].as<uint8_t>(), P->m[prev].as<float>(), P->e[prev].as<float>(),
-                                             P->mode, P->wmode, loffs, P->lent.ptr, lbase, P->Ws.as<float>());
+                                             P->mode, P->wmode, loffs, P->lent.ptr, lbase, P->Ws.as<float>(),
+                                             P->k_pred >= SUB_TILE_MIN ? 1 : 0);
         RUMB_LAUNCH("backtrace_kernel");
+        if (P->k_pred >= SUB_TILE_MIN) sublattice_tile(*P, scores);
     }
 }
 

@@ -375,6 +375,7 @@ class Context:
 
 PRICE_MODES = {"mask": 0, "f32": 1, "u16": 2, "u24": 3}
 PRICE_SCAN = 16
+PRICE_STREAM = 32
 
 
 def to_bf16_bits(x):
@@ -559,12 +560,14 @@ class DrawRows:
 class Pricer:
     """Flow-CG pricer on one GPU (rows in x-major order; see rumb_cg_pricer_create)."""
 
-    def __init__(self, ctx, n, menus, offsets, mode="u24", k_pred=None, fma_decode=True, lists=True):
-        """lists=False: scan x's rows in every sweep instead of walking the cover lists."""
+    def __init__(self, ctx, n, menus, offsets, mode="u24", k_pred=None, fma_decode=True, lists=True, stream=False):
+        """lists=False: scan x's rows in every sweep instead of walking the cover lists.
+        stream=True (float32 storage): keep the two rank-indexed layers even when the lattice would
+        fit by mask."""
         menus = np.ascontiguousarray(menus, dtype=np.uint64)
         offsets = np.ascontiguousarray(offsets, dtype=np.int64)
         h = ctypes.c_void_p()
-        code = PRICE_MODES[mode] | (0 if lists else PRICE_SCAN)
+        code = PRICE_MODES[mode] | (0 if lists else PRICE_SCAN) | (PRICE_STREAM if stream else 0)
         check(load().rumb_cg_pricer_create(ctx.h, int(n), menus.size, _p(menus), _p(offsets), code,
                                            0 if k_pred is None else int(k_pred), int(bool(fma_decode)),
                                            ctypes.byref(h)))

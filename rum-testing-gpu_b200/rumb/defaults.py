@@ -26,7 +26,7 @@ METHOD_ARGS = {
     ),
     "flow_cg": dict(
         dtype="auto",           # pricing values "float32", "uint24" or "uint16"; auto = the first that fits
-        pricing="auto",         # "mask" (one value per subset, n <= 30) or "stream" (two live layers)
+        pricing="auto",         # "mask" (one value per subset, n <= 34) or "stream" (two live layers)
         layers="auto",          # accepted for compatibility; the lattice layers are implicit here
         max_iters=4000,         # columns
     ),

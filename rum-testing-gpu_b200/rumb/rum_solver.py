@@ -479,14 +479,14 @@ def _plan_flow_cg(n, mp, a):
     budget = defaults.AUTO["gpu_memory_fraction"] * gpu_free_bytes()
     tried = []
     for (lay, d), engine in _CG_ENGINE.items():
-        if layout not in ("auto", lay) or dt not in ("auto", d) or (lay == "mask" and n > 30):
+        if layout not in ("auto", lay) or dt not in ("auto", d) or (lay == "mask" and n > 34):
             continue
         need = _flow_cg_bytes(n, engine)
         if need <= budget:
             a.update(pricing=lay, dtype=d, _engine=engine, _gpu_bytes=need)
             return a
         tried.append("%s %s %.1f GB" % (lay, d, need / 2 ** 30))
-    raise RuntimeError("flow_cg at n = %d does not fit the GPU (%s)" % (n, "; ".join(tried) or "mask needs n <= 30"))
+    raise RuntimeError("flow_cg at n = %d does not fit the GPU (%s)" % (n, "; ".join(tried) or "mask needs n <= 34"))
 
 
 _PLAN = {"bm_admm": _plan_bm_admm, "flow_cg": _plan_flow_cg}

@@ -27,10 +27,13 @@ CASES = list(_cases())
 
 
 @pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("mode", ["mask", "f32", "u16", "u24"])
+@pytest.mark.parametrize("mode", ["mask", "f32", "f32_stream", "u16", "u24"])
 def test_pricer_bit_exact_against_oracle(ctx, name, cd, n, mode):
+    """f32 stores the lattice by mask where it fits; f32_stream keeps the two rank-indexed layers."""
     menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
-    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+    stream = mode == "f32_stream"
+    mode = "f32" if stream else mode
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode, stream=stream)
     rng = np.random.RandomState(7)
     trials = 2 if n >= 16 else 3
     for trial in range(trials):
@@ -64,9 +67,9 @@ def test_cover_lists_equal_row_scan(ctx, name, cd, n):
     rng = np.random.RandomState(11)
     scores = [rng.randn(menus.size).astype(np.float32), (p32 - p32.mean()).astype(np.float32),
               np.round(rng.randn(menus.size) * 4).astype(np.float32)]       # many exact ties
-    for mode in ("mask", "f32", "u16", "u24"):
-        a = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
-        b = _lib.Pricer(ctx, n, menus, offsets, mode=mode, lists=False)
+    for mode, stream in (("mask", False), ("f32", False), ("f32", True), ("u16", False), ("u24", False)):
+        a = _lib.Pricer(ctx, n, menus, offsets, mode=mode, stream=stream)
+        b = _lib.Pricer(ctx, n, menus, offsets, mode=mode, lists=False, stream=stream)
         assert a.list_entries == _cover_entries(menus, n) and b.list_entries == -1
         for s in scores:
             va, ra, ma, sa = a.price(s, want_steps=True)
@@ -171,7 +174,7 @@ def test_mask_and_f32_stream_identical(ctx):
     cd, mp = PI.gen_medium(14, mult=4)
     menus, alts, p32, offsets, _ = O.cg_layout(14, cd[:, 0], cd[:, 1], cd[:, 2])
     a = _lib.Pricer(ctx, 14, menus, offsets, mode="mask")
-    b = _lib.Pricer(ctx, 14, menus, offsets, mode="f32", k_pred=6)
+    b = _lib.Pricer(ctx, 14, menus, offsets, mode="f32", k_pred=6, stream=True)
     rng = np.random.RandomState(3)
     for _ in range(4):
         s = rng.randn(menus.size).astype(np.float32)
@@ -280,8 +283,10 @@ def test_pricer_matches_recorded_reference_kernels(ctx):
     g = np.load(_REPLAY)
     for name, n, m, a, p in MR.cases():
         menus, alts, p32, offsets, _ = O.cg_layout(n, m, a, p)
-        for mode in ("f32", "u16", "u24") + (("mask",) if n <= 16 else ()):
-            pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+        for mode in ("f32", "f32_stream", "u16", "u24") + (("mask",) if n <= 16 else ()):
+            stream = mode == "f32_stream"
+            mode = "f32" if stream else mode
+            pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode, stream=stream)
             for trial in range(2):
                 key = "%s_t%d" % (name, trial)
                 s = g[key + "_scores"]
@@ -318,18 +323,151 @@ def test_config3_column_sequence_matches_recorded_reference(ctx, mode):
     assert [res["lb"], res["distance"]] == g["bracket_" + mode].tolist()
 
 
-def test_mask_pricer_at_n28_equals_float32_stream(ctx):
+def _mask_pricer(ctx, monkeypatch, form, n, menus, offsets, **kw):
+    monkeypatch.setenv("RUMB_MASK_FORM", form)
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode="mask", **kw)
+    monkeypatch.delenv("RUMB_MASK_FORM")
+    return pr
+
+
+MASK_CASES = [c for c in CASES if c[2] >= 9]
+
+
+@pytest.mark.parametrize("name,cd,n", MASK_CASES, ids=[c[0] for c in MASK_CASES])
+@pytest.mark.parametrize("lists", [True, False], ids=["lists", "scan"])
+def test_mask_tile_sweep_bit_exact(ctx, monkeypatch, name, cd, n, lists):
+    """The tile sweep of the mask storage (one warp per 256 masks, launches by the popcount of the
+    high part) against the oracle and against the layer kernels: value and ranking bit for bit on
+    random, tie-heavy (integer) and residual-like scores."""
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    pt = _mask_pricer(ctx, monkeypatch, "tile", n, menus, offsets, lists=lists)
+    pl = _mask_pricer(ctx, monkeypatch, "layer", n, menus, offsets, lists=lists)
+    rng = np.random.RandomState(17)
+    for scores in (rng.randn(menus.size).astype(np.float32),
+                   np.round(rng.randn(menus.size) * 3).astype(np.float32),
+                   (p32 - p32.mean()).astype(np.float32)):
+        v_ref, r_ref = O.price_mask(n, menus, scores, offsets)
+        for pr in (pt, pl):
+            v, r, m = pr.price(scores)
+            assert v == v_ref and m == 0.0
+            np.testing.assert_array_equal(r, r_ref)
+    pt.close()
+    pl.close()
+
+
+def test_mask_pricer_at_n28_equals_float32_stream(ctx, monkeypatch):
     """The mask pricer at n = 28 (2^28 float32 values, 1 GiB) gives the float32 stream pricer's
     value and ranking bit for bit (the reference's own check, validation/feasibility/
-    test_stream_pricer.py:56-84, at the large-n end)."""
+    test_stream_pricer.py:56-84, at the large-n end), in both mask forms."""
     n = 28
     cd, _ = PI.gen_pairwise(n)
     menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
     scores = (np.random.RandomState(29).randn(menus.size)).astype(np.float32)
-    pm = _lib.Pricer(ctx, n, menus, offsets, mode="mask")
-    ps = _lib.Pricer(ctx, n, menus, offsets, mode="f32")
-    vm, rm, _ = pm.price(scores)
+    pt = _mask_pricer(ctx, monkeypatch, "tile", n, menus, offsets)
+    pl = _mask_pricer(ctx, monkeypatch, "layer", n, menus, offsets)
+    ps = _lib.Pricer(ctx, n, menus, offsets, mode="f32", stream=True)
     vs, rs, _ = ps.price(scores)
-    assert vm == vs and np.array_equal(rm, rs)
-    pm.close()
+    for pm in (pt, pl):
+        vm, rm, _ = pm.price(scores)
+        assert vm == vs and np.array_equal(rm, rs)
+        pm.close()
     ps.close()
+
+
+def test_mask_pricer_at_n32_equals_float32_stream(ctx):
+    """Mask storage at n = 32 (2^32 values: 16 GiB of float32 and 4 GiB of predecessors, the tile
+    sweep) against the float32 stream pricer on the pairwise instance."""
+    n = 32
+    cd, _ = PI.gen_pairwise(n)
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    scores = (np.random.RandomState(32).randn(menus.size)).astype(np.float32)
+    pm = _lib.Pricer(ctx, n, menus, offsets, mode="mask")
+    vm, rm, _ = pm.price(scores)
+    pm.close()
+    ps = _lib.Pricer(ctx, n, menus, offsets, mode="f32", stream=True)
+    vs, rs, _ = ps.price(scores)
+    ps.close()
+    assert vm == vs and np.array_equal(rm, rs)
+
+
+STREAM_CASES = [c for c in CASES if c[2] >= 12]
+
+
+def _stream_pricer(ctx, monkeypatch, form, n, menus, offsets, mode, **kw):
+    monkeypatch.setenv("RUMB_STREAM_FORM", form)
+    stream = mode == "f32_stream"
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode="f32" if stream else mode, stream=stream, **kw)
+    monkeypatch.delenv("RUMB_STREAM_FORM")
+    return pr
+
+
+@pytest.mark.parametrize("name,cd,n", STREAM_CASES, ids=[c[0] for c in STREAM_CASES])
+@pytest.mark.parametrize("mode", ["f32_stream", "u16", "u24"])
+def test_stream_group_sweep_bit_exact(ctx, monkeypatch, name, cd, n, mode):
+    """The group sweep of the rank-indexed storage (one warp per set of subsets sharing their
+    elements >= 10) against the oracle and the layer kernels: value, ranking, per-layer steps and
+    margin bit for bit, with cover lists and with rows scanned."""
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    omode = "f32" if mode == "f32_stream" else mode
+    rng = np.random.RandomState(23)
+    scores = [rng.randn(menus.size).astype(np.float32), np.round(rng.randn(menus.size) * 3).astype(np.float32),
+              (p32 - p32.mean()).astype(np.float32)]
+    for lists in (True, False):
+        pg = _stream_pricer(ctx, monkeypatch, "group", n, menus, offsets, mode, lists=lists)
+        pl = _stream_pricer(ctx, monkeypatch, "layer", n, menus, offsets, mode, lists=lists)
+        for s in scores:
+            v_ref, r_ref, m_ref, steps_ref = O.price_stream(n, menus, s, offsets, mode=omode)
+            for pr in (pg, pl):
+                v, r, m, steps = pr.price(s, want_steps=True)
+                assert v == v_ref, (lists, v, v_ref)
+                np.testing.assert_array_equal(r, r_ref)
+                np.testing.assert_array_equal(steps, steps_ref)
+                assert m == m_ref
+        pg.close()
+        pl.close()
+
+
+@pytest.mark.parametrize("mode", ["f32_stream", "u16", "u24"])
+def test_sublattice_by_tile_sweep(ctx, mode):
+    """Sub-lattices of 12 elements and more (k_pred >= 12) are solved by a tile sweep over the
+    restricted rows; the value and ranking equal the oracle's with the same k_pred. In float32
+    storage the ranking is also the one of the default k_pred (whose sub-lattice one CTA solves);
+    quantized storages descend through predecessors chosen on decoded values, so theirs may move
+    with k_pred."""
+    omode = "f32" if mode == "f32_stream" else mode
+    for name, cd, n in [c for c in CASES if c[2] >= 16]:
+        menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+        s = np.random.RandomState(n).randn(menus.size).astype(np.float32)
+        v0, r0, m0 = _lib.Pricer(ctx, n, menus, offsets, mode=omode, stream=True).price(s)
+        for kp in (12, 14, n - 1):
+            pr = _lib.Pricer(ctx, n, menus, offsets, mode=omode, stream=True, k_pred=kp)
+            v_ref, r_ref, m_ref, _ = O.price_stream(n, menus, s, offsets, mode=omode, k_pred=kp)
+            v, r, m = pr.price(s)
+            pr.close()
+            assert v == v_ref == v0 and m == m_ref
+            np.testing.assert_array_equal(r, r_ref)
+            if omode == "f32":
+                np.testing.assert_array_equal(r, r0)
+
+
+def test_stream_pricers_at_n33(ctx):
+    """n = 33 (pairwise): the float32 stream (two rank-indexed layers, 9 GB; its 23-element
+    sub-lattice by the tile sweep) equals the mask storage (40 GB) bit for bit, and the uint16
+    stream's value lies within its margin of the exact one (validation/feasibility/
+    test_stream_pricer.py:56-84)."""
+    n = 33
+    cd, _ = PI.gen_pairwise(n)
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    scores = (np.random.RandomState(33).randn(menus.size)).astype(np.float32)
+    pm = _lib.Pricer(ctx, n, menus, offsets, mode="mask")
+    vm, rm, _ = pm.price(scores)
+    pm.close()
+    ps = _lib.Pricer(ctx, n, menus, offsets, mode="f32", stream=True)
+    vs, rs, _ = ps.price(scores)
+    ps.close()
+    assert vm == vs and np.array_equal(rm, rs)
+    pu = _lib.Pricer(ctx, n, menus, offsets, mode="u16")
+    vu, ru, mu = pu.price(scores)
+    pu.close()
+    assert mu > 0 and abs(vu - vm) <= mu + 1e-5 + 1e-6 * abs(vm)
+    assert sorted(ru.tolist()) == list(range(n))

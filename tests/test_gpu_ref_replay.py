@@ -29,10 +29,13 @@ CASES = list(_cases())
 
 
 @pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("mode", ["f32", "u16", "u24"])
+@pytest.mark.parametrize("mode", ["f32", "f32_stream", "u16", "u24"])
 def test_stream_pricer_matches_reference_kernels(ctx, name, cd, n, mode):
+    """f32: the lattice by mask where it fits (the tile sweep); f32_stream: two rank-indexed layers."""
     menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
-    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+    stream = mode == "f32_stream"
+    mode = "f32" if stream else mode
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode, stream=stream)
     rng = np.random.RandomState(11)
     for trial in range(2):
         scores = (rng.randn(menus.size) * (1.0 if trial == 0 else 0.02)).astype(np.float32)
@@ -211,7 +214,7 @@ def test_config3_columns_match_reference_kernels_every_iteration(ctx, mode):
 
 
 # ------------------------------------------------------------------ large lattices
-@pytest.mark.parametrize("mode", ["f32", "u16", "u24"])
+@pytest.mark.parametrize("mode", ["f32", "f32_stream", "u16", "u24"])
 def test_stream_pricer_at_n28_matches_reference_kernels(ctx, mode):
     """The stream pricer at n = 28 (pairwise menus, 756 rows; 2^28 subsets, rows scanned per
     subset as the lists are not built above n = 26) against the reference's own stream kernels:
@@ -220,7 +223,9 @@ def test_stream_pricer_at_n28_matches_reference_kernels(ctx, mode):
     n = 28
     cd, _ = PI.gen_pairwise(n)
     menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
-    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode)
+    stream = mode == "f32_stream"
+    mode = "f32" if stream else mode
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode=mode, stream=stream)
     scores = (np.random.RandomState(28).randn(menus.size)).astype(np.float32)
     v_ref, r_ref, m_ref, steps_ref = ref_replay.price_stream(menus, alts, scores, offsets, n, mode=mode)
     v, r, m, steps = pr.price(scores, want_steps=True)
