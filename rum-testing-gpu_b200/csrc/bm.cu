@@ -730,9 +730,9 @@ static void enqueue_iteration_ptrs(const IterPtrs<T> &I, const BmCoef &C, int n,
     if (g_prof) {
         double S = (double)P.Nloc * n * K, e = sizeof(T);
         static const char *form_name[PROX_FORMS] = {"prox_tile", "prox_lanes2", "prox_lanes4", "prox_lanes8", "prox_tau",
-                                                    "prox_tau2"};
-        const int f = (n > PROX_LANES_MAX_N && C.prox_form != PROX_TAU && C.prox_form != PROX_TAU2) ? PROX_TILE
-                                                                                                      : C.prox_form;
+                                                    "prox_tau2", "prox_pair"};
+        const int f = (n > PROX_LANES_MAX_N && C.prox_form != PROX_TAU && C.prox_form != PROX_TAU2 &&
+                       C.prox_form != PROX_PAIR) ? PROX_TILE : C.prox_form;
         prof_begin(std::string(form_name[f]) + (e == 8 ? "<f64>" : "<f32>"), 5.0 * S * e + 4.0 * (1LL << n), st);
     }
     launch_prox_tile<T>(P, st, K, C.prox_form);

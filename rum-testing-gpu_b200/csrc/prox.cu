@@ -367,9 +367,12 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tau_kernel(ProxTileArgs<T>
 }
 
 // The one-walk form with two staged arrays (more CTAs per SM): xo formed while staging, the
-// previous support kept as one bit per element.
-template <class T, int N>
-__global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T> P) {
+// previous support kept as one bit per element. TPM = 2: two threads per menu (a lane pair), each
+// walking every other member, the walk's sums, extremes and support joined by one shuffle each
+// (more resident warps for the same shared memory, half of each thread's dependent chain).
+template <class T, int N, int TPM = 1>
+__global__ void __launch_bounds__(PT_THREADS * TPM, TPM == 1 ? 6 : 5) prox_tau2_kernel(ProxTileArgs<T> P) {
+    constexpr int NT = PT_THREADS * TPM;
     extern __shared__ __align__(128) unsigned char pt_smem[];
     if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
     {
@@ -406,24 +409,43 @@ __global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T
     const T one = (T)1, two = (T)2;
     // z staged as it is; the relaxed point xo = alpha x + (1 - alpha) x2 formed on the way in, with
     // one bit per element for x2 > 0 (the previous support): two staged arrays instead of three
-    for (int c = tid; c < Et / VEC; c += PT_THREADS) {
-        const int e = c * VEC;
-        const int i = run_of(e);
-        const ll g = rg[i] + (e - roff[i]);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sz + e)), "l"(P.z + g) : "memory");
-        T xv[VEC], x2v[VEC];
-        *reinterpret_cast<uint4 *>(xv) = *reinterpret_cast<const uint4 *>(P.x + g);
-        *reinterpret_cast<uint4 *>(x2v) = *reinterpret_cast<const uint4 *>(P.x2 + g);
-        const unsigned am = __activemask();
+    // SU chunks per thread in flight: every load of a round is issued before any is used
+    constexpr int SU = 4;
+    const int nch = Et / VEC;
+    for (int c0 = tid; c0 < nch; c0 += NT * SU) {
+        T xv[SU][VEC], x2v[SU][VEC];
 #pragma unroll
-        for (int t = 0; t < VEC; ++t) {
-            sx[e + t] = P.alpha * xv[t] + (one - P.alpha) * x2v[t];
-            const unsigned b = __ballot_sync(am, x2v[t] > (T)0);
-            if ((threadIdx.x & 31) == __ffs(am) - 1) sbit[(c >> 5) * VEC + t] = b;
+        for (int u = 0; u < SU; ++u) {
+            const int c = c0 + u * NT;
+            if (c < nch) {
+                const int e = c * VEC;
+                const int i = run_of(e);
+                const ll g = rg[i] + (e - roff[i]);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sz + e)), "l"(P.z + g)
+                             : "memory");
+                *reinterpret_cast<uint4 *>(xv[u]) = *reinterpret_cast<const uint4 *>(P.x + g);
+                *reinterpret_cast<uint4 *>(x2v[u]) = *reinterpret_cast<const uint4 *>(P.x2 + g);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int c = c0 + u * NT;
+            if (c < nch) {
+                const int e = c * VEC;
+                const unsigned am = __activemask();
+#pragma unroll
+                for (int t = 0; t < VEC; ++t) {
+                    sx[e + t] = P.alpha * xv[u][t] + (one - P.alpha) * x2v[u][t];
+                    const unsigned b = __ballot_sync(am, x2v[u][t] > (T)0);
+                    if ((threadIdx.x & 31) == __ffs(am) - 1) sbit[(c >> 5) * VEC + t] = b;
+                }
+            }
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
-    const uint32_t low = (uint32_t)tid;
+    const uint32_t low = (uint32_t)(tid / TPM);
+    const int h = tid % TPM;                              // this thread's share of the members
+    const unsigned pm = TPM == 2 ? 3u << ((threadIdx.x & 31) & ~1) : 0u;
     const uint32_t S = base | low;
     const uint32_t wb = P.menu_obs[S];
     asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -435,7 +457,9 @@ __global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T
     uint32_t A0 = 0;
     double s1 = 0.0, s2 = 0.0, f1 = 0.0, f2 = 0.0;
     double min_on = INFINITY, max_off = -INFINITY;
-    for (uint32_t SS = S; SS; SS &= SS - 1) {
+    uint32_t SS = S;
+    if (TPM == 2 && h) SS &= SS - 1;
+    for (; SS; SS &= SS - 1) {
         const int i = __ffs(SS) - 1;
         const int e = roff[i] + (int)(i < PT_M ? cb32(low, i) : low);
         const int ce = e / VEC;
@@ -467,6 +491,16 @@ __global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T
         } else {
             max_off = ti > max_off ? ti : max_off;
         }
+        if (TPM == 2) SS &= SS - 1;                        // the partner's member
+    }
+    if constexpr (TPM == 2) {
+        A0 |= __shfl_xor_sync(pm, A0, 1);
+        s1 += __shfl_xor_sync(pm, s1, 1);
+        s2 += __shfl_xor_sync(pm, s2, 1);
+        f1 += __shfl_xor_sync(pm, f1, 1);
+        f2 += __shfl_xor_sync(pm, f2, 1);
+        min_on = fmin(min_on, __shfl_xor_sync(pm, min_on, 1));
+        max_off = fmax(max_off, __shfl_xor_sync(pm, max_off, 1));
     }
     auto t_of = [&](int i, int e) -> double {
         double ti = (double)sx[e];
@@ -488,7 +522,9 @@ __global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T
             uint32_t A2 = 0;
             s1 = 0.0;
             s2 = 0.0;
-            for (uint32_t AA = A; AA; AA &= AA - 1) {
+            uint32_t AA = A;
+            if (TPM == 2 && h) AA &= AA - 1;
+            for (; AA; AA &= AA - 1) {
                 const int i = __ffs(AA) - 1;
                 const double ti = t_of(i, roff[i] + (int)(i < PT_M ? cb32(low, i) : low));
                 const double ic = mixed ? (((wb >> i) & 1u) ? icw : icu) : 1.0;
@@ -497,19 +533,27 @@ __global__ void __launch_bounds__(PT_THREADS, 6) prox_tau2_kernel(ProxTileArgs<T
                     s1 += mixed ? ti * ic : ti;
                     s2 += ic;
                 }
+                if (TPM == 2) AA &= AA - 1;
+            }
+            if constexpr (TPM == 2) {
+                A2 |= __shfl_xor_sync(pm, A2, 1);
+                s1 += __shfl_xor_sync(pm, s1, 1);
+                s2 += __shfl_xor_sync(pm, s2, 1);
             }
             if (A2 == A) break;
             A = A2;
             tau = (s1 - 1.0) / s2;
         }
     }
-    stau[low] = tau;
-    sobs[low] = wb;
-    sflag[low] = (unsigned char)(k == 1 ? PT_SINGLE : (mixed ? PT_MIXED : PT_PLAIN));
+    if (h == 0) {
+        stau[low] = tau;
+        sobs[low] = wb;
+        sflag[low] = (unsigned char)(k == 1 ? PT_SINGLE : (mixed ? PT_MIXED : PT_PLAIN));
+    }
     __syncthreads();
     // the projection and the write-back, element by element: element e of run i belongs to the
     // menu base | low, low = e - roff[i] for a high run, the lows containing i in order for a low run
-    for (int c = tid; c < Et / VEC; c += PT_THREADS) {
+    for (int c = tid; c < Et / VEC; c += NT) {
         const int e = c * VEC;
         const int i = run_of(e);
         const int pos = e - roff[i];
@@ -724,14 +768,14 @@ static void launch_tau_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     RUMB_LAUNCH("prox_tau_kernel");
 }
 
-template <class T, int N>
+template <class T, int N, int TPM = 1>
 static void launch_tau2_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     static std::atomic<unsigned long long> optin{0};   // the opt-in above 48 KB, per device
     constexpr int E_max = (int)prox_tile_elems(N), VEC = 16 / (int)sizeof(T);
     const size_t smem = 256 + 2 * (size_t)E_max * sizeof(T) + (size_t)((E_max / VEC + 31) / 32) * VEC * 4;
-    smem_optin(prox_tau2_kernel<T, N>, (int)smem, optin);
+    smem_optin(prox_tau2_kernel<T, N, TPM>, (int)smem, optin);
     dim3 grid((unsigned)(1LL << (N - PT_M)), (unsigned)slots);
-    prox_tau2_kernel<T, N><<<grid, PT_THREADS, smem, st>>>(P);
+    prox_tau2_kernel<T, N, TPM><<<grid, PT_THREADS * TPM, smem, st>>>(P);
     RUMB_LAUNCH("prox_tau2_kernel");
 }
 
@@ -750,13 +794,14 @@ static void launch_form_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots, 
         case PROX_LANES8: launch_lanes_n<T, N, 8>(P, st, slots); return;
         case PROX_TAU: launch_tau_n<T, N>(P, st, slots); return;
         case PROX_TAU2: launch_tau2_n<T, N>(P, st, slots); return;
+        case PROX_PAIR: launch_tau2_n<T, N, 2>(P, st, slots); return;
         default: launch_tile_n<T, N>(P, st, slots); return;
     }
 }
 
 template <class T>
 void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots, int form) {
-    if (P.n > PROX_LANES_MAX_N && form != PROX_TAU && form != PROX_TAU2) form = PROX_TILE;
+    if (P.n > PROX_LANES_MAX_N && form != PROX_TAU && form != PROX_TAU2 && form != PROX_PAIR) form = PROX_TILE;
     switch (P.n) {
 #define RUMB_PT_CASE(NN) \
     case NN: launch_form_n<T, NN>(P, st, slots, form); return;
@@ -768,6 +813,7 @@ void launch_prox_tile(const ProxTileArgs<T> &P, cudaStream_t st, int slots, int 
     case NN:                                                                                                      \
         if (form == PROX_TAU) launch_tau_n<T, NN>(P, st, slots);                                                  \
         else if (form == PROX_TAU2) launch_tau2_n<T, NN>(P, st, slots);                                           \
+        else if (form == PROX_PAIR) launch_tau2_n<T, NN, 2>(P, st, slots);                                        \
         else launch_tile_n<T, NN>(P, st, slots);                                                                  \
         return;
         RUMB_PT_CASE(23) RUMB_PT_CASE(24) RUMB_PT_CASE(25)

@@ -112,7 +112,7 @@ __device__ __forceinline__ ll pt_rstart(uint32_t base, int i, ll Nloc) {
 // lanes per menu reading the slab straight into registers
 // (n <= PROX_LANES_MAX_N). Picked per GPU, n and dtype by timing (the iteration's autotuner).
 constexpr int PROX_TILE = 0, PROX_LANES2 = 1, PROX_LANES4 = 2, PROX_LANES8 = 3, PROX_TAU = 4, PROX_TAU2 = 5,
-              PROX_FORMS = 6;
+              PROX_PAIR = 6, PROX_FORMS = 7;
 constexpr int PROX_LANES_MAX_N = 22;
 
 // The prox for one dtype (csrc/prox.cu; grid.y = batched draws' slots).

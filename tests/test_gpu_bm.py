@@ -134,13 +134,13 @@ def test_iterates_track_oracle(ctx, case, dtype):
             assert d <= tol[total] * max(1.0, float(np.max(np.abs(getattr(bm, name))))), (name, total, d)
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("case", ["n10_all_k20", "n16_mix"])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
 def test_prox_forms_track_oracle(ctx, monkeypatch, case, form, dtype):
     """Every form of the iteration's prox kernel (RUMB_PROX_FORM: 0 the shared-memory tile, 1..3
     two, four or eight lanes per menu reading the slab into registers, 4 the tile with one member walk
-    and the projection element by element, 5 the same with two staged arrays) keeps the iterates on
+    and the projection element by element, 5 the same with two staged arrays, 6 that with two threads per menu) keeps the iterates on
     the oracle's: float64 to 1e-10 after 10 iterations, float32 at its rounding floor."""
     monkeypatch.setenv("RUMB_PROX_FORM", str(form))
     n, menu, alt, p = _instance(case)
