@@ -274,7 +274,7 @@ class Bootstrap:
         self.n = int(self.draws.default_n if n is None else n)
         self.r_n, self.eps_n, self.s = scaling(self.n, r_n, eps_n)
         self.draws.check_n(self.n)
-        self.session = rum.session(method=method, method_args=method_args)
+        self._session, self._session_args = None, dict(method=method, method_args=method_args)
         self.batch_slots = batch_slots
         self.L, self.U = np.zeros(self.B), np.full(self.B, np.inf)
         self.solved = np.zeros(self.B, dtype=bool)
@@ -314,6 +314,19 @@ class Bootstrap:
     @property
     def tau(self):
         return (self.s * self.L0, self.s * self.U0)
+
+    @property
+    def session(self):
+        """The Session every solve of this bootstrap goes through, opened on first use as the
+        reference opens its own (solver/inference/bootstrap.py:261-266): the record's plan stays
+        None until a solve has run."""
+        if self._session is None:
+            self._session = self.rum.session(**self._session_args)
+        return self._session
+
+    @session.setter
+    def session(self, s):
+        self._session = s
 
     def _certify(self):
         """p_hat's bracket at the current tolerances (a later, tighter one only narrows it)."""
@@ -480,9 +493,10 @@ class Bootstrap:
     def record(self):
         """Everything needed to report or resume the run, as plain Python values, in the reference's
         record layout (solver/inference/bootstrap.py:356-370)."""
-        s = self.session
+        s = self._session
         return dict(version=VERSION, settings=self.settings, fingerprints=self.fingerprints,
-                    plan=dict(method=s.method, method_args=s.method_args, auto_reason=s.auto_reason),
+                    plan=None if s is None else dict(method=s.method, method_args=s.method_args,
+                                                    auto_reason=s.auto_reason),
                     p_hat=dict(lb=self.L0, ub=self.U0, certificates=getattr(self, "certificates", [])),
                     tau=None if self.L0 is None else list(self.tau),
                     scaling=dict(r_n=self.r_n, eps_n=self.eps_n, s=self.s),

@@ -69,6 +69,11 @@ class Result:
     machine: str = ""
     info: dict = field(default_factory=dict)
     mode: str = "certificate"
+    # the reference's race fields (solver/rum_solver.py:109-112); a certified distance leaves them None
+    opt: float = None
+    target: float = None
+    abs_to_opt: float = None
+    rel_to_opt: float = None
 
     def __repr__(self):
         rows = [("exit_flag", "%d (%s)" % (self.exit_flag, self.status)), ("distance", "%.10g" % self.distance),

@@ -348,3 +348,29 @@ def test_bootstrap_inputs_refused(fake_gpu):
     assert set(b.record()) >= {"replies", "p_hat", "draws", "results"}
     with pytest.raises(ValueError, match="replies per menu"):
         rr.bootstrap(replies=replies, B=4, n=10 ** 6)
+
+
+_RECORDS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "records.json")
+
+
+@pytest.mark.skipif(not os.path.exists(_RECORDS), reason="reference records not recorded")
+def test_records_byte_compatible_with_the_reference(fake_gpu):
+    """Result.to_dict() and Bootstrap.record() give the JSON text the reference's own writers gave
+    for the same values and inputs (tests/golden/make_record_golden.py; solver/rum_solver.py:143-149,
+    solver/inference/bootstrap.py:356-370), byte for byte: field names, order and values."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_record_golden as MRG
+    from rumb import cells_from_panel
+    g = json.load(open(_RECORDS))
+    assert json.dumps(rum_solver.Result(**MRG.RESULT_FIELDS).to_dict()) == g["result_to_dict"]
+    panel, m, a, p = MRG.panel_case()
+    rec = rum_solver.RUM(m, a, p, num_alternatives=8).bootstrap(panel=panel, B=12, weights="multinomial",
+                                                               seed=5).record()
+    rec.pop("when")
+    assert json.dumps(rec, indent=1) == g["bootstrap_panel_record"]
+    replies = dict(menu=panel["menu"], chosen=panel["chosen"])
+    rec = rum_solver.RUM(*cells_from_panel(replies, 8), num_alternatives=8).bootstrap(replies=replies, B=6,
+                                                                                      seed=3).record()
+    rec.pop("when")
+    assert json.dumps(rec, indent=1) == g["bootstrap_replies_record"]
