@@ -485,6 +485,55 @@ def run_pricing_large(args, rank, sweeps=3):
                       "runs": out, "reference_rtx5090": LARGE_N_PUBLISHED}), flush=True)
 
 
+def run_learned_n10(args, rank):
+    """Workload learned_n10: the learned warm start at shapes whose distances are large against the
+    network's error (n = 10 panels of 200 respondents x 20 menus and 120 x 30, K = 8 / 6): 128
+    draws, the first 96 train the network, the last 32 are solved to abs 5e-4 seeded by it (lower
+    bound at the prediction and, with y0_state, the start state's fitted cells) and without it;
+    reports the Frank-Wolfe bound at the prediction against the one at p_hat's fit, iterations
+    both ways and the draws' decisions against the band."""
+    if rank != 0:
+        return
+    from rumb import RUM
+    from rumb import bootstrap as BS
+    from rumb.instances import panel_instance
+    from rumb.rum_solver import context
+    runs = []
+    for (dens, resp, per, K, seed) in ((0.5, 200, 20, 8, 3), (1.0, 120, 30, 6, 4)):
+        panel, (m, a, p) = panel_instance(10, dens, resp, per, K, seed=seed)
+        rum = RUM(m, a, p, num_alternatives=10)
+        ntr, nte = 96, 32
+        kw = dict(panel=panel, B=ntr + nte, weights="multinomial", seed=0, method="bm_admm",
+                  method_args={"dtype": "float64"})
+        row = {"rows": int(p.size)}
+        for y0_state in (False, True):
+            boot = rum.bootstrap(learned=True, train_draws=ntr, mlp_epochs=300, y0_state=y0_state, **kw)
+            plain = rum.bootstrap(**kw)
+            for b in (boot, plain):
+                b._certify()
+            idx = np.arange(ntr + nte)
+            boot.solve_draws(idx, stops=False)
+            plain.solve_draws(idx, stops=False)
+            te = idx[ntr:]
+            g, ctx = rum._geom, context()
+            P = BS.perturb(boot.p_hat, boot.draws.rows(te), boot.r_n, boot.eps_n)
+            yp = boot.predict_fit(P)
+            lb_net = [ctx.fw_lb64(10, g.menu, g.alternative, yp[j], P[j]) for j in range(nte)]
+            lb_hat = [ctx.fw_lb64(10, g.menu, g.alternative, boot.session.fit, P[j]) for j in range(nte)]
+            dec = BS.decide(boot.L[te], boot.U[te], *boot.tau)
+            row["y0_state" if y0_state else "lb_seed"] = dict(
+                iters_learned=int(boot.iters[te].sum()), iters_plain=int(plain.iters[te].sum()),
+                lb_at_prediction_median=float(np.median(lb_net)), lb_at_p_hat_fit_median=float(np.median(lb_hat)))
+        row.update(p_hat_bracket=[boot.L0, boot.U0], band=list(boot.tau),
+                   distance_min_median_max=[float(np.min(plain.U[te])), float(np.median(plain.U[te])),
+                                            float(np.max(plain.U[te]))],
+                   decided_below_above_open=[int((dec == BS.BELOW).sum()), int((dec == BS.ABOVE).sum()),
+                                             int((dec == BS.UNDECIDED).sum())])
+        runs.append(row)
+    print(json.dumps({"metric": "learned warm start at n = 10 panels: iterations of 32 seeded draws against plain",
+                      "unit": "iterations", "n_gpus": 1, "data": "synthetic", "runs": runs}), flush=True)
+
+
 def run_dsr_n25(args, rank, seconds=90.0):
     """Workload dsr_n25 (n25_dsr301_panel520: n = 25, alternative 0 observed on 301 menus, a
     520-respondent panel, K = 40; the learned warm start's configuration): p_hat's own certified
@@ -562,7 +611,8 @@ def main():
     ap.add_argument("--no-bootstrap", action="store_true", help="skip the bootstrap leg of the bench line")
     ap.add_argument("--pricing-n", default="", help="pricing_large: comma-separated n to run (default all)")
     ap.add_argument("--pricing-modes", default="", help="pricing_large: comma-separated storages to run")
-    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing", "pricing_large", "dsr_n25"],
+    ap.add_argument("--workload", default="bm_n18", choices=["bm_n18", "bootstrap_n20", "paper", "pricing", "pricing_large", "dsr_n25",
+                             "learned_n10"],
                     help="bootstrap_n20: the batched-draw comparison; paper: the reference's certified runs on "
                          "its paper instances beside its published times (each prints its own line)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="ITERS",
@@ -584,6 +634,9 @@ def main():
         return
     if args.workload == "dsr_n25":
         run_dsr_n25(args, rank)
+        return
+    if args.workload == "learned_n10":
+        run_learned_n10(args, rank)
         return
     if args.workload == "pricing_large":
         run_pricing_large(args, rank)
