@@ -49,6 +49,7 @@ struct PricerArgs {
     const uint16_t *vprev_h;
     const uint8_t *lprev;
     const float *mprev, *eprev;
+    const float *vprev_dec;    // the previous layer already decoded to float32 (or nullptr)
     // current layer
     float *vcur_f;
     uint16_t *vcur_h;
@@ -113,6 +114,7 @@ __device__ __forceinline__ ull colex_rank_without(ull r, ull D, int x, int j, in
 }
 
 __device__ __forceinline__ float decode_prev(const PricerArgs &A, ull rp) {
+    if (A.vprev_dec) return A.vprev_dec[rp];
     if (A.mode == 1) return A.vprev_f[rp];
     unsigned int q = A.vprev_h[rp];
     if (A.mode == 3) q = (q << 8) | (unsigned int)A.lprev[rp];
@@ -397,6 +399,13 @@ __global__ void cover_build_kernel(int n, ull nD, const ull *binom, const ull *l
         }
         if (in) ++p;
     }
+}
+
+// The previous layer's quantized values decoded once to float32 (decode_prev's arithmetic, so the
+// same floats), for the group sweep: a rank reads k predecessors, each a value, an offset and a step.
+__global__ void stream_decode_kernel(PricerArgs A, ull count_prev, float *dec) {
+    const ull r = blockIdx.x * (ull)blockDim.x + threadIdx.x;
+    if (r < count_prev) dec[r] = decode_prev(A, r);
 }
 
 __global__ void __launch_bounds__(PB) stream_quant_kernel(PricerArgs A, const float *vals) {
@@ -786,7 +795,8 @@ __global__ void sub_readout_kernel(int K, const float *V, const uint8_t *pred, S
 //   x in L: D \ {x} is (L \ {x}, H), rank base(H, l - 1) + rank_{l-1}(L \ {x});
 //   w(x, D): one pass over x's rows for the group; a row whose menu's high part is not within H
 //   fails for every slot (a warp-uniform skip), the others are tested on the low part per slot.
-// Values are decoded from the previous layer's storage and candidates merge with the larger value
+// Values are decoded from the previous layer's storage (in quantized storage once per layer by
+// stream_decode_kernel when the float32 copy fits) and candidates merge with the larger value
 // winning and, on equal values, the lower x (the row scan's x descending with `>=`): the layer is
 // the layer kernels' bit for bit, and stream_quant_kernel quantizes it as before.
 constexpr int SG_LOW = 10, SG_REGS = 8, SG_WARPS = 4, SG_PF = 4;   // SG_PF: rows read ahead
@@ -936,6 +946,7 @@ struct Pricer {
     DevBuf Vs, Ps;                          // sub-lattice / mask scratch
     DevBuf Ws;                              // sub-lattice sums w(x_j, D(s)): 2^k_pred * k_pred floats
     DevBuf vals;                            // a layer's float32 values before quantization
+    DevBuf dec;                             // the group sweep's decoded previous layer (quantized storage)
     DevBuf out;                             // PriceOut
     std::vector<ll> host_offsets;
     // cover lists (wmode != W_SCAN)
@@ -1175,11 +1186,20 @@ static void choose_stream_form(Pricer &P) {
         RUMB_CUDA(cudaMemcpy(P.lowtab.ptr, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
     }
     const char *env = getenv("RUMB_STREAM_FORM");
-    if (env && std::strcmp(env, "group") == 0 && group_ok) { P.stream_group = true; return; }
     if (env && std::strcmp(env, "layer") == 0) { P.stream_group = false; return; }
     if (!group_ok) { P.stream_group = false; return; }
-    if (P.wmode == W_SCAN) { P.stream_group = true; return; }
-    P.stream_group = faster_second(P, [&](bool second) { P.stream_group = second; });
+    // quantized storage: each layer decoded once for the group sweep while it fits a quarter of the
+    // free memory (one float32 per rank of the largest layer)
+    if (P.mode >= 2) {
+        ull cap = 0;
+        for (ull v : P.counts) cap = v > cap ? v : cap;
+        size_t free_b = 0, total_b = 0;
+        RUMB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        if ((double)cap * 4.0 <= 0.25 * (double)free_b) P.dec.ensure((size_t)cap * 4);
+    }
+    if (P.wmode == W_SCAN || (env && std::strcmp(env, "group") == 0)) P.stream_group = true;
+    else P.stream_group = faster_second(P, [&](bool second) { P.stream_group = second; });
+    if (!P.stream_group) P.dec.release();
 }
 
 // Float32 storage keeps the same float32 value for every subset whether it is stored by colex rank
@@ -1441,6 +1461,14 @@ static void run_sweep(Pricer *P, const float *scores) {
                 }
                 G.rows = P->rows.as<int4>();
                 G.lowtab = P->lowtab.as<uint16_t>();
+                if (P->dec.ptr && A.mode >= 2) {
+                    const ull cprev = P->counts[k - 1];
+                    stream_decode_kernel<<<grid_for((ll)cprev, 256), 256, 0, st>>>(A, cprev, P->dec.as<float>());
+                    RUMB_LAUNCH("stream_decode_kernel");
+                    A.vprev_dec = P->dec.as<float>();
+                } else if (A.mode == 1) {
+                    A.vprev_dec = A.vprev_f;                    // float32 storage is its own decoded copy
+                }
                 const ull groups = G.cum[G.lmax - G.lmin + 1];
                 stream_group_kernel<<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
                     A, G, P->vals.as<float>());
