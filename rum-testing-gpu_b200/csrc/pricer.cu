@@ -766,6 +766,117 @@ __global__ void __launch_bounds__(32 * MT_WARPS) mask_tile_kernel(MaskTileArgs A
     }
 }
 
+// The tile sweep's form for launches with few tiles (small n, the first and last popcounts): one
+// CTA of MT_SPLIT warps per tile, warp w taking the alternatives x = w (mod MT_SPLIT) through the
+// same row pass as mask_tile_kernel, the warps' high candidates merged through shared memory, and
+// the low candidates' popcount rounds spread over the CTA's threads. A launch then waits for an
+// eighth of a tile's row pass instead of all of it. The candidates, their sums and the merge rule
+// are mask_tile_kernel's, so V and the predecessor bytes are the same bits.
+constexpr int MT_SPLIT = 8;
+__global__ void __launch_bounds__(32 * MT_SPLIT) mask_tile_split_kernel(MaskTileArgs A, MtOrder ord) {
+    __shared__ float wl[MT_LOW][MT_TILE / 2];
+    __shared__ float pv[MT_SPLIT][MT_TILE];
+    __shared__ signed char pb[MT_SPLIT][MT_TILE];
+    __shared__ float vt[MT_TILE];
+    __shared__ uint8_t bt[MT_TILE];
+    __shared__ unsigned sbin[(MASK_MAX_N - MT_LOW + 1) * (MASK_MAX_N - MT_LOW + 1)];
+    __shared__ uint8_t sord[MT_TILE];
+    const int n = A.n, h = A.h;
+    for (int i = threadIdx.x; i < (h + 1) * (h + 1); i += blockDim.x)
+        sbin[i] = (unsigned)A.binom[(i / (h + 1)) * A.bstride + i % (h + 1)];
+    for (int i = threadIdx.x; i < MT_TILE; i += blockDim.x) sord[i] = ord.order[i];
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned H = 0;
+    {
+        unsigned r = (unsigned)blockIdx.x;
+        int b = h - 1;
+        for (int k = A.t; k >= 1; --k) {
+            while (sbin[b * (h + 1) + k] > r) --b;
+            H |= 1u << b;
+            r -= sbin[b * (h + 1) + k];
+            --b;
+        }
+    }
+    const unsigned nH = ~H, nlane = ~(unsigned)lane;
+    const ull base = (ull)H << MT_LOW;
+    float best[MT_REGS];
+    int bx[MT_REGS];
+#pragma unroll
+    for (int j = 0; j < MT_REGS; ++j) {
+        best[j] = 0.0f;
+        bx[j] = -1;
+    }
+    for (int x = w; x < n; x += MT_SPLIT) {
+        const bool high = x >= MT_LOW;
+        if (high && !((H >> (x - MT_LOW)) & 1u)) continue;      // uniform per warp
+        float prev[MT_REGS];
+        if (high) {
+            const float *pvp = A.V + (base ^ (1ULL << x)) + lane;
+#pragma unroll
+            for (int j = 0; j < MT_REGS; ++j) prev[j] = pvp[32 * j];
+        }
+        float acc[MT_REGS];
+#pragma unroll
+        for (int j = 0; j < MT_REGS; ++j) acc[j] = 0.0f;
+        const int lo = (int)A.offsets[x], hi = (int)A.offsets[x + 1];
+        for (int i0 = lo; i0 < hi; i0 += ROW_PF) {
+            int4 R[ROW_PF];
+#pragma unroll
+            for (int u = 0; u < ROW_PF; ++u) R[u] = i0 + u < hi ? __ldg(A.rows + i0 + u) : ROW_NONE;
+#pragma unroll
+            for (int u = 0; u < ROW_PF; ++u) {
+                if ((unsigned)R[u].x & nH) continue;
+                const float sc = ((unsigned)R[u].y & nlane) ? 0.0f : __int_as_float(R[u].z);
+                mt_add(acc, R[u].w, sc);
+            }
+        }
+        if (high) {
+#pragma unroll
+            for (int j = 0; j < MT_REGS; ++j) mt_merge(best[j], bx[j], __fadd_rn(prev[j], acc[j]), x);
+        } else {
+#pragma unroll
+            for (int j = 0; j < MT_REGS; ++j) {
+                const int L = lane + 32 * j;
+                if ((L >> x) & 1) wl[x][mt_half(L, x)] = acc[j];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < MT_REGS; ++j) {
+        pv[w][lane + 32 * j] = best[j];
+        pb[w][lane + 32 * j] = (signed char)bx[j];
+    }
+    __syncthreads();
+    for (int L = threadIdx.x; L < MT_TILE; L += blockDim.x) {     // the warps' high candidates merged
+        float v = 0.0f;
+        int b = -1;
+        for (int q = 0; q < MT_SPLIT; ++q)
+            if (pb[q][L] >= 0) mt_merge(v, b, pv[q][L], pb[q][L]);
+        vt[L] = v;
+        bt[L] = (uint8_t)(b < 0 ? 255 : b);
+    }
+    __syncthreads();
+    for (int q = 1; q <= MT_LOW; ++q) {                         // low candidates, popcount rounds
+        for (int idx = ord.qoff[q] + (int)threadIdx.x; idx < ord.qoff[q + 1]; idx += blockDim.x) {
+            const int L = sord[idx];
+            float v = vt[L];
+            int b = bt[L] == 255 ? -1 : (int)bt[L];
+            for (unsigned m = (unsigned)L; m; m &= m - 1u) {
+                const int x = __ffs((int)m) - 1;
+                mt_merge(v, b, __fadd_rn(vt[L ^ (1 << x)], wl[x][mt_half(L, x)]), x);
+            }
+            vt[L] = v;
+            bt[L] = (uint8_t)(b < 0 ? 255 : b);
+        }
+        __syncthreads();
+    }
+    for (int L = threadIdx.x; L < MT_TILE; L += blockDim.x) {
+        A.V[base + L] = vt[L];
+        A.P[base + L] = bt[L] == 255 ? (uint8_t)0 : bt[L];
+    }
+}
+
 // The sub-lattice ranking after a tile sweep over the K elements left by the descent: positions
 // pos .. pos + K - 1 in the order the sub-lattice's predecessors give (element j of the sub-problem
 // is alternative elems[j]).
@@ -1064,6 +1175,9 @@ static void tile_sweep(cudaStream_t st, int n, ll mp, const ull *menus, const fl
     }
     const int h = n - MT_LOW;
     std::vector<ull> bt = binom_host(h);
+    int dev = 0;
+    RUMB_CUDA(cudaGetDevice(&dev));
+    const ull split_below = (ull)num_sms(dev) * 16;
     for (int t = 0; t <= h; ++t) {
         MaskTileArgs A{};
         A.n = n;
@@ -1076,8 +1190,13 @@ static void tile_sweep(cudaStream_t st, int n, ll mp, const ull *menus, const fl
         A.offsets = offsets;
         A.V = V;
         A.P = pred;
-        mask_tile_kernel<<<(unsigned)((A.count + MT_WARPS - 1) / MT_WARPS), 32 * MT_WARPS, 0, st>>>(A, order);
-        RUMB_LAUNCH("mask_tile_kernel");
+        if (A.count < split_below) {                    // too few tiles to fill the GPU: split each tile
+            mask_tile_split_kernel<<<(unsigned)A.count, 32 * MT_SPLIT, 0, st>>>(A, order);
+            RUMB_LAUNCH("mask_tile_split_kernel");
+        } else {
+            mask_tile_kernel<<<(unsigned)((A.count + MT_WARPS - 1) / MT_WARPS), 32 * MT_WARPS, 0, st>>>(A, order);
+            RUMB_LAUNCH("mask_tile_kernel");
+        }
     }
 }
 
