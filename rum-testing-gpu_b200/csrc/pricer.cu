@@ -623,7 +623,21 @@ __global__ void rows_kernel(ll mp, const ull *menus, const float *scores, const 
 constexpr int ROW_PF = 8;
 #define ROW_NONE make_int4(-1, 0, 0, 0)
 
-__device__ __forceinline__ void mt_merge(float &v, int &b, float c, int x) {
+// Row records of the float64 max sweep's group form: {menu >> shift, menu & ymask, score low and
+// high words}.
+__global__ void rows64_kernel(ll mp, const ull *menus, const double *scores, int shift, unsigned ymask, int4 *rows) {
+    const ll i = blockIdx.x * (ll)blockDim.x + threadIdx.x;
+    if (i >= mp) return;
+    const ull m = menus[i];
+    const double sc = scores[i];
+    rows[i] = make_int4((int)(unsigned)(m >> shift), (int)((unsigned)m & ymask), __double2loint(sc), __double2hiint(sc));
+}
+
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+template <class T>
+__device__ __forceinline__ void mt_merge(T &v, int &b, T c, int x) {
     if (b < 0 || c > v || (c == v && x < b)) {
         v = c;
         b = x;
@@ -917,25 +931,30 @@ struct StreamGroupArgs {
     int lmin, lmax;
     ull cum[SG_LOW + 2];       // groups before low popcount lmin + i
     int loff[SG_LOW + 2];      // first index of popcount l in the low-mask order
-    const int4 *rows;          // {menu >> SG_LOW, menu & (2^SG_LOW - 1), score bits, -}
+    const int4 *rows;          // {menu >> SG_LOW, menu & (2^SG_LOW - 1), score bits (float: .z, double: .z/.w)}
     const uint16_t *lowtab;    // [0, 2^SG_LOW): low masks by (popcount, value); then each mask's rank
+    const double *vprev64;     // the float64 max sweep: previous and current layer
+    double *vcur64;
 };
 
 // One group's slots, NR registers per lane (NR * 32 >= the group's C(SG_LOW, l) slots).
-template <int NR>
+// T = float: the pricing sweep (values decoded from the previous layer, predecessors, lowest x on
+// ties); T = double: the float64 max sweep (previous layer G.vprev64, scores as double bits in the
+// row records, only the maximum kept, G.vcur64 out).
+template <int NR, class T>
 __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupArgs &G, float *vals, const ull *sbin,
                                          const uint16_t *sord, const uint16_t *srk, int lane, int l, unsigned H,
                                          ull base, ull tsum, int nsl) {
     const int n = A.n;
     unsigned Lj[NR], nLj[NR];
-    float best[NR];
+    T best[NR];
     int bx[NR];
 #pragma unroll
     for (int j = 0; j < NR; ++j) {
         const int sl = lane + 32 * j;
         Lj[j] = sl < nsl ? (unsigned)sord[G.loff[l] + sl] : 0u;
         nLj[j] = ~Lj[j];
-        best[j] = 0.0f;
+        best[j] = (T)0;
         bx[j] = -1;
     }
     const unsigned nH = ~H;
@@ -952,17 +971,18 @@ __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupA
             cle += c0;
             ++ih;
         }
-        float prev[NR];
+        T prev[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
             const int sl = lane + 32 * j;
             const bool use = sl < nsl && (high || ((Lj[j] >> x) & 1u));
             const ull rp = high ? hbase + (ull)sl : tsum + (ull)srk[Lj[j] ^ (1u << x)];
-            prev[j] = use ? decode_prev(A, rp) : 0.0f;
+            if constexpr (sizeof(T) == 8) prev[j] = use ? G.vprev64[rp] : 0.0;
+            else prev[j] = use ? decode_prev(A, rp) : 0.0f;
         }
-        float acc[NR];
+        T acc[NR];
 #pragma unroll
-        for (int j = 0; j < NR; ++j) acc[j] = 0.0f;
+        for (int j = 0; j < NR; ++j) acc[j] = (T)0;
         const int lo = (int)A.offsets[x], hi = (int)A.offsets[x + 1];
         for (int i0 = lo; i0 < hi; i0 += SG_PF) {
             int4 R[SG_PF];
@@ -972,21 +992,23 @@ __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupA
             for (int u = 0; u < SG_PF; ++u) {
                 if ((unsigned)R[u].x & nH) continue;            // uniform: fails for the whole group
                 const unsigned ml = (unsigned)R[u].y;
-                const float sc = __int_as_float(R[u].z);
+                T sc;
+                if constexpr (sizeof(T) == 8) sc = __hiloint2double(R[u].w, R[u].z);
+                else sc = __int_as_float(R[u].z);
                 if (ml == 0u) {                                 // uniform: a menu within H fits every slot
 #pragma unroll
-                    for (int j = 0; j < NR; ++j) acc[j] = __fadd_rn(acc[j], sc);
+                    for (int j = 0; j < NR; ++j) acc[j] = add_rn(acc[j], sc);
                 } else {
 #pragma unroll
                     for (int j = 0; j < NR; ++j)
-                        if (!(ml & nLj[j])) acc[j] = __fadd_rn(acc[j], sc);
+                        if (!(ml & nLj[j])) acc[j] = add_rn(acc[j], sc);
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
             const int sl = lane + 32 * j;
-            if (sl < nsl && (high || ((Lj[j] >> x) & 1u))) mt_merge(best[j], bx[j], __fadd_rn(prev[j], acc[j]), x);
+            if (sl < nsl && (high || ((Lj[j] >> x) & 1u))) mt_merge(best[j], bx[j], add_rn(prev[j], acc[j]), x);
         }
     }
 #pragma unroll
@@ -994,12 +1016,17 @@ __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupA
         const int sl = lane + 32 * j;
         if (sl >= nsl) continue;
         const ull r = base + (ull)sl;
-        if (A.pred) A.pred[r] = (uint8_t)bx[j];
-        if (A.mode == 1) A.vcur_f[r] = best[j];
-        else vals[r] = best[j];
+        if constexpr (sizeof(T) == 8) {
+            G.vcur64[r] = best[j];
+        } else {
+            if (A.pred) A.pred[r] = (uint8_t)bx[j];
+            if (A.mode == 1) A.vcur_f[r] = best[j];
+            else vals[r] = best[j];
+        }
     }
 }
 
+template <class T>
 __global__ void __launch_bounds__(32 * SG_WARPS) stream_group_kernel(PricerArgs A, StreamGroupArgs G, float *vals) {
     __shared__ ull sbin[BIN_MAX];
     __shared__ uint16_t sord[1 << SG_LOW], srk[1 << SG_LOW];
@@ -1037,10 +1064,10 @@ __global__ void __launch_bounds__(32 * SG_WARPS) stream_group_kernel(PricerArgs 
         }
     }
     const int nsl = (int)sbin[SG_LOW * (n + 1) + l];
-    if (nsl <= 32) sg_group<1>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
-    else if (nsl <= 64) sg_group<2>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
-    else if (nsl <= 128) sg_group<4>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
-    else sg_group<SG_REGS>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    if (nsl <= 32) sg_group<1, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    else if (nsl <= 64) sg_group<2, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    else if (nsl <= 128) sg_group<4, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    else sg_group<SG_REGS, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
 }
 
 // ----------------------------------------------------------------- host object
@@ -1068,6 +1095,7 @@ struct Pricer {
     DevBuf lbase_dev, loffs, lent;
     std::vector<char> wide;                 // per layer: layer_wide_kernel (1) or layer_eval_kernel (0)
     DevBuf d64[2], s64;                     // the float64 max sweep's two layers and scores (on first use)
+    DevBuf rows64;                          // its group form's row records
     // mask storage: the tile sweep (mask_tile_kernel) or the layer kernels over the layer table
     bool by_mask = false;                   // the lattice is stored by mask (mask storage, or float32 routed)
     bool mask_tile = false;
@@ -1284,6 +1312,23 @@ static void choose_mask_form(Pricer &P) {
     P.mask_tile = faster_second(P, [&](bool second) { P.mask_tile = second; });
 }
 
+// The group sweep's low-mask table: the 2^SG_LOW masks by (popcount, value), then each mask's rank
+// among those of its popcount (once per pricer).
+static void ensure_lowtab(Pricer &P) {
+    if (P.lowtab.ptr) return;
+    std::vector<uint16_t> tab(2 << SG_LOW);
+    int k = 0;
+    std::vector<int> rk(SG_LOW + 1, 0);
+    for (int q = 0; q <= SG_LOW; ++q)
+        for (int L = 0; L < (1 << SG_LOW); ++L)
+            if (__builtin_popcount(L) == q) {
+                tab[k++] = (uint16_t)L;
+                tab[(1 << SG_LOW) + L] = (uint16_t)rk[q]++;
+            }
+    P.lowtab.ensure(tab.size() * 2);
+    RUMB_CUDA(cudaMemcpy(P.lowtab.ptr, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
+}
+
 // Stream storage: the group sweep from n = 12 on. Without cover lists it is taken; with them one
 // sweep of each form on zero scores picks the faster. RUMB_STREAM_FORM = "group" or "layer" pins
 // the form where it can run.
@@ -1292,17 +1337,7 @@ static void choose_stream_form(Pricer &P) {
     const bool group_ok = n >= SG_MIN_N;
     if (group_ok) {
         P.rows.ensure((size_t)std::max<ll>(P.mp, 1) * sizeof(int4));
-        std::vector<uint16_t> tab(2 << SG_LOW);
-        int k = 0;
-        std::vector<int> rk(SG_LOW + 1, 0);
-        for (int q = 0; q <= SG_LOW; ++q)
-            for (int L = 0; L < (1 << SG_LOW); ++L)
-                if (__builtin_popcount(L) == q) {
-                    tab[k++] = (uint16_t)L;
-                    tab[(1 << SG_LOW) + L] = (uint16_t)rk[q]++;
-                }
-        P.lowtab.ensure(tab.size() * 2);
-        RUMB_CUDA(cudaMemcpy(P.lowtab.ptr, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
+        ensure_lowtab(P);
     }
     const char *env = getenv("RUMB_STREAM_FORM");
     if (env && std::strcmp(env, "layer") == 0) { P.stream_group = false; return; }
@@ -1422,6 +1457,22 @@ void pricer_max64(Pricer *P, const double *scores_host, double *vmax) {
     P->s64.ensure((size_t)std::max<ll>(P->mp, 1) * 8);
     for (int i = 0; i < 2; ++i) P->d64[i].ensure((size_t)cap * 8);
     if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->s64.ptr, scores_host, (size_t)P->mp * 8, cudaMemcpyHostToDevice, st));
+    // the group form (rows scanned per group of ranks) where no cover lists were built, from n = 12 on
+    const char *env = getenv("RUMB_STREAM_FORM");
+    const bool group = n >= SG_MIN_N && !(env && std::strcmp(env, "layer") == 0) &&
+                       (P->wmode == W_SCAN || (env && std::strcmp(env, "group") == 0));
+    std::vector<ull> bh, b10;
+    if (group) {
+        ensure_lowtab(*P);
+        P->rows64.ensure((size_t)std::max<ll>(P->mp, 1) * sizeof(int4));
+        if (P->mp) {
+            rows64_kernel<<<grid_for(P->mp, 256), 256, 0, st>>>(P->mp, P->menus.as<ull>(), P->s64.as<double>(), SG_LOW,
+                                                               (1u << SG_LOW) - 1u, P->rows64.as<int4>());
+            RUMB_LAUNCH("rows64_kernel");
+        }
+        bh = binom_host(n - SG_LOW);
+        b10 = binom_host(SG_LOW);
+    }
     int cur = 0, prev = 1;
     RUMB_CUDA(cudaMemsetAsync(P->d64[prev].ptr, 0, 8, st));     // layer 0: V[empty set] = 0
     for (int k = 1; k <= n; ++k) {
@@ -1438,7 +1489,25 @@ void pricer_max64(Pricer *P, const double *scores_host, double *vmax) {
         A.lbase = P->wmode == W_SCAN ? 0 : P->lbase[k];
         const double *vp = P->d64[prev].as<double>();
         double *vc = P->d64[cur].as<double>();
-        if ((long long)A.count < 2LL * num_sms(c.device) * PE_R) {
+        if (group) {
+            const int hb = n - SG_LOW;
+            StreamGroupArgs G{};
+            G.lmin = std::max(0, k - hb);
+            G.lmax = std::min(SG_LOW, k);
+            for (int l = G.lmin; l <= G.lmax; ++l) G.cum[l - G.lmin + 1] = G.cum[l - G.lmin] + bh[hb * (hb + 1) + (k - l)];
+            for (int l = 0, o = 0; l <= SG_LOW; ++l) {
+                G.loff[l] = o;
+                o += (int)b10[SG_LOW * (SG_LOW + 1) + l];
+            }
+            G.rows = P->rows64.as<int4>();
+            G.lowtab = P->lowtab.as<uint16_t>();
+            G.vprev64 = vp;
+            G.vcur64 = vc;
+            const ull groups = G.cum[G.lmax - G.lmin + 1];
+            stream_group_kernel<double><<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
+                A, G, nullptr);
+            RUMB_LAUNCH("stream_group_kernel<f64>");
+        } else if ((long long)A.count < 2LL * num_sms(c.device) * PE_R) {
             max64_layer_kernel<PE_R_SMALL><<<(unsigned)((A.count + PE_R_SMALL - 1) / PE_R_SMALL), PE_R_SMALL * PE_G,
                                              0, st>>>(A, P->s64.as<double>(), vp, vc);
         } else {
@@ -1589,7 +1658,7 @@ static void run_sweep(Pricer *P, const float *scores) {
                     A.vprev_dec = A.vprev_f;                    // float32 storage is its own decoded copy
                 }
                 const ull groups = G.cum[G.lmax - G.lmin + 1];
-                stream_group_kernel<<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
+                stream_group_kernel<float><<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
                     A, G, P->vals.as<float>());
                 RUMB_LAUNCH("stream_group_kernel");
             } else {

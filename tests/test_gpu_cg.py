@@ -110,8 +110,9 @@ def test_cover_lists_wide_alternative(ctx):
 
 @pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
 def test_max64_sweep_bit_exact(ctx, name, cd, n):
-    """The float64 max sweep (rumb_cg_pricer_max64, cover lists and row scan) equals the oracle's and
-    the reference's own bf_stream_max64 kernel bit for bit."""
+    """The float64 max sweep (rumb_cg_pricer_max64: the layer kernels over cover lists; rows scanned,
+    from n = 12 the group form) equals the oracle's and the reference's own bf_stream_max64 kernel
+    bit for bit."""
     import ref_replay
     menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
     rng = np.random.RandomState(13)

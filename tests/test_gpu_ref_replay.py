@@ -234,3 +234,18 @@ def test_stream_pricer_at_n28_matches_reference_kernels(ctx, mode):
     np.testing.assert_array_equal(steps, steps_ref)
     assert abs(m - m_ref) <= 1e-6 * max(1.0, m_ref)
     pr.close()
+
+
+def test_max64_at_n28_matches_reference_kernels(ctx):
+    """The float64 max sweep at n = 28 (pairwise menus, rows scanned: the group form) against the
+    reference's own bf_stream_max64 kernel (solver/flow_cg/pricing_stream.py:190-249), bit for bit."""
+    if "max64" not in ref_replay._mods():
+        pytest.skip("the reference's max64 kernel is not built")
+    n = 28
+    cd, _ = PI.gen_pairwise(n)
+    menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
+    s = np.random.RandomState(281).randn(menus.size)
+    pr = _lib.Pricer(ctx, n, menus, offsets, mode="u16")
+    v = pr.max64(s)
+    pr.close()
+    assert v == ref_replay.sweep_max64(menus, s, offsets, n)
