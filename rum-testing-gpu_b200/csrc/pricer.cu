@@ -932,7 +932,7 @@ struct StreamGroupArgs {
     ull cum[SG_LOW + 2];       // groups before low popcount lmin + i
     int loff[SG_LOW + 2];      // first index of popcount l in the low-mask order
     const int4 *rows;          // {menu >> SG_LOW, menu & (2^SG_LOW - 1), score bits (float: .z, double: .z/.w)}
-    const uint16_t *lowtab;    // [0, 2^SG_LOW): low masks by (popcount, value); then each mask's rank
+    const uint16_t *lowtab;    // low masks by (popcount, value); each mask's rank; the 9-bit masks by (popcount, value)
     const double *vprev64;     // the float64 max sweep: previous and current layer
     double *vcur64;
 };
@@ -941,11 +941,16 @@ struct StreamGroupArgs {
 // T = float: the pricing sweep (values decoded from the previous layer, predecessors, lowest x on
 // ties); T = double: the float64 max sweep (previous layer G.vprev64, scores as double bits in the
 // row records, only the maximum kept, G.vcur64 out).
-template <int NR, class T>
+template <int NR, int NRC, class T>
 __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupArgs &G, float *vals, const ull *sbin,
-                                         const uint16_t *sord, const uint16_t *srk, int lane, int l, unsigned H,
-                                         ull base, ull tsum, int nsl) {
+                                         const uint16_t *sord, const uint16_t *srk, const uint16_t *sord9,
+                                         const int *off9, T *cbuf, int lane, int l, unsigned H, ull base, ull tsum,
+                                         int nsl) {
     const int n = A.n;
+    auto read_prev = [&](ull rp) -> T {
+        if constexpr (sizeof(T) == 8) return G.vprev64[rp];
+        else return decode_prev(A, rp);
+    };
     unsigned Lj[NR], nLj[NR];
     T best[NR];
     int bx[NR];
@@ -971,14 +976,61 @@ __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupA
             cle += c0;
             ++ih;
         }
+        if (!high && l == 0) continue;                    // no slot holds a low alternative
+        if constexpr (NRC < NR) {
+            if (!high) {
+                // only the slots that contain x: the (l-1)-subsets of the other 9 low bits, expanded
+                // around x (NRC registers instead of NR); each one's candidate goes to its slot
+                // through shared memory
+                const int c9 = (int)sbin[9 * (n + 1) + (l - 1)];
+                unsigned Lc[NRC], nLc[NRC];
+                T prevc[NRC], accc[NRC];
+#pragma unroll
+                for (int jc = 0; jc < NRC; ++jc) {
+                    const int cs = lane + 32 * jc;
+                    const unsigned m9 = cs < c9 ? (unsigned)sord9[off9[l - 1] + cs] : 0u;
+                    Lc[jc] = ((m9 >> x) << (x + 1)) | (1u << x) | (m9 & ((1u << x) - 1u));
+                    nLc[jc] = ~Lc[jc];
+                    prevc[jc] = cs < c9 ? read_prev(tsum + (ull)srk[Lc[jc] ^ (1u << x)]) : (T)0;
+                    accc[jc] = (T)0;
+                }
+                const int lo = (int)A.offsets[x], hi = (int)A.offsets[x + 1];
+                for (int i0 = lo; i0 < hi; i0 += SG_PF) {
+                    int4 R[SG_PF];
+#pragma unroll
+                    for (int u = 0; u < SG_PF; ++u) R[u] = i0 + u < hi ? __ldg(G.rows + i0 + u) : ROW_NONE;
+#pragma unroll
+                    for (int u = 0; u < SG_PF; ++u) {
+                        if ((unsigned)R[u].x & nH) continue;        // uniform: fails for the whole group
+                        const unsigned ml = (unsigned)R[u].y;
+                        T sc;
+                        if constexpr (sizeof(T) == 8) sc = __hiloint2double(R[u].w, R[u].z);
+                        else sc = __int_as_float(R[u].z);
+#pragma unroll
+                        for (int jc = 0; jc < NRC; ++jc)
+                            if (!(ml & nLc[jc])) accc[jc] = add_rn(accc[jc], sc);
+                    }
+                }
+#pragma unroll
+                for (int jc = 0; jc < NRC; ++jc)
+                    if (lane + 32 * jc < c9) cbuf[srk[Lc[jc]]] = add_rn(prevc[jc], accc[jc]);
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < NR; ++j) {
+                    const int sl = lane + 32 * j;
+                    if (sl < nsl && ((Lj[j] >> x) & 1u)) mt_merge(best[j], bx[j], cbuf[sl], x);
+                }
+                __syncwarp();
+                continue;
+            }
+        }
         T prev[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
             const int sl = lane + 32 * j;
             const bool use = sl < nsl && (high || ((Lj[j] >> x) & 1u));
             const ull rp = high ? hbase + (ull)sl : tsum + (ull)srk[Lj[j] ^ (1u << x)];
-            if constexpr (sizeof(T) == 8) prev[j] = use ? G.vprev64[rp] : 0.0;
-            else prev[j] = use ? decode_prev(A, rp) : 0.0f;
+            prev[j] = use ? read_prev(rp) : (T)0;
         }
         T acc[NR];
 #pragma unroll
@@ -1029,13 +1081,21 @@ __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupA
 template <class T>
 __global__ void __launch_bounds__(32 * SG_WARPS) stream_group_kernel(PricerArgs A, StreamGroupArgs G, float *vals) {
     __shared__ ull sbin[BIN_MAX];
-    __shared__ uint16_t sord[1 << SG_LOW], srk[1 << SG_LOW];
+    __shared__ uint16_t sord[1 << SG_LOW], srk[1 << SG_LOW], sord9[1 << (SG_LOW - 1)];
+    __shared__ int off9[SG_LOW + 1];
+    __shared__ T cbuf[SG_WARPS][SG_REGS * 32];
     const int n = A.n, k = A.k, hb = n - SG_LOW;
     stage_binom(sbin, A.binom, n);
     for (int i = threadIdx.x; i < (1 << SG_LOW); i += blockDim.x) {
         sord[i] = G.lowtab[i];
         srk[i] = G.lowtab[(1 << SG_LOW) + i];
     }
+    for (int i = threadIdx.x; i < (1 << (SG_LOW - 1)); i += blockDim.x) sord9[i] = G.lowtab[(2 << SG_LOW) + i];
+    if (threadIdx.x == 0)
+        for (int q = 0, o = 0; q <= SG_LOW; ++q) {
+            off9[q] = o;
+            o += q <= SG_LOW - 1 ? (int)A.binom[(SG_LOW - 1) * (n + 1) + q] : 0;
+        }
     __syncthreads();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const ull g = (ull)blockIdx.x * SG_WARPS + w;
@@ -1063,11 +1123,18 @@ __global__ void __launch_bounds__(32 * SG_WARPS) stream_group_kernel(PricerArgs 
             tsum += sbin[a * (n + 1) + l + i];
         }
     }
+    // registers per lane for all slots (C(SG_LOW, l)) and for the slots holding one low alternative
+    // (C(SG_LOW - 1, l - 1)); the compact pass runs where it needs fewer
     const int nsl = (int)sbin[SG_LOW * (n + 1) + l];
-    if (nsl <= 32) sg_group<1, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
-    else if (nsl <= 64) sg_group<2, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
-    else if (nsl <= 128) sg_group<4, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
-    else sg_group<SG_REGS, T>(A, G, vals, sbin, sord, srk, lane, l, H, base, tsum, nsl);
+    const int nc = l >= 1 ? (int)sbin[(SG_LOW - 1) * (n + 1) + (l - 1)] : 0;
+    const int rc = (nc + 31) / 32;
+    T *cb = cbuf[w];
+#define SG_CALL(NR, NRC) sg_group<NR, NRC, T>(A, G, vals, sbin, sord, srk, sord9, off9, cb, lane, l, H, base, tsum, nsl)
+    if (nsl <= 32) SG_CALL(1, 1);
+    else if (nsl <= 64) { if (rc <= 1) SG_CALL(2, 1); else SG_CALL(2, 2); }
+    else if (nsl <= 128) { if (rc <= 2) SG_CALL(4, 2); else if (rc == 3) SG_CALL(4, 3); else SG_CALL(4, 4); }
+    else { if (rc <= 3) SG_CALL(SG_REGS, 3); else SG_CALL(SG_REGS, 4); }
+#undef SG_CALL
 }
 
 // ----------------------------------------------------------------- host object
@@ -1316,7 +1383,7 @@ static void choose_mask_form(Pricer &P) {
 // among those of its popcount (once per pricer).
 static void ensure_lowtab(Pricer &P) {
     if (P.lowtab.ptr) return;
-    std::vector<uint16_t> tab(2 << SG_LOW);
+    std::vector<uint16_t> tab((2 << SG_LOW) + (1 << (SG_LOW - 1)));
     int k = 0;
     std::vector<int> rk(SG_LOW + 1, 0);
     for (int q = 0; q <= SG_LOW; ++q)
@@ -1325,6 +1392,10 @@ static void ensure_lowtab(Pricer &P) {
                 tab[k++] = (uint16_t)L;
                 tab[(1 << SG_LOW) + L] = (uint16_t)rk[q]++;
             }
+    k = 2 << SG_LOW;                                      // then the (SG_LOW - 1)-bit masks by (popcount, value)
+    for (int q = 0; q < SG_LOW; ++q)
+        for (int L = 0; L < (1 << (SG_LOW - 1)); ++L)
+            if (__builtin_popcount(L) == q) tab[k++] = (uint16_t)L;
     P.lowtab.ensure(tab.size() * 2);
     RUMB_CUDA(cudaMemcpy(P.lowtab.ptr, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
 }
