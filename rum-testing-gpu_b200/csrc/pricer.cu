@@ -620,7 +620,7 @@ __global__ void rows_kernel(ll mp, const ull *menus, const float *scores, const 
 
 // Row records are read ROW_PF at a time ahead of their use; ROW_NONE pads the last batch (its high
 // part has every bit set, so no tile or group takes it: their high parts have at most 29 bits).
-constexpr int ROW_PF = 8;
+constexpr int ROW_PF = 4;
 #define ROW_NONE make_int4(-1, 0, 0, 0)
 
 // Row records of the float64 max sweep's group form: {menu >> shift, menu & ymask, score low and
