@@ -1363,10 +1363,16 @@ static bool faster_second(Pricer &P, F set) {
     return ms[1] <= ms[0];
 }
 
+// Up to this n a pricer times one sweep of each form at creation and keeps the faster (a layer-kernel
+// sweep is cheap there; the tile and group forms lose where a layer has few tiles or groups and every
+// alternative many rows); above it the tile / group forms are taken (the layer kernels scan every
+// row of every alternative per rank and the cover lists are not built).
+constexpr int TIMED_FORMS_MAX_N = 26;
+
 // Mask storage: the tile sweep from n = 9 on (the layer kernels below that, and above n = 30 the
-// layer table would not fit). Where both run and the cover lists were built (n <= 26), one sweep of
-// each on zero scores picks the faster (both give the same bits); without the lists the tile sweep
-// is taken. RUMB_MASK_FORM = "tile" or "layer" pins the form where it can run.
+// layer table would not fit). Up to TIMED_FORMS_MAX_N one sweep of each on zero scores picks the
+// faster (both give the same bits); above it the tile sweep is taken. RUMB_MASK_FORM = "tile" or
+// "layer" pins the form where it can run.
 static void choose_mask_form(Pricer &P) {
     const int n = P.n;
     const bool tile_ok = n >= MASK_MIN_N_TILE, layer_ok = n <= 30;
@@ -1375,7 +1381,7 @@ static void choose_mask_form(Pricer &P) {
     if (env && std::strcmp(env, "tile") == 0 && tile_ok) { P.mask_tile = true; return; }
     if (env && std::strcmp(env, "layer") == 0 && layer_ok) { P.mask_tile = false; return; }
     if (!tile_ok || !layer_ok) { P.mask_tile = tile_ok; return; }
-    if (P.wmode == W_SCAN) { P.mask_tile = true; return; }
+    if (n > TIMED_FORMS_MAX_N) { P.mask_tile = true; return; }
     P.mask_tile = faster_second(P, [&](bool second) { P.mask_tile = second; });
 }
 
@@ -1400,9 +1406,9 @@ static void ensure_lowtab(Pricer &P) {
     RUMB_CUDA(cudaMemcpy(P.lowtab.ptr, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
 }
 
-// Stream storage: the group sweep from n = 12 on. Without cover lists it is taken; with them one
-// sweep of each form on zero scores picks the faster. RUMB_STREAM_FORM = "group" or "layer" pins
-// the form where it can run.
+// Stream storage: the group sweep from n = 12 on. Up to TIMED_FORMS_MAX_N one sweep of each form on
+// zero scores picks the faster; above it the group sweep is taken. RUMB_STREAM_FORM = "group" or
+// "layer" pins the form where it can run.
 static void choose_stream_form(Pricer &P) {
     const int n = P.n;
     const bool group_ok = n >= SG_MIN_N;
@@ -1422,7 +1428,7 @@ static void choose_stream_form(Pricer &P) {
         RUMB_CUDA(cudaMemGetInfo(&free_b, &total_b));
         if ((double)cap * 4.0 <= 0.25 * (double)free_b) P.dec.ensure((size_t)cap * 4);
     }
-    if (P.wmode == W_SCAN || (env && std::strcmp(env, "group") == 0)) P.stream_group = true;
+    if (n > TIMED_FORMS_MAX_N || (env && std::strcmp(env, "group") == 0)) P.stream_group = true;
     else P.stream_group = faster_second(P, [&](bool second) { P.stream_group = second; });
     if (!P.stream_group) P.dec.release();
 }
@@ -1528,10 +1534,11 @@ void pricer_max64(Pricer *P, const double *scores_host, double *vmax) {
     P->s64.ensure((size_t)std::max<ll>(P->mp, 1) * 8);
     for (int i = 0; i < 2; ++i) P->d64[i].ensure((size_t)cap * 8);
     if (P->mp) RUMB_CUDA(cudaMemcpyAsync(P->s64.ptr, scores_host, (size_t)P->mp * 8, cudaMemcpyHostToDevice, st));
-    // the group form (rows scanned per group of ranks) where no cover lists were built, from n = 12 on
+    // the group form (rows scanned per group of ranks) above TIMED_FORMS_MAX_N where no cover lists
+    // were built, or where RUMB_STREAM_FORM = "group" asks for it
     const char *env = getenv("RUMB_STREAM_FORM");
     const bool group = n >= SG_MIN_N && !(env && std::strcmp(env, "layer") == 0) &&
-                       (P->wmode == W_SCAN || (env && std::strcmp(env, "group") == 0));
+                       ((P->wmode == W_SCAN && n > TIMED_FORMS_MAX_N) || (env && std::strcmp(env, "group") == 0));
     std::vector<ull> bh, b10;
     if (group) {
         ensure_lowtab(*P);

@@ -109,14 +109,15 @@ def test_cover_lists_wide_alternative(ctx):
 
 
 @pytest.mark.parametrize("name,cd,n", CASES, ids=[c[0] for c in CASES])
-def test_max64_sweep_bit_exact(ctx, name, cd, n):
-    """The float64 max sweep (rumb_cg_pricer_max64: the layer kernels over cover lists; rows scanned,
-    from n = 12 the group form) equals the oracle's and the reference's own bf_stream_max64 kernel
-    bit for bit."""
+def test_max64_sweep_bit_exact(ctx, monkeypatch, name, cd, n):
+    """The float64 max sweep (rumb_cg_pricer_max64: the layer kernels over cover lists or scanning
+    rows, and from n = 12 the group form) equals the oracle's and the reference's own
+    bf_stream_max64 kernel bit for bit."""
     import ref_replay
     menus, alts, p32, offsets, _ = O.cg_layout(n, cd[:, 0], cd[:, 1], cd[:, 2])
     rng = np.random.RandomState(13)
-    for lists in (True, False):
+    for lists, form in ((True, "layer"), (False, "layer"), (False, "group")):
+        monkeypatch.setenv("RUMB_STREAM_FORM", form)
         pr = _lib.Pricer(ctx, n, menus, offsets, mode="u24", lists=lists)
         for trial in range(2):
             s = rng.randn(menus.size) * (1.0 if trial == 0 else 1e-3)
