@@ -12,6 +12,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -103,6 +104,41 @@ inline void smem_optin(K *kernel, int bytes, std::atomic<unsigned long long> &do
     if (done.load(std::memory_order_acquire) & bit) return;
     RUMB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     done.fetch_or(bit, std::memory_order_release);
+}
+
+// Programmatic dependent launch for the iteration's kernels. A kernel launched by launch_pdl may be
+// scheduled while the kernel before it on the stream is still finishing (its CTAs take SMs as the
+// earlier kernel's last CTAs retire, and the launch latency is hidden); every such kernel calls
+// pdl_grid_sync() first, before it touches memory: it lets the kernel after it be scheduled in turn,
+// then waits until the kernel before it has completed and its writes are visible. Because every
+// kernel so launched waits before it can complete, completion stays ordered down the stream.
+// RUMB_PDL=0 launches them in plain stream order.
+__device__ __forceinline__ void pdl_grid_sync() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("RUMB_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cuda_check(cudaLaunchKernelEx(&cfg, kern, args...), "cudaLaunchKernelEx");
 }
 
 inline int num_sms(int dev) {

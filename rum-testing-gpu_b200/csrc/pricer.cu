@@ -190,6 +190,7 @@ constexpr int PE_R_SMALL = 32;
 
 template <bool MASK, int PR>
 __global__ void __launch_bounds__(PR * PE_G) layer_eval_kernel(PricerArgs A, float *vals) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     static_assert(PR % 32 == 0 && (PR / 32) * PE_G <= 32, "at most 32 warps");
     __shared__ float pbest[PE_G][PR];
     __shared__ signed char pbx[PE_G][PR];
@@ -251,6 +252,7 @@ __global__ void __launch_bounds__(PR * PE_G) layer_eval_kernel(PricerArgs A, flo
 template <int PR>
 __global__ void __launch_bounds__(PR * PE_G) max64_layer_kernel(PricerArgs A, const double *scores,
                                                                  const double *vprev, double *vcur) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     static_assert(PR % 32 == 0 && (PR / 32) * PE_G <= 32, "at most 32 warps");
     __shared__ double pbest[PE_G][PR];
     __shared__ signed char pok[PE_G][PR];
@@ -317,6 +319,7 @@ __global__ void __launch_bounds__(PR * PE_G) max64_layer_kernel(PricerArgs A, co
 // candidates then merge in x order with `>` (ties -> lowest x).
 template <bool MASK, class IT>
 __global__ void __launch_bounds__(1024) layer_wide_kernel(PricerArgs A, float *vals) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     __shared__ ull sbin[MASK ? 1 : BIN_MAX];
     __shared__ float cv[MAXN_PR];
     __shared__ ull sD;
@@ -404,11 +407,13 @@ __global__ void cover_build_kernel(int n, ull nD, const ull *binom, const ull *l
 // The previous layer's quantized values decoded once to float32 (decode_prev's arithmetic, so the
 // same floats), for the group sweep: a rank reads k predecessors, each a value, an offset and a step.
 __global__ void stream_decode_kernel(PricerArgs A, ull count_prev, float *dec) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     const ull r = blockIdx.x * (ull)blockDim.x + threadIdx.x;
     if (r < count_prev) dec[r] = decode_prev(A, r);
 }
 
 __global__ void __launch_bounds__(PB) stream_quant_kernel(PricerArgs A, const float *vals) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     __shared__ float smin[PB / 32], smax[PB / 32];
     const ull r = (ull)blockIdx.x * PB + threadIdx.x;
     const bool valid = r < A.count;
@@ -682,6 +687,7 @@ static MtOrder mt_order_host() {
 __device__ __forceinline__ int mt_half(int L, int x) { return ((L >> (x + 1)) << x) | (L & ((1 << x) - 1)); }
 
 __global__ void __launch_bounds__(32 * MT_WARPS) mask_tile_kernel(MaskTileArgs A, MtOrder ord) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     __shared__ float wl[MT_WARPS][MT_LOW][MT_TILE / 2];   // w(x, D) for low x, at mt_half(L, x) (x in L)
     __shared__ float vt[MT_WARPS][MT_TILE];
     __shared__ uint8_t bt[MT_WARPS][MT_TILE];
@@ -788,6 +794,7 @@ __global__ void __launch_bounds__(32 * MT_WARPS) mask_tile_kernel(MaskTileArgs A
 // are mask_tile_kernel's, so V and the predecessor bytes are the same bits.
 constexpr int MT_SPLIT = 8;
 __global__ void __launch_bounds__(32 * MT_SPLIT) mask_tile_split_kernel(MaskTileArgs A, MtOrder ord) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     __shared__ float wl[MT_LOW][MT_TILE / 2];
     __shared__ float pv[MT_SPLIT][MT_TILE];
     __shared__ signed char pb[MT_SPLIT][MT_TILE];
@@ -1080,6 +1087,7 @@ __device__ __forceinline__ void sg_group(const PricerArgs &A, const StreamGroupA
 
 template <class T>
 __global__ void __launch_bounds__(32 * SG_WARPS) stream_group_kernel(PricerArgs A, StreamGroupArgs G, float *vals) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     __shared__ ull sbin[BIN_MAX];
     __shared__ uint16_t sord[1 << SG_LOW], srk[1 << SG_LOW], sord9[1 << (SG_LOW - 1)];
     __shared__ int off9[SG_LOW + 1];
@@ -1286,10 +1294,10 @@ static void tile_sweep(cudaStream_t st, int n, ll mp, const ull *menus, const fl
         A.V = V;
         A.P = pred;
         if (A.count < split_below) {                    // too few tiles to fill the GPU: split each tile
-            mask_tile_split_kernel<<<(unsigned)A.count, 32 * MT_SPLIT, 0, st>>>(A, order);
+            launch_pdl(mask_tile_split_kernel, dim3((unsigned)A.count), dim3(32 * MT_SPLIT), 0, st, A, order);
             RUMB_LAUNCH("mask_tile_split_kernel");
         } else {
-            mask_tile_kernel<<<(unsigned)((A.count + MT_WARPS - 1) / MT_WARPS), 32 * MT_WARPS, 0, st>>>(A, order);
+            launch_pdl(mask_tile_kernel, dim3((unsigned)((A.count + MT_WARPS - 1) / MT_WARPS)), dim3(32 * MT_WARPS), 0, st, A, order);
             RUMB_LAUNCH("mask_tile_kernel");
         }
     }
@@ -1582,15 +1590,12 @@ void pricer_max64(Pricer *P, const double *scores_host, double *vmax) {
             G.vprev64 = vp;
             G.vcur64 = vc;
             const ull groups = G.cum[G.lmax - G.lmin + 1];
-            stream_group_kernel<double><<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
-                A, G, nullptr);
+            launch_pdl(stream_group_kernel<double>, dim3((unsigned)((groups + SG_WARPS - 1) / SG_WARPS)), dim3(32 * SG_WARPS), 0, st, A, G, nullptr);
             RUMB_LAUNCH("stream_group_kernel<f64>");
         } else if ((long long)A.count < 2LL * num_sms(c.device) * PE_R) {
-            max64_layer_kernel<PE_R_SMALL><<<(unsigned)((A.count + PE_R_SMALL - 1) / PE_R_SMALL), PE_R_SMALL * PE_G,
-                                             0, st>>>(A, P->s64.as<double>(), vp, vc);
+            launch_pdl(max64_layer_kernel<PE_R_SMALL>, dim3((unsigned)((A.count + PE_R_SMALL - 1) / PE_R_SMALL)), dim3(PE_R_SMALL * PE_G), 0, st, A, P->s64.as<double>(), vp, vc);
         } else {
-            max64_layer_kernel<PE_R><<<(unsigned)((A.count + PE_R - 1) / PE_R), PE_R * PE_G, 0, st>>>(
-                A, P->s64.as<double>(), vp, vc);
+            launch_pdl(max64_layer_kernel<PE_R>, dim3((unsigned)((A.count + PE_R - 1) / PE_R)), dim3(PE_R * PE_G), 0, st, A, P->s64.as<double>(), vp, vc);
         }
         RUMB_LAUNCH("max64_layer_kernel");
         std::swap(cur, prev);
@@ -1625,21 +1630,21 @@ static void run_sweep(Pricer *P, const float *scores) {
             if ((long long)A.count < 2LL * num_sms(c.device) * PE_R) {
                 constexpr int PR = PE_R_SMALL;
                 const unsigned grid = (unsigned)((A.count + PR - 1) / PR);
-                if (mask) layer_eval_kernel<true, PR><<<grid, PR * PE_G, 0, st>>>(A, vals);
-                else layer_eval_kernel<false, PR><<<grid, PR * PE_G, 0, st>>>(A, vals);
+                if (mask) launch_pdl(layer_eval_kernel<true, PR>, dim3(grid), dim3(PR * PE_G), 0, st, A, vals);
+                else launch_pdl(layer_eval_kernel<false, PR>, dim3(grid), dim3(PR * PE_G), 0, st, A, vals);
             } else {
                 const unsigned grid = (unsigned)((A.count + PE_R - 1) / PE_R);
-                if (mask) layer_eval_kernel<true, PE_R><<<grid, PE_R * PE_G, 0, st>>>(A, vals);
-                else layer_eval_kernel<false, PE_R><<<grid, PE_R * PE_G, 0, st>>>(A, vals);
+                if (mask) launch_pdl(layer_eval_kernel<true, PE_R>, dim3(grid), dim3(PE_R * PE_G), 0, st, A, vals);
+                else launch_pdl(layer_eval_kernel<false, PE_R>, dim3(grid), dim3(PE_R * PE_G), 0, st, A, vals);
             }
             RUMB_LAUNCH("layer_eval_kernel");
         };
         auto wide_kernel = [&]() {
             const unsigned threads = 32u * (unsigned)std::min(n, 32), grid = (unsigned)A.count;
-            if (mask && P->wmode == W_LIST16) layer_wide_kernel<true, uint16_t><<<grid, threads, 0, st>>>(A, vals);
-            else if (mask) layer_wide_kernel<true, uint32_t><<<grid, threads, 0, st>>>(A, vals);
-            else if (P->wmode == W_LIST16) layer_wide_kernel<false, uint16_t><<<grid, threads, 0, st>>>(A, vals);
-            else layer_wide_kernel<false, uint32_t><<<grid, threads, 0, st>>>(A, vals);
+            if (mask && P->wmode == W_LIST16) launch_pdl(layer_wide_kernel<true, uint16_t>, dim3(grid), dim3(threads), 0, st, A, vals);
+            else if (mask) launch_pdl(layer_wide_kernel<true, uint32_t>, dim3(grid), dim3(threads), 0, st, A, vals);
+            else if (P->wmode == W_LIST16) launch_pdl(layer_wide_kernel<false, uint16_t>, dim3(grid), dim3(threads), 0, st, A, vals);
+            else launch_pdl(layer_wide_kernel<false, uint32_t>, dim3(grid), dim3(threads), 0, st, A, vals);
             RUMB_LAUNCH("layer_wide_kernel");
         };
         if (P->wmode != W_SCAN && P->wide[A.k]) wide_kernel();
@@ -1729,21 +1734,20 @@ static void run_sweep(Pricer *P, const float *scores) {
                 G.lowtab = P->lowtab.as<uint16_t>();
                 if (P->dec.ptr && A.mode >= 2) {
                     const ull cprev = P->counts[k - 1];
-                    stream_decode_kernel<<<grid_for((ll)cprev, 256), 256, 0, st>>>(A, cprev, P->dec.as<float>());
+                    launch_pdl(stream_decode_kernel, dim3(grid_for((ll)cprev, 256)), dim3(256), 0, st, A, cprev, P->dec.as<float>());
                     RUMB_LAUNCH("stream_decode_kernel");
                     A.vprev_dec = P->dec.as<float>();
                 } else if (A.mode == 1) {
                     A.vprev_dec = A.vprev_f;                    // float32 storage is its own decoded copy
                 }
                 const ull groups = G.cum[G.lmax - G.lmin + 1];
-                stream_group_kernel<float><<<(unsigned)((groups + SG_WARPS - 1) / SG_WARPS), 32 * SG_WARPS, 0, st>>>(
-                    A, G, P->vals.as<float>());
+                launch_pdl(stream_group_kernel<float>, dim3((unsigned)((groups + SG_WARPS - 1) / SG_WARPS)), dim3(32 * SG_WARPS), 0, st, A, G, P->vals.as<float>());
                 RUMB_LAUNCH("stream_group_kernel");
             } else {
                 layer(A, false, P->vals.as<float>());
             }
             if (A.mode != 1) {
-                stream_quant_kernel<<<(unsigned)((A.count + PB - 1) / PB), PB, 0, st>>>(A, P->vals.as<float>());
+                launch_pdl(stream_quant_kernel, dim3((unsigned)((A.count + PB - 1) / PB)), dim3(PB), 0, st, A, P->vals.as<float>());
                 RUMB_LAUNCH("stream_quant_kernel");
             }
             std::swap(cur, prev);

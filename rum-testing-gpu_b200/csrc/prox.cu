@@ -34,6 +34,7 @@ __device__ __forceinline__ uint32_t cb32(uint32_t mask, int x) {
 
 template <class T, int N>
 __global__ void __launch_bounds__(PT_THREADS, 5) prox_tile_kernel(ProxTileArgs<T> P) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     extern __shared__ __align__(128) unsigned char pt_smem[];
     if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
     {
@@ -200,6 +201,7 @@ constexpr int PT_PLAIN = 0, PT_SINGLE = 1, PT_MIXED = 2;
 
 template <class T, int N>
 __global__ void __launch_bounds__(PT_THREADS, 5) prox_tau_kernel(ProxTileArgs<T> P) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     extern __shared__ __align__(128) unsigned char pt_smem[];
     if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
     {
@@ -372,6 +374,7 @@ __global__ void __launch_bounds__(PT_THREADS, 5) prox_tau_kernel(ProxTileArgs<T>
 // (more resident warps for the same shared memory, half of each thread's dependent chain).
 template <class T, int N, int TPM = 1>
 __global__ void __launch_bounds__(PT_THREADS * TPM, TPM == 1 ? 6 : 5) prox_tau2_kernel(ProxTileArgs<T> P) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     constexpr int NT = PT_THREADS * TPM;
     extern __shared__ __align__(128) unsigned char pt_smem[];
     if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
@@ -619,6 +622,7 @@ __device__ __forceinline__ uint32_t group_or(uint32_t v, unsigned m) {
 
 template <class T, int N, int G>
 __global__ void __launch_bounds__(256, G >= 4 ? 4 : 2) prox_lanes_kernel(ProxTileArgs<T> P) {
+    pdl_grid_sync();                                       // launched by launch_pdl
     if (P.active && !P.active[blockIdx.y]) return;         // a retired slot (uniform per CTA)
     const ll boff = (ll)blockIdx.y * P.bstride;
     const T *X = P.x + boff;
@@ -754,7 +758,7 @@ static void launch_tile_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) 
     const size_t smem = prox_tile_smem<T>(N);
     smem_optin(prox_tile_kernel<T, N>, (int)smem, optin);
     dim3 grid((unsigned)(1LL << (N - PT_M)), (unsigned)slots);
-    prox_tile_kernel<T, N><<<grid, PT_THREADS, smem, st>>>(P);
+    launch_pdl(prox_tile_kernel<T, N>, grid, dim3(PT_THREADS), smem, st, P);
     RUMB_LAUNCH("prox_tile_kernel");
 }
 
@@ -764,7 +768,7 @@ static void launch_tau_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     const size_t smem = prox_tile_smem<T>(N);
     smem_optin(prox_tau_kernel<T, N>, (int)smem, optin);
     dim3 grid((unsigned)(1LL << (N - PT_M)), (unsigned)slots);
-    prox_tau_kernel<T, N><<<grid, PT_THREADS, smem, st>>>(P);
+    launch_pdl(prox_tau_kernel<T, N>, grid, dim3(PT_THREADS), smem, st, P);
     RUMB_LAUNCH("prox_tau_kernel");
 }
 
@@ -775,14 +779,14 @@ static void launch_tau2_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) 
     const size_t smem = 256 + 2 * (size_t)E_max * sizeof(T) + (size_t)((E_max / VEC + 31) / 32) * VEC * 4;
     smem_optin(prox_tau2_kernel<T, N, TPM>, (int)smem, optin);
     dim3 grid((unsigned)(1LL << (N - PT_M)), (unsigned)slots);
-    prox_tau2_kernel<T, N, TPM><<<grid, PT_THREADS * TPM, smem, st>>>(P);
+    launch_pdl(prox_tau2_kernel<T, N, TPM>, grid, dim3(PT_THREADS * TPM), smem, st, P);
     RUMB_LAUNCH("prox_tau2_kernel");
 }
 
 template <class T, int N, int G>
 static void launch_lanes_n(const ProxTileArgs<T> &P, cudaStream_t st, int slots) {
     dim3 grid((unsigned)(((1LL << N) * G) / 256), (unsigned)slots);
-    prox_lanes_kernel<T, N, G><<<grid, 256, 0, st>>>(P);
+    launch_pdl(prox_lanes_kernel<T, N, G>, grid, dim3(256), 0, st, P);
     RUMB_LAUNCH("prox_lanes_kernel");
 }
 

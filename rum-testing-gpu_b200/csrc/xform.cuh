@@ -203,6 +203,7 @@ constexpr int xf_min_blocks() {
 
 template <class T, class TI, int L, int RB, int WB, int KIND>
 __global__ void __launch_bounds__(32 << WB, xf_min_blocks<L, RB, WB, KIND>()) xform_pass(XfArgs<T, TI> A) {
+    pdl_grid_sync();                                        // launched by launch_pdl: nothing read before
     extern __shared__ __align__(16) unsigned char xf_smem[];
     T *sm = reinterpret_cast<T *>(xf_smem);
     constexpr int R = 1 << RB;
@@ -406,7 +407,7 @@ inline void xf_launch_one(const XfArgs<T, TI> &A, int n, cudaStream_t st, int sl
         snprintf(nm, sizeof nm, "xform<%s,%s>[s=%d,B=%d]", sizeof(T) == 8 ? "f64" : "f32", kn[KIND], A.s0, A.B);
         prof_begin(nm, bytes, st);
     }
-    xform_pass<T, TI, L, RB, WB, KIND><<<dim3((unsigned)tiles, (unsigned)slots), 32 << WB, smem, st>>>(A);
+    launch_pdl(xform_pass<T, TI, L, RB, WB, KIND>, dim3((unsigned)tiles, (unsigned)slots), dim3(32u << WB), smem, st, A);
     RUMB_LAUNCH("xform_pass");
     prof_end(st);
 }
