@@ -1,4 +1,4 @@
-"""Records the Flow-CG column sequence of BASELINE config 3 as a golden vector.
+"""Records the Flow-CG column sequence of the n18_d05pct_k50 workload (n = 18, 0.5 % menus) as a golden vector.
 
     python tests/golden/make_cg_golden.py          # on a GPU host, after build()
 

@@ -308,10 +308,10 @@ def test_pricer_matches_recorded_reference_kernels(ctx):
 _CG3 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cg_config3.npz")
 
 
-@pytest.mark.skipif(not os.path.exists(_CG3), reason="config 3 column sequence not recorded")
+@pytest.mark.skipif(not os.path.exists(_CG3), reason="the n18_d05pct_k50 column sequence is not recorded")
 @pytest.mark.parametrize("mode", ["u24", "u16"])
 def test_config3_column_sequence_matches_recorded_reference(ctx, mode):
-    """Flow-CG at n = 18, 0.5 % menus to abs 1e-5 (uint16: 1,000 columns,
+    """Flow-CG at n = 18, 0.5 % menus (the n18_d05pct_k50 workload) to abs 1e-5 (uint16: 1,000 columns,
     whose quantization margin keeps the bound above abs 1e-5): every CG iteration's column
     is the recorded one, which the reference's own pricing kernels picked on the same residual
     (tests/golden/make_cg_golden.py), and the bracket is the recorded bracket."""

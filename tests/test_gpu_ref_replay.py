@@ -165,7 +165,7 @@ def test_certified_bracket_matches_reference_float64(ctx, case, dtype):
         assert res["iters"] == ref["iters"], (res["iters"], ref["iters"])
 
 
-# ------------------------------------------------------------------ Flow-CG config 3, every column
+# ------------------------------------------------------------------ Flow-CG n18_d05pct_k50, every column
 # uint16's block quantization margin enters the Frank-Wolfe bound, and at this density it keeps the
 # bracket above abs 1e-5 (the run reaches 4,000 columns without certifying): uint16 runs a fixed
 # number of columns instead
@@ -199,7 +199,7 @@ def _config3_run(ctx, mode, check_reference):
 
 @pytest.mark.parametrize("mode", ["u24", "u16"])
 def test_config3_columns_match_reference_kernels_every_iteration(ctx, mode):
-    """BASELINE config 3's check: Flow-CG at n = 18, 0.5 % density, run to abs 1e-5 (uint24; uint16
+    """The n18_d05pct_k50 workload's check: Flow-CG at n = 18, 0.5 % density, run to abs 1e-5 (uint24; uint16
     for 1,000 columns, see CG3_MAX), and the column
     (the ranking) the library prices at every CG iteration is the one the reference's own
     bf_stream_u24 / bf_stream_u16 kernels and backtrace pick on the same residual
@@ -213,7 +213,7 @@ def test_config3_columns_match_reference_kernels_every_iteration(ctx, mode):
         np.testing.assert_array_equal(np.array(res["picked"]), g["picked_" + mode])
 
 
-# ------------------------------------------------------------------ large lattices
+# ------------------------------------------------------------------ large lattices (n = 28)
 @pytest.mark.parametrize("mode", ["f32", "f32_stream", "u16", "u24"])
 def test_stream_pricer_at_n28_matches_reference_kernels(ctx, mode):
     """The stream pricer at n = 28 (pairwise menus, 756 rows; 2^28 subsets, rows scanned per
