@@ -1,4 +1,4 @@
-"""The binding a maintainer of the reference would add, written against
+"""The binding a maintainer of the reference would add to its solver package, written against
 module objects so that a test can install it: it routes the reference's RUM runner and planner
 tables for bm_admm and flow_cg (solver/rum_solver.py:858,1186-1187) to rumb's."""
 

@@ -1,4 +1,4 @@
-"""The reference-side binding (INTEGRATION.md section 3, tests/rumb_backend_stub.py) installed in
+"""The reference-side binding (tests/rumb_backend_stub.py) installed in
 the reference's own RUM class: calculate_distance(method="bm_admm") through the reference's
 planner and runner tables reaches rumb's planner and runner, and returns the Result rumb's own RUM
 returns (distance, bracket, exit flag, iterations, p_fit). Runs where the reference's source tree
