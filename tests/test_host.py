@@ -374,3 +374,18 @@ def test_records_byte_compatible_with_the_reference(fake_gpu):
                                                                                       seed=3).record()
     rec.pop("when")
     assert json.dumps(rec, indent=1) == g["bootstrap_replies_record"]
+
+
+def test_prox_profile_records_match_the_built_source():
+    """bench.py reads the prox's DRAM traffic from the committed ncu summary whose source digest is
+    the digest of csrc/prox.cu + prox.cuh as built, and reports null otherwise: every prox form the
+    tuner picks at the bench's workload (one or two threads per menu) has a record for this source."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(os.path.dirname(os.path.dirname(
+        os.path.abspath(__file__))), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for kernel in ("prox_pair<f64>", "prox_tau2<f64>"):
+        traffic, src = bench.kernel_traffic(kernel)
+        assert traffic is not None and src is not None, kernel
+        assert 55e6 < traffic < 70e6, (kernel, traffic)
